@@ -1,0 +1,289 @@
+// cp_integrand.cuh -- FP32 evaluation of the pp -> 2 jets hard-process integrand, shared by
+// every kernel of the integrator (and compiled for the host by the accuracy probe in tests).
+//
+// Physics follows Pythia 8.317:
+//   matrix elements      pythia8317/src/SigmaQCD.cc:115-325 (Sigma2gg2gg, gg2qqbar, qg2qg,
+//                        qq2qq, qqbar2gg sigmaKin / sigmaHat)
+//   channel sums         pythia8317/src/SigmaProcess.cc:124-193 (initFlux) and :423-480
+//                        (sigmaPDF); CONVERT2MB :24
+//   scales               pythia8317/src/SigmaProcess.cc:846-925 (store2Kin, massless branch)
+//   alpha_s              pythia8317/src/StandardModel.cc:189-215 (first order)
+//   CTEQ5L               pythia8317/src/PartonDistributions.cc:922-1062
+//   region and Jacobian  pythia8317/src/PhaseSpace.cc:1149-1250 (limitTau/Y/Z), :1072-1074
+//
+// FP32 conditioning.  The formulas are evaluated in algebraically identical forms that keep
+// FP32 accurate to ~1e-6 relative:
+//   * 1 - z and 1 + z come from the complement of the zMax bound, 1 - zMax = r / (1 + zMax),
+//     r = pT^2_min / p^2 = tauMin / tau = exp(x0 ln tauMin), never from a rounded z;
+//   * ln x1 = -2 yMax (1 - v), ln x2 = -2 yMax v (v the rapidity variable), so x = exp(ln x)
+//     and 1 - x = -expm1(ln x) are both accurate and CTEQ5L's y = -ln x needs no log;
+//   * in CTEQ5L's exponent af0 (1-x) + af3 x + af1 y^p (1 + af8 u), whose O(100) terms cancel
+//     for the gluon, the constant parts are pre-combined in FP64 on the host:
+//       A = af0 + af1, B = af3 - af0, C = af1 af8, and y^p = 1 + expm1(p ln y), giving
+//       exponent = A + B x + C u + af1 expm1(p ln y) (1 + af8 u) + part3 + part4;
+//   * matrix elements are written in tHat/sHat and uHat/sHat with all terms of one sign.
+#pragma once
+#include <stdint.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define CP_HD __host__ __device__ __forceinline__
+#else
+#define CP_HD static inline
+#endif
+
+#ifndef CP_PI_F
+#define CP_PI_F 3.14159265358979f
+#endif
+
+// ------------------------------------------------------------------------------------------
+// Uniform parameters of the hadronic integrand (built on the host in FP64, stored in FP32).
+// ------------------------------------------------------------------------------------------
+struct CpCteqPoly {
+  // per parametrisation i: polynomial coefficients in sb1 = ln ln(Q/alpha_i) - 1.2
+  float A[3], B[3], af1[3], af2[3], p[3], af5[3], af6[3], af7[3], af8[3];
+  float lnAlpha;  // ln(alpha_i)
+  float qlim;     // max(Qmin_i, alpha_i)
+  float qmin;     // Qmin_i
+  float ut1;      // ut1_i
+  float eut2;     // exp(ut2_i)
+  int   useX1L;   // ut2_i < -100: part4 uses ln(1 - x) twice
+};
+
+struct CpHadParams {
+  CpCteqPoly cteq[8];
+  float lnTauMin;     // ln(tauMin), tauMin = max(4 pTmin^2, mHatMin^2) / s
+  float K0;           // 2 pi CONVERT2MB (-ln tauMin) / s : w = K0 alpha_s^2 B yMax zMax / tau
+  float s;            // sqrt(s)^2
+  float kR, kF;       // muR^2 = kR pT^2, muF^2 = kF pT^2
+  float lnL2[4];      // ln Lambda_nf^2, nf = 3, 4, 5, 6
+  float thr2[3];      // mc^2, mb^2, mt^2
+  float scale2Min;    // (1.07 Lambda_3)^2
+  float nQuarkNew;    // HardQCD:nQuarkNew
+  float mask[5];      // gg2gg, gg2qqbar, qg2qg, qq2qq, qqbar2gg switches (0 or 1)
+  int   nfmax6;       // 1 if nf = 6 above mt
+};
+
+// Math on the device is CUDA's accurate single-precision library; on the host, libm.
+CP_HD float cp_expf(float x) { return expf(x); }
+CP_HD float cp_logf(float x) { return logf(x); }
+CP_HD float cp_expm1f(float x) { return expm1f(x); }
+CP_HD float cp_sqrtf(float x) { return sqrtf(x); }
+CP_HD float cp_fmaf(float a, float b, float c) { return fmaf(a, b, c); }
+CP_HD float cp_poly(const float c[3], float t) { return cp_fmaf(cp_fmaf(c[2], t, c[1]), t, c[0]); }
+
+// ------------------------------------------------------------------------------------------
+// alpha_s(Q2) at first order with threshold matching (StandardModel.cc:189-215).
+// ------------------------------------------------------------------------------------------
+CP_HD float cp_alphas(const CpHadParams& P, float Q2)
+{
+  if (Q2 < P.scale2Min) Q2 = P.scale2Min;
+  float lnQ2 = cp_logf(Q2);
+  float b0, lnL2;
+  if (Q2 > P.thr2[2] && P.nfmax6) { b0 = 21.f; lnL2 = P.lnL2[3]; }
+  else if (Q2 > P.thr2[1]) { b0 = 23.f; lnL2 = P.lnL2[2]; }
+  else if (Q2 > P.thr2[0]) { b0 = 25.f; lnL2 = P.lnL2[1]; }
+  else { b0 = 27.f; lnL2 = P.lnL2[0]; }
+  return (12.f * CP_PI_F) / (b0 * (lnQ2 - lnL2));
+}
+
+// Q-dependent CTEQ5L coefficients, shared by both beams.
+struct CpCteqQ {
+  float A, B, af1, af2, p, af5, af6, af7, af8, qfac;
+};
+
+CP_HD void cp_cteq_q(const CpHadParams& P, float Q2, CpCteqQ q[8])
+{
+  // Q2 clamp of PartonDistributions.cc:925
+  if (Q2 > 1e8f) Q2 = 1e8f;
+  if (Q2 < 1.f) Q2 = 1.f;
+  float Q = cp_sqrtf(Q2);
+  float lnQ = 0.5f * cp_logf(Q2);
+  float invQ = 1.f / Q;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const CpCteqPoly& c = P.cteq[i];
+    float sb1 = cp_logf(lnQ - c.lnAlpha) - 1.2f;
+    q[i].A = cp_poly(c.A, sb1);
+    q[i].B = cp_poly(c.B, sb1);
+    q[i].af1 = cp_poly(c.af1, sb1);
+    q[i].af2 = cp_poly(c.af2, sb1);
+    q[i].p = cp_poly(c.p, sb1);
+    q[i].af5 = cp_poly(c.af5, sb1);
+    q[i].af6 = cp_poly(c.af6, sb1);
+    q[i].af7 = cp_poly(c.af7, sb1);
+    q[i].af8 = cp_poly(c.af8, sb1);
+    q[i].qfac = (Q > c.qlim) ? (1.f - c.qmin * invQ) : 0.f;
+  }
+}
+
+// Proton x f for one beam from ln x (<= 0): out = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.
+CP_HD void cp_cteq_x(const CpHadParams& P, const CpCteqQ q[8], float lnx, float out[8])
+{
+  // x clamp of PartonDistributions.cc:926
+  const float lnxMin = -13.815510558f;   // ln 1e-6
+  if (lnx < lnxMin) lnx = lnxMin;
+  float x = cp_expf(lnx);
+  float omx = -cp_expm1f(lnx);           // 1 - x
+  if (omx < 1e-10f) { omx = 1e-10f; x = 1.f - 1e-10f; lnx = -1e-10f; }
+  float y = -lnx;
+  float lny = cp_logf(y);
+  float u = lnx + 11.512925465f;         // ln(x / 1e-5)
+  float x1L = cp_logf(omx);
+  float sumUbarDbar = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const CpCteqPoly& c = P.cteq[i];
+    const CpCteqQ& a = q[i];
+    // y^p - 1 with the rounding residual of p ln y carried into first order
+    float ah = a.p * lny;
+    float al = cp_fmaf(a.p, lny, -ah);
+    float ym1 = cp_expm1f(ah);
+    ym1 = cp_fmaf(1.f + ym1, al, ym1);
+    float U = cp_fmaf(a.af8, u, 1.f);
+    float part3 = x * omx * (a.af5 + a.af6 * omx + a.af7 * x * omx);
+    float L = c.useX1L ? x1L : cp_logf(omx + c.eut2);
+    float e = a.A + a.B * x + (a.af1 * a.af8) * u + a.af1 * ym1 * U + part3 + c.ut1 * x1L + a.af2 * L;
+    float answer = x * cp_expf(e) * a.qfac;
+    if (i == 3) sumUbarDbar = x * answer;
+    else if (i == 4) {
+      float inv = 1.f / (1.f + answer);
+      out[3] = sumUbarDbar * inv;
+      out[4] = sumUbarDbar * answer * inv;
+    } else {
+      out[i] = x * answer;
+    }
+  }
+  // max(0, .) of PDF::xf (PartonDistributions.cc:133-180)
+#pragma unroll
+  for (int k = 0; k < 8; ++k) out[k] = out[k] > 0.f ? out[k] : 0.f;
+}
+
+// ------------------------------------------------------------------------------------------
+// Channel sum B = sum over processes and pairs of bracket(t', u') * xfA * xfB, where
+//   dsigma/dtHat = pi alpha_s^2 / sH^2 * bracket,   t' = tH/sH, u' = uH/sH.
+// ------------------------------------------------------------------------------------------
+struct CpBrackets {
+  float gg2gg, gg2qqbar, qg2qg, qqbar2gg, qqT, qqU, qqTU, qqST;
+};
+
+CP_HD void cp_brackets(const CpHadParams& P, float tp, float up, CpBrackets& b)
+{
+  float rt = 1.f / tp, ru = 1.f / up, tu = tp * ru, ut = up * rt;
+  // Sigma2gg2gg::sigmaKin: each 9/4 (a^2 + 2a + 3 + 2/a + 1/a^2) = 9/4 ((a+1)^2 + (1/a+1)^2 + 1)
+  float sTS = (tp + 1.f) * (tp + 1.f) + (rt + 1.f) * (rt + 1.f) + 1.f;
+  float sUS = (up + 1.f) * (up + 1.f) + (ru + 1.f) * (ru + 1.f) + 1.f;
+  float sTU = (tu + 1.f) * (tu + 1.f) + (ut + 1.f) * (ut + 1.f) + 1.f;
+  b.gg2gg = 0.5f * 2.25f * (sTS + sUS + sTU);
+  // Sigma2gg2qqbar::sigmaKin
+  b.gg2qqbar = P.nQuarkNew * ((1.f / 6.f) * (ut + tu) - (3.f / 8.f) * (up * up + tp * tp));
+  // Sigma2qg2qg::sigmaKin
+  b.qg2qg = (up * up + 1.f) * (rt * rt) - (4.f / 9.f) * (up + ru);
+  // Sigma2qqbar2gg::sigmaKin
+  b.qqbar2gg = 0.5f * ((32.f / 27.f) * (ut + tu) - (8.f / 3.f) * (up * up + tp * tp));
+  // Sigma2qq2qq::sigmaKin terms
+  b.qqT = (4.f / 9.f) * (1.f + up * up) * (rt * rt);
+  b.qqU = (4.f / 9.f) * (1.f + tp * tp) * (ru * ru);
+  b.qqTU = -(8.f / 27.f) * (rt * ru);
+  b.qqST = -(8.f / 27.f) * (up * up) * rt;
+}
+
+CP_HD float cp_channel_sum(const CpHadParams& P, const CpBrackets& b, const float A[8], const float Bq[8])
+{
+  // flavour sums over q = +-1..+-5 (s, c, b enter twice: quark = antiquark)
+  float QA = A[0] + A[1] + A[3] + A[4] + 2.f * (A[5] + A[6] + A[7]);
+  float QB = Bq[0] + Bq[1] + Bq[3] + Bq[4] + 2.f * (Bq[5] + Bq[6] + Bq[7]);
+  float Dsame = A[0] * Bq[0] + A[1] * Bq[1] + A[3] * Bq[3] + A[4] * Bq[4] +
+                2.f * (A[5] * Bq[5] + A[6] * Bq[6] + A[7] * Bq[7]);
+  float Dopp = A[0] * Bq[4] + A[4] * Bq[0] + A[1] * Bq[3] + A[3] * Bq[1] +
+               2.f * (A[5] * Bq[5] + A[6] * Bq[6] + A[7] * Bq[7]);
+  float G = A[2] * Bq[2];
+  float sum = G * (P.mask[0] * b.gg2gg + P.mask[1] * b.gg2qqbar);
+  sum += P.mask[2] * b.qg2qg * (QA * Bq[2] + A[2] * QB);
+  // Sigma2qq2qq::sigmaHat: identical 1/2 (T + U + TU), q qbar T + ST, otherwise T
+  sum += P.mask[3] * (QA * QB * b.qqT + Dsame * (0.5f * (b.qqU + b.qqTU - b.qqT)) + Dopp * b.qqST);
+  sum += P.mask[4] * Dopp * b.qqbar2gg;
+  return sum;
+}
+
+// ------------------------------------------------------------------------------------------
+// Weight f * J_base of a point x in [0,1]^3 (x0 -> tau, x1 -> y, x2 -> z), in mb.
+// ------------------------------------------------------------------------------------------
+struct CpKin {
+  float tau, yMax, zMax, sH, omz, opz, lnx1, lnx2, pT2, alphaS;
+};
+
+CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, CpKin* kin)
+{
+  float lnTau = (1.f - x0) * P.lnTauMin;
+  float tau = cp_expf(lnTau);
+  float invTau = cp_expf(-lnTau);
+  float yMax = -0.5f * lnTau;
+  float r = cp_expf(x0 * P.lnTauMin);            // pT^2_min / p^2 = tauMin / tau
+  float zMax = cp_sqrtf(-cp_expm1f(x0 * P.lnTauMin));   // sqrt(1 - r) without cancellation
+  float omzMax = r / (1.f + zMax);               // 1 - zMax
+  float omz = cp_fmaf(2.f * zMax, 1.f - x2, omzMax);   // 1 - z
+  float opz = cp_fmaf(2.f * zMax, x2, omzMax);         // 1 + z
+  float tp = -0.5f * omz, up = -0.5f * opz;
+  float sH = tau * P.s;
+  float pT2 = 0.25f * sH * omz * opz;
+  float lnx1 = -2.f * yMax * (1.f - x1);
+  float lnx2 = -2.f * yMax * x1;
+  float alphaS = cp_alphas(P, P.kR * pT2);
+  CpCteqQ q[8];
+  cp_cteq_q(P, P.kF * pT2, q);
+  float fa[8], fb[8];
+  cp_cteq_x(P, q, lnx1, fa);
+  cp_cteq_x(P, q, lnx2, fb);
+  CpBrackets b;
+  cp_brackets(P, tp, up, b);
+  float B = cp_channel_sum(P, b, fa, fb);
+  if (kin) {
+    kin->tau = tau; kin->yMax = yMax; kin->zMax = zMax; kin->sH = sH; kin->omz = omz;
+    kin->opz = opz; kin->lnx1 = lnx1; kin->lnx2 = lnx2; kin->pT2 = pT2; kin->alphaS = alphaS;
+  }
+  if (!(zMax > 0.f)) return 0.f;
+  return P.K0 * (alphaS * alphaS) * B * yMax * zMax * invTau;
+}
+
+// ------------------------------------------------------------------------------------------
+// Philox-4x32-10 (Salmon et al., SC'11) and the point -> words layout used everywhere:
+//   key = (seed lo, seed hi), counter = (point lo, point hi, iteration, stream).
+// Words 0..2 drive the three map dimensions, word 3 the unweighting accept draw.
+// ------------------------------------------------------------------------------------------
+CP_HD void cp_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1,
+                     uint32_t out[4])
+{
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+#if defined(__CUDA_ARCH__)
+    uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+#else
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+#endif
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+CP_HD void cp_point_words(uint64_t seed, uint64_t point, uint32_t iter, uint32_t stream, uint32_t w[4])
+{
+  cp_philox((uint32_t)point, (uint32_t)(point >> 32), iter, stream, (uint32_t)seed,
+            (uint32_t)(seed >> 32), w);
+}
+
+// 24-bit uniform in [0, 1): exact in FP32 and FP64
+CP_HD float cp_u24(uint32_t w) { return (float)(w >> 8) * (1.f / 16777216.f); }
+
+// VEGAS bin and in-bin fraction of a 24-bit word, in integer arithmetic (exact everywhere)
+CP_HD void cp_bin_frac(uint32_t w, int nb, int& bin, float& frac)
+{
+  uint32_t m = (w >> 8) * (uint32_t)nb;      // < 2^24 * nb <= 2^31 for nb <= 128
+  bin = (int)(m >> 24);
+  frac = (float)(m & 0xFFFFFFu) * (1.f / 16777216.f);
+}

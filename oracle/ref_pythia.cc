@@ -1,0 +1,158 @@
+// ref_pythia.cc -- driver over the reference's own Pythia 8.317 code (built by oracle/ref.mk).
+//
+// TEST INFRASTRUCTURE ONLY: it produces golden vectors for the oracle and is the timed CPU
+// reference arm of bench.py.  It calls stock Pythia through its public API:
+//   pdf    <x> <Q2> ...                 CTEQ5L xf for ids -5..5, 21   (PDF::xf, PartonDistributions.cc:122)
+//   alphas <aSmZ> <Q2> ...              first-order AlphaStrong       (StandardModel.cc:42-252)
+//   sigma  <file>                       per process set2Kin + sigmaKin + sigmaPDF on lines
+//                                       "x1 x2 sH tH"                (SigmaProcess.cc:423-480,846-925)
+//   gen    <nAccepted> <seed> <threads> [pTmin] [aSmZ]
+//                                       ProcessLevel-only HardQCD generation, one Pythia per thread,
+//                                       prints tried/accepted/s and sigmaGen +- sigmaErr
+// Settings follow the hadronic dijet configuration: pp at 13 TeV, HardQCD gg2gg, qg2qg,
+// qqbar2gg, gg2qqbar, qq2qq on, PhaseSpace:pTHatMin = 20, PDF:pSet = 2 (CTEQ5L),
+// SigmaProcess:alphaSvalue = 0.13 at first order, parton and hadron levels off.
+#include "Pythia8/Pythia.h"
+#include "Pythia8/SigmaQCD.h"
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <thread>
+#include <vector>
+#include <unistd.h>
+#include <libgen.h>
+#include <climits>
+
+using namespace Pythia8;
+
+static std::string xmlDir()
+{
+  const char* env = getenv("CP_PYTHIA_XMLDOC");
+  if (env) return env;
+  char buf[PATH_MAX];
+  ssize_t n = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+  if (n <= 0) return "xmldoc";
+  buf[n] = 0;
+  return std::string(dirname(buf)) + "/xmldoc";
+}
+
+static void configure(Pythia& p, double pTmin, double aSmZ, bool processes, int seed)
+{
+  p.readString("Beams:idA = 2212");
+  p.readString("Beams:idB = 2212");
+  p.readString("Beams:eCM = 13000.");
+  if (processes) {
+    p.readString("HardQCD:gg2gg = on");
+    p.readString("HardQCD:qg2qg = on");
+    p.readString("HardQCD:qqbar2gg = on");
+    p.readString("HardQCD:gg2qqbar = on");
+    p.readString("HardQCD:qq2qq = on");
+  }
+  p.readString("PhaseSpace:pTHatMin = " + std::to_string(pTmin));
+  p.readString("PDF:pSet = 2");
+  p.readString("SigmaProcess:alphaSvalue = " + std::to_string(aSmZ));
+  p.readString("SigmaProcess:alphaSorder = 1");
+  p.readString("PartonLevel:all = off");
+  p.readString("HadronLevel:all = off");
+  p.readString("Next:numberCount = 0");
+  p.readString("Print:quiet = on");
+  p.readString("Random:setSeed = on");
+  p.readString("Random:seed = " + std::to_string(seed));
+}
+
+static int cmd_pdf(int argc, char** argv)
+{
+  CTEQ5L pdf(2212);
+  for (int i = 0; i + 1 < argc; i += 2) {
+    double x = atof(argv[i]), Q2 = atof(argv[i + 1]);
+    printf("%.17g %.17g", x, Q2);
+    const int ids[11] = {-5, -4, -3, -2, -1, 1, 2, 3, 4, 5, 21};
+    for (int k = 0; k < 11; ++k) printf(" %.17g", pdf.xf(ids[k], x, Q2));
+    printf("\n");
+  }
+  return 0;
+}
+
+static int cmd_alphas(int argc, char** argv)
+{
+  AlphaStrong a;
+  a.init(atof(argv[0]), 1, 6, false);
+  for (int i = 1; i < argc; ++i) printf("%.17g %.17g\n", atof(argv[i]), a.alphaS(atof(argv[i])));
+  return 0;
+}
+
+static int cmd_sigma(const char* path)
+{
+  Pythia p(xmlDir(), false);
+  configure(p, 20.0, 0.13, false, 1);
+  std::vector<SigmaProcessPtr> procs = {
+      std::make_shared<Sigma2gg2gg>(), std::make_shared<Sigma2gg2qqbar>(),
+      std::make_shared<Sigma2qg2qg>(), std::make_shared<Sigma2qq2qq>(),
+      std::make_shared<Sigma2qqbar2gg>()};
+  for (auto& s : procs) p.addSigmaPtr(s);
+  if (!p.init()) { fprintf(stderr, "pythia init failed\n"); return 1; }
+  std::ifstream in(path);
+  double x1, x2, sH, tH;
+  while (in >> x1 >> x2 >> sH >> tH) {
+    printf("%.17g %.17g %.17g %.17g", x1, x2, sH, tH);
+    for (auto& s : procs) {
+      s->set2Kin(x1, x2, sH, tH, 0., 0., 1., 1.);
+      double sp = s->sigmaPDF();
+      printf(" %.17g", sp);
+    }
+    printf(" %.17g %.17g\n", procs[0]->alphaSRen(), procs[0]->Q2Ren());
+  }
+  return 0;
+}
+
+struct GenResult { long tried = 0, accepted = 0; double sigma = 0, err = 0; };
+
+static int cmd_gen(long nAcc, int seed, int threads, double pTmin, double aSmZ)
+{
+  std::vector<GenResult> res(threads);
+  std::vector<double> initT(threads);
+  auto worker = [&](int t) {
+    Pythia p(xmlDir(), false);
+    configure(p, pTmin, aSmZ, true, seed + t);
+    if (!p.init()) return;
+    long per = nAcc / threads + (t < nAcc % threads ? 1 : 0);
+    for (long i = 0; i < per; ++i) p.next();
+    res[t].tried = p.info.nTried();
+    res[t].accepted = p.info.nAccepted();
+    res[t].sigma = p.info.sigmaGen();
+    res[t].err = p.info.sigmaErr();
+  };
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> th;
+  for (int t = 0; t < threads; ++t) th.emplace_back(worker, t);
+  for (auto& x : th) x.join();
+  double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  long tried = 0, acc = 0;
+  double wsum = 0, w2 = 0;
+  for (auto& r : res) {
+    tried += r.tried;
+    acc += r.accepted;
+    if (r.err > 0) { wsum += r.sigma / (r.err * r.err); w2 += 1.0 / (r.err * r.err); }
+  }
+  double sig = w2 > 0 ? wsum / w2 : 0, err = w2 > 0 ? 1.0 / sqrt(w2) : 0;
+  printf("{\"tried\": %ld, \"accepted\": %ld, \"seconds\": %.6f, \"threads\": %d, "
+         "\"sigma_mb\": %.8g, \"sigma_err_mb\": %.8g}\n",
+         tried, acc, sec, threads, sig, err);
+  return 0;
+}
+
+int main(int argc, char** argv)
+{
+  if (argc < 2) { fprintf(stderr, "usage: pythia_ref pdf|alphas|sigma|gen ...\n"); return 1; }
+  if (!strcmp(argv[1], "pdf")) return cmd_pdf(argc - 2, argv + 2);
+  if (!strcmp(argv[1], "alphas")) return cmd_alphas(argc - 2, argv + 2);
+  if (!strcmp(argv[1], "sigma") && argc > 2) return cmd_sigma(argv[2]);
+  if (!strcmp(argv[1], "gen") && argc > 4)
+    return cmd_gen(atol(argv[2]), atoi(argv[3]), atoi(argv[4]), argc > 5 ? atof(argv[5]) : 20.0,
+                   argc > 6 ? atof(argv[6]) : 0.13);
+  fprintf(stderr, "bad arguments\n");
+  return 1;
+}
