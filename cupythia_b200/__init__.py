@@ -1,0 +1,179 @@
+"""cupythia_b200 -- B200-native (sm_100a) batched QCD 2->2 hard-process Monte-Carlo integrator.
+
+Host-side mirror of the reference's interfaces for this path:
+  * :class:`Integrator` -- the stage-driver surface (fused partonic MC, VEGAS iterations,
+    unweighting, adjoint, flow), one CUDA handle of the C ABI (include/cupythia_b200.h);
+  * :mod:`cupythia_b200.sigma` -- Pythia's ``SigmaProcess`` surface (set2Kin / sigmaKin /
+    sigmaHat / sigmaPDF) over batches.
+Device buffers are torch CUDA tensors; torch is only the allocator here, every number is
+computed by the library's own kernels.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (CP_PROC_ALL, CP_PROC_GG2GG, CP_PROC_GG2QQBAR, CP_PROC_QG2QG,  # noqa: F401
+                   CP_PROC_QQ2QQ, CP_PROC_QQBAR2GG, CpError, cp_config, cp_event, cp_grad,
+                   cp_result)
+
+__all__ = ["Integrator", "CpError", "default_config", "CP_PROC_ALL"]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise CpError(_lib.CP_ERR_CUDA, "no CUDA device available")
+    return torch
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def default_config(**overrides):
+    lib = _lib.load()
+    cfg = cp_config()
+    lib.cp_config_default(C.byref(cfg))
+    for k, v in overrides.items():
+        if not hasattr(cfg, k):
+            raise KeyError(f"unknown config field {k}")
+        setattr(cfg, k, v)
+    return cfg
+
+
+class Integrator:
+    """One handle of the CUDA integrator (pp -> 2 jets at 13 TeV by default)."""
+
+    def __init__(self, **cfg):
+        self.lib = _lib.load()
+        self.cfg = default_config(**cfg)
+        h = C.c_void_p()
+        rc = self.lib.cp_create(C.byref(self.cfg), C.byref(h))
+        if rc != 0:
+            raise CpError(rc, "cp_create failed (no device, bad configuration or out of memory)")
+        self.h = h
+        self.nb = self.cfg.n_bins
+        self.device = f"cuda:{self.cfg.device}"
+
+    # ------------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.cp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        return _lib.check(self.lib, self.h, rc)
+
+    def set_stream(self, stream):
+        self._check(self.lib.cp_set_stream(self.h, C.c_void_p(stream)))
+
+    def sm_count(self):
+        n = C.c_int()
+        self._check(self.lib.cp_device_sm_count(self.h, C.byref(n)))
+        return n.value
+
+    # ------------------------------------------------------------------ RNG surface
+    def philox_words(self, seed, point0, n, iteration=0, stream=0):
+        torch = _torch()
+        out = torch.empty((n, 4), dtype=torch.int32, device=self.device)
+        self._check(self.lib.cp_philox_words(self.h, seed, point0, n, iteration, stream, _ptr(out)))
+        return out.cpu().numpy().view(np.uint32)
+
+    def splitmix_uniforms(self, seed, n_threads, k_per):
+        torch = _torch()
+        out = torch.empty(n_threads * k_per, dtype=torch.float64, device=self.device)
+        self._check(self.lib.cp_splitmix_uniforms(self.h, seed, n_threads, k_per, _ptr(out)))
+        return out.cpu().numpy()
+
+    def event_keys(self, base, e0, n):
+        torch = _torch()
+        out = torch.empty(n, dtype=torch.int64, device=self.device)
+        self._check(self.lib.cp_event_keys(self.h, base, e0, n, _ptr(out)))
+        return out.cpu().numpy().view(np.uint64)
+
+    # ------------------------------------------------------------------ PDFs
+    def pdf(self, x, q2):
+        """CTEQ5L x f for ids -5..-1, 1..5, 21 at (x, Q2); returns (n, 11) float32."""
+        torch = _torch()
+        x = torch.as_tensor(np.asarray(x, np.float32), device=self.device)
+        q2 = torch.as_tensor(np.asarray(q2, np.float32), device=self.device)
+        out = torch.empty((x.numel(), 11), dtype=torch.float32, device=self.device)
+        self._check(self.lib.cp_pdf_batch(self.h, _ptr(x), _ptr(q2), x.numel(), _ptr(out)))
+        return out.cpu().numpy()
+
+    # ------------------------------------------------------------------ VEGAS grid
+    @property
+    def grid(self):
+        e = (C.c_double * (3 * (self.nb + 1)))()
+        self._check(self.lib.cp_grid_get(self.h, e))
+        return np.array(e[:]).reshape(3, self.nb + 1)
+
+    @grid.setter
+    def grid(self, edges):
+        e = np.ascontiguousarray(np.asarray(edges, np.float64).reshape(-1))
+        self._check(self.lib.cp_grid_set(self.h, e.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def reset_grid(self):
+        self._check(self.lib.cp_grid_reset(self.h))
+
+    def iteration(self, n_points, iteration=0, alpha=1.5):
+        r = cp_result()
+        self._check(self.lib.cp_vegas_iteration(self.h, n_points, iteration, alpha, C.byref(r)))
+        return r.as_dict()
+
+    def integrate(self, n_iter, n_points, alpha=1.5, skip=0):
+        per = (cp_result * n_iter)()
+        comb = cp_result()
+        self._check(self.lib.cp_integrate(self.h, n_iter, n_points, alpha, skip, per, C.byref(comb)))
+        return [p.as_dict() for p in per], comb.as_dict()
+
+    def point_weights(self, point0, n, iteration=0, with_x=False):
+        torch = _torch()
+        w = torch.empty(n, dtype=torch.float32, device=self.device)
+        x = torch.empty((n, 3), dtype=torch.float32, device=self.device) if with_x else None
+        self._check(self.lib.cp_point_weights(self.h, point0, n, iteration, _ptr(w),
+                                              _ptr(x) if with_x else None))
+        return (w, x) if with_x else w
+
+    def weight_at(self, x):
+        torch = _torch()
+        x = torch.as_tensor(np.asarray(x, np.float32).reshape(-1, 3), device=self.device).contiguous()
+        w = torch.empty(x.shape[0], dtype=torch.float32, device=self.device)
+        self._check(self.lib.cp_weight_at(self.h, _ptr(x), x.shape[0], _ptr(w)))
+        return w
+
+    # ------------------------------------------------------------------ partonic gg -> gg
+    def partonic_integrate(self, n_points, sqrt_shat=100.0, alphas=0.13, cmax=0.9,
+                           conv=0.3893793721, seed=42):
+        r = cp_result()
+        self._check(self.lib.cp_partonic_integrate(self.h, sqrt_shat, alphas, cmax, conv, seed,
+                                                   n_points, C.byref(r)))
+        return r.as_dict()
+
+    def partonic_splitmix(self, n_threads, k_per, sqrt_shat=100.0, alphas=0.118, cmax=0.9,
+                          conv=0.3893793721, seed=0xABCDEF01):
+        r = cp_result()
+        self._check(self.lib.cp_partonic_splitmix(self.h, sqrt_shat, alphas, cmax, conv, seed,
+                                                  n_threads, k_per, C.byref(r)))
+        return r.as_dict()
+
+    def partonic_weights(self, point0, n, sqrt_shat=100.0, alphas=0.13, cmax=0.9,
+                         conv=0.3893793721, seed=42):
+        torch = _torch()
+        w = torch.empty(n, dtype=torch.float64, device=self.device)
+        self._check(self.lib.cp_partonic_weights(self.h, sqrt_shat, alphas, cmax, conv, seed,
+                                                 point0, n, _ptr(w)))
+        return w

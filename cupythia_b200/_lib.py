@@ -1,0 +1,138 @@
+"""ctypes binding of the C ABI declared in include/cupythia_b200.h.
+
+The product path is the CUDA library only: if ``libcupythia_b200.so`` cannot be loaded the
+import raises, there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("CUPYTHIA_B200_LIB") or os.path.join(HERE, "libcupythia_b200.so")
+
+CP_OK = 0
+CP_ERR_INVALID = 1
+CP_ERR_CUDA = 2
+CP_ERR_NUMERIC = 3
+CP_ERR_TIMEOUT = 4
+CP_ERR_CAPACITY = 5
+CP_ERR_NOMEM = 6
+
+CP_PROC_GG2GG = 1
+CP_PROC_GG2QQBAR = 2
+CP_PROC_QG2QG = 4
+CP_PROC_QQ2QQ = 8
+CP_PROC_QQBAR2GG = 16
+CP_PROC_ALL = 31
+CP_MAX_BINS = 128
+
+
+class cp_config(C.Structure):
+    _fields_ = [
+        ("sqrt_s", C.c_double), ("pt_hat_min", C.c_double), ("alphas_mz", C.c_double),
+        ("k_ren", C.c_double), ("k_fac", C.c_double), ("convert2mb", C.c_double),
+        ("n_quark_in", C.c_int), ("n_quark_new", C.c_int), ("proc_mask", C.c_int),
+        ("n_bins", C.c_int), ("device", C.c_int), ("reserved", C.c_int), ("seed", C.c_uint64),
+    ]
+
+
+class cp_result(C.Structure):
+    _fields_ = [
+        ("sigma", C.c_double), ("sigma_err", C.c_double), ("sum_w", C.c_double),
+        ("sum_w2", C.c_double), ("w_max", C.c_double), ("n_points", C.c_uint64),
+        ("n_bad", C.c_uint64), ("eta", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class cp_event(C.Structure):
+    _fields_ = [
+        ("id", C.c_int16 * 4), ("pz_in", C.c_float * 2), ("p3", C.c_float * 4),
+        ("p4", C.c_float * 4), ("weight", C.c_float), ("pt_hat", C.c_float),
+        ("process", C.c_uint32), ("point", C.c_uint32),
+    ]
+
+
+class cp_grad(C.Structure):
+    _fields_ = [
+        ("sigma", C.c_double), ("var", C.c_double), ("dsigma", C.c_double * 3),
+        ("dvar", C.c_double * 3), ("n_points", C.c_uint64), ("n_bad", C.c_uint64),
+    ]
+
+
+_P = C.c_void_p
+_u64 = C.c_uint64
+_u32 = C.c_uint32
+_i64 = C.c_int64
+_d = C.c_double
+_i = C.c_int
+
+# name -> argtypes; every function returns int status except where noted
+SIGNATURES = {
+    "cp_abi_version": [],
+    "cp_config_default": [C.POINTER(cp_config)],
+    "cp_create": [C.POINTER(cp_config), C.POINTER(_P)],
+    "cp_destroy": [_P],
+    "cp_set_stream": [_P, _P],
+    "cp_synchronize": [_P],
+    "cp_device_sm_count": [_P, C.POINTER(_i)],
+    "cp_philox_words": [_P, _u64, _u64, _u64, _u32, _u32, _P],
+    "cp_splitmix_uniforms": [_P, _u64, _u64, _u64, _P],
+    "cp_event_keys": [_P, _u64, _u64, _u64, _P],
+    "cp_set2kin_batch": [_P, _P, _P, _P, _P, _i64],
+    "cp_sigma_kin_batch": [_P, _i, _P],
+    "cp_sigma_hat_batch": [_P, _i, _i, _i, _P],
+    "cp_sigma_pdf_batch": [_P, _i, _P],
+    "cp_scales_batch": [_P, _P, _P, _P],
+    "cp_pdf_batch": [_P, _P, _P, _i64, _P],
+    "cp_grid_reset": [_P],
+    "cp_grid_set": [_P, C.POINTER(_d)],
+    "cp_grid_get": [_P, C.POINTER(_d)],
+    "cp_vegas_iteration": [_P, _u64, _u32, _d, C.POINTER(cp_result)],
+    "cp_integrate": [_P, _i, _u64, _d, _i, C.POINTER(cp_result), C.POINTER(cp_result)],
+    "cp_point_weights": [_P, _u64, _u64, _u32, _P, _P],
+    "cp_weight_at": [_P, _P, _i64, _P],
+    "cp_partonic_integrate": [_P, _d, _d, _d, _d, _u64, _u64, C.POINTER(cp_result)],
+    "cp_partonic_splitmix": [_P, _d, _d, _d, _d, _u64, _u64, _u64, C.POINTER(cp_result)],
+    "cp_partonic_weights": [_P, _d, _d, _d, _d, _u64, _u64, _u64, _P],
+}
+OPTIONAL = {}
+EXTRA_RESTYPES = {"cp_last_error": C.c_char_p}
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library (raises OSError when it is missing: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing; build it with `python -m cupythia_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, args in list(SIGNATURES.items()) + list(OPTIONAL.items()):
+        if not hasattr(lib, name):
+            if name in OPTIONAL:
+                continue
+            raise OSError(f"{LIB_PATH} does not export {name}")
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    lib.cp_last_error.argtypes = [_P]
+    lib.cp_last_error.restype = C.c_char_p
+    _lib = lib
+    return lib
+
+
+class CpError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cupythia_b200 error {code}: {msg}")
+        self.code = code
+
+
+def check(lib, handle, rc):
+    if rc != CP_OK:
+        msg = lib.cp_last_error(handle).decode() if handle else ""
+        raise CpError(rc, msg)
+    return rc

@@ -15,12 +15,15 @@
 // FP32 accurate to ~1e-6 relative:
 //   * 1 - z and 1 + z come from the complement of the zMax bound, 1 - zMax = r / (1 + zMax),
 //     r = pT^2_min / p^2 = tauMin / tau = exp(x0 ln tauMin), never from a rounded z;
-//   * ln x1 = -2 yMax (1 - v), ln x2 = -2 yMax v (v the rapidity variable), so x = exp(ln x)
-//     and 1 - x = -expm1(ln x) are both accurate and CTEQ5L's y = -ln x needs no log;
+//   * ln x1 = ln tau (1 - v), ln x2 = ln tau v (v the rapidity variable), so x = exp(ln x)
+//     and 1 - x = -expm1(ln x) are both accurate and CTEQ5L's y = -ln x needs no log; ln tau and
+//     ln x are carried as FP32 (hi, lo) pairs (error-free TwoSum / FMA products);
 //   * in CTEQ5L's exponent af0 (1-x) + af3 x + af1 y^p (1 + af8 u), whose O(100) terms cancel
 //     for the gluon, the constant parts are pre-combined in FP64 on the host:
 //       A = af0 + af1, B = af3 - af0, C = af1 af8, and y^p = 1 + expm1(p ln y), giving
-//       exponent = A + B x + C u + af1 expm1(p ln y) (1 + af8 u) + part3 + part4;
+//       exponent = A + B x + C u + af1 expm1(p ln y) (1 + af8 u) + part3 + part4,
+//     summed in FP32 with the products' FMA residuals and the additions' TwoSum errors
+//     carried in a second float, and exp(hi + lo) = exp(hi) (1 + lo);
 //   * matrix elements are written in tHat/sHat and uHat/sHat with all terms of one sign.
 #pragma once
 #include <stdint.h>
@@ -52,8 +55,10 @@ struct CpCteqPoly {
 
 struct CpHadParams {
   CpCteqPoly cteq[8];
-  float lnTauMin;     // ln(tauMin), tauMin = max(4 pTmin^2, mHatMin^2) / s
+  float lnTauMin;     // ln(tauMin), tauMin = 4 pTmin^2 / s
+  float lnTauMinLo;   // ln(tauMin) - lnTauMin (FP64 residual)
   float K0;           // 2 pi CONVERT2MB (-ln tauMin) / s : w = K0 alpha_s^2 B yMax zMax / tau
+  float conv;         // CONVERT2MB
   float s;            // sqrt(s)^2
   float kR, kF;       // muR^2 = kR pT^2, muF^2 = kF pT^2
   float lnL2[4];      // ln Lambda_nf^2, nf = 3, 4, 5, 6
@@ -117,18 +122,42 @@ CP_HD void cp_cteq_q(const CpHadParams& P, float Q2, CpCteqQ q[8])
   }
 }
 
-// Proton x f for one beam from ln x (<= 0): out = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.
-CP_HD void cp_cteq_x(const CpHadParams& P, const CpCteqQ q[8], float lnx, float out[8])
+// Error-free transformations on FP32 (Knuth TwoSum, FMA TwoProd) used to carry the few
+// quantities whose FP32 rounding would otherwise be amplified (ln tau, ln x, the CTEQ5L exponent).
+CP_HD void cp_twosum(float a, float b, float& s, float& e)
+{
+  s = a + b;
+  float bp = s - a;
+  e = (a - (s - bp)) + (b - bp);
+}
+// (s, c) += v, with the rounding error of the addition kept in c
+CP_HD void cp_acc2(float& s, float& c, float v)
+{
+  float t, e;
+  cp_twosum(s, v, t, e);
+  s = t;
+  c += e;
+}
+
+// Proton x f for one beam from ln x = lnx + lnxLo (<= 0, lnxLo a sub-ulp correction):
+// out = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.
+CP_HD void cp_cteq_x(const CpHadParams& P, const CpCteqQ q[8], float lnx, float lnxLo, float out[8])
 {
   // x clamp of PartonDistributions.cc:926
   const float lnxMin = -13.815510558f;   // ln 1e-6
-  if (lnx < lnxMin) lnx = lnxMin;
+  if (lnx < lnxMin) { lnx = lnxMin; lnxLo = 0.f; }
   float x = cp_expf(lnx);
   float omx = -cp_expm1f(lnx);           // 1 - x
-  if (omx < 1e-10f) { omx = 1e-10f; x = 1.f - 1e-10f; lnx = -1e-10f; }
-  float y = -lnx;
-  float lny = cp_logf(y);
-  float u = lnx + 11.512925465f;         // ln(x / 1e-5)
+  x = cp_fmaf(x, lnxLo, x);
+  omx = cp_fmaf(-x, lnxLo, omx);
+  if (omx < 1e-10f) { omx = 1e-10f; x = 1.f - 1e-10f; lnx = -1e-10f; lnxLo = 0.f; }
+  float y = -lnx;                        // y = -ln x, correction -lnxLo
+  float lny = cp_logf(y) - lnxLo / y;
+  // u = ln(x / 1e-5) = ln x + ln 1e5 as a (hi, lo) pair
+  const float LN1E5_HI = 11.512925148f, LN1E5_LO = 3.1696e-07f;
+  float uh, ul;
+  cp_twosum(lnx, LN1E5_HI, uh, ul);
+  ul += LN1E5_LO + lnxLo;
   float x1L = cp_logf(omx);
   float sumUbarDbar = 0.f;
 #pragma unroll
@@ -140,11 +169,26 @@ CP_HD void cp_cteq_x(const CpHadParams& P, const CpCteqQ q[8], float lnx, float 
     float al = cp_fmaf(a.p, lny, -ah);
     float ym1 = cp_expm1f(ah);
     ym1 = cp_fmaf(1.f + ym1, al, ym1);
-    float U = cp_fmaf(a.af8, u, 1.f);
+    float U = cp_fmaf(a.af8, uh, 1.f);
     float part3 = x * omx * (a.af5 + a.af6 * omx + a.af7 * x * omx);
     float L = c.useX1L ? x1L : cp_logf(omx + c.eut2);
-    float e = a.A + a.B * x + (a.af1 * a.af8) * u + a.af1 * ym1 * U + part3 + c.ut1 * x1L + a.af2 * L;
-    float answer = x * cp_expf(e) * a.qfac;
+    // exponent = A + B x + C u + af1 (y^p - 1) U + part3 + ut1 ln(1-x) + af2 L, C = af1 af8,
+    // summed with the product residuals and addition errors carried in a second float
+    float Ch = a.af1 * a.af8, Cl = cp_fmaf(a.af1, a.af8, -Ch);
+    float t3 = Ch * uh, t3l = cp_fmaf(Ch, uh, -t3) + Ch * ul + Cl * uh;
+    float qv = a.af1 * ym1;
+    float t4 = qv * U, t4l = cp_fmaf(qv, U, -t4);
+    float t2 = a.B * x, t2l = cp_fmaf(a.B, x, -t2);
+    float t6 = c.ut1 * x1L, t6l = cp_fmaf(c.ut1, x1L, -t6);
+    float t7 = a.af2 * L, t7l = cp_fmaf(a.af2, L, -t7);
+    float eh = a.A, el = (t2l + t3l) + (t4l + t6l + t7l);
+    cp_acc2(eh, el, t3);
+    cp_acc2(eh, el, t4);
+    cp_acc2(eh, el, t2);
+    cp_acc2(eh, el, part3);
+    cp_acc2(eh, el, t6);
+    cp_acc2(eh, el, t7);
+    float answer = x * cp_fmaf(cp_expf(eh), el, cp_expf(eh)) * a.qfac;
     if (i == 3) sumUbarDbar = x * answer;
     else if (i == 4) {
       float inv = 1.f / (1.f + answer);
@@ -188,7 +232,7 @@ CP_HD void cp_brackets(const CpHadParams& P, float tp, float up, CpBrackets& b)
   b.qqST = -(8.f / 27.f) * (up * up) * rt;
 }
 
-CP_HD float cp_channel_sum(const CpHadParams& P, const CpBrackets& b, const float A[8], const float Bq[8])
+CP_HD float cp_channel_sum(const float mask[5], const CpBrackets& b, const float A[8], const float Bq[8])
 {
   // flavour sums over q = +-1..+-5 (s, c, b enter twice: quark = antiquark)
   float QA = A[0] + A[1] + A[3] + A[4] + 2.f * (A[5] + A[6] + A[7]);
@@ -198,11 +242,11 @@ CP_HD float cp_channel_sum(const CpHadParams& P, const CpBrackets& b, const floa
   float Dopp = A[0] * Bq[4] + A[4] * Bq[0] + A[1] * Bq[3] + A[3] * Bq[1] +
                2.f * (A[5] * Bq[5] + A[6] * Bq[6] + A[7] * Bq[7]);
   float G = A[2] * Bq[2];
-  float sum = G * (P.mask[0] * b.gg2gg + P.mask[1] * b.gg2qqbar);
-  sum += P.mask[2] * b.qg2qg * (QA * Bq[2] + A[2] * QB);
+  float sum = G * (mask[0] * b.gg2gg + mask[1] * b.gg2qqbar);
+  sum += mask[2] * b.qg2qg * (QA * Bq[2] + A[2] * QB);
   // Sigma2qq2qq::sigmaHat: identical 1/2 (T + U + TU), q qbar T + ST, otherwise T
-  sum += P.mask[3] * (QA * QB * b.qqT + Dsame * (0.5f * (b.qqU + b.qqTU - b.qqT)) + Dopp * b.qqST);
-  sum += P.mask[4] * Dopp * b.qqbar2gg;
+  sum += mask[3] * (QA * QB * b.qqT + Dsame * (0.5f * (b.qqU + b.qqTU - b.qqT)) + Dopp * b.qqST);
+  sum += mask[4] * Dopp * b.qqbar2gg;
   return sum;
 }
 
@@ -215,9 +259,15 @@ struct CpKin {
 
 CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, CpKin* kin)
 {
-  float lnTau = (1.f - x0) * P.lnTauMin;
-  float tau = cp_expf(lnTau);
-  float invTau = cp_expf(-lnTau);
+  // ln tau = (1 - x0) ln tauMin as a (hi, lo) pair: both factors carry their rounding
+  float omx0, omx0l;
+  cp_twosum(1.f, -x0, omx0, omx0l);
+  float lnTau = omx0 * P.lnTauMin;
+  float lnTauL = cp_fmaf(omx0, P.lnTauMin, -lnTau) + omx0 * P.lnTauMinLo + omx0l * P.lnTauMin;
+  float eT = cp_expf(lnTau);
+  float tau = cp_fmaf(eT, lnTauL, eT);
+  float eI = cp_expf(-lnTau);
+  float invTau = cp_fmaf(-eI, lnTauL, eI);
   float yMax = -0.5f * lnTau;
   float r = cp_expf(x0 * P.lnTauMin);            // pT^2_min / p^2 = tauMin / tau
   float zMax = cp_sqrtf(-cp_expm1f(x0 * P.lnTauMin));   // sqrt(1 - r) without cancellation
@@ -227,17 +277,22 @@ CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, Cp
   float tp = -0.5f * omz, up = -0.5f * opz;
   float sH = tau * P.s;
   float pT2 = 0.25f * sH * omz * opz;
-  float lnx1 = -2.f * yMax * (1.f - x1);
-  float lnx2 = -2.f * yMax * x1;
+  // ln x1 = ln tau (1 - v), ln x2 = ln tau v, each as (hi, lo)
+  float omv, omvl;
+  cp_twosum(1.f, -x1, omv, omvl);
+  float lnx1 = lnTau * omv;
+  float lnx1L = cp_fmaf(lnTau, omv, -lnx1) + lnTauL * omv + lnTau * omvl;
+  float lnx2 = lnTau * x1;
+  float lnx2L = cp_fmaf(lnTau, x1, -lnx2) + lnTauL * x1;
   float alphaS = cp_alphas(P, P.kR * pT2);
   CpCteqQ q[8];
   cp_cteq_q(P, P.kF * pT2, q);
   float fa[8], fb[8];
-  cp_cteq_x(P, q, lnx1, fa);
-  cp_cteq_x(P, q, lnx2, fb);
+  cp_cteq_x(P, q, lnx1, lnx1L, fa);
+  cp_cteq_x(P, q, lnx2, lnx2L, fb);
   CpBrackets b;
   cp_brackets(P, tp, up, b);
-  float B = cp_channel_sum(P, b, fa, fb);
+  float B = cp_channel_sum(P.mask, b, fa, fb);
   if (kin) {
     kin->tau = tau; kin->yMax = yMax; kin->zMax = zMax; kin->sH = sH; kin->omz = omz;
     kin->opz = opz; kin->lnx1 = lnx1; kin->lnx2 = lnx2; kin->pT2 = pT2; kin->alphaS = alphaS;

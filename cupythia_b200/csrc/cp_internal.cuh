@@ -1,0 +1,165 @@
+// cp_internal.cuh -- handle layout, error plumbing and device helpers shared by the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include "../../include/cupythia_b200.h"
+#include "cp_params.h"
+
+#define CP_THREADS 256
+#ifndef CP_MIN_BLOCKS
+#define CP_MIN_BLOCKS 1   // resident blocks per SM the hot kernels are compiled for
+#endif
+#define CP_WARPS (CP_THREADS / 32)
+// per-block slot of the hadronic accumulation: sum w, sum w^2, max w, n_bad, then 3*nb hist
+#define CP_SLOT_HEAD 4
+
+// Per-iteration record written by the device refinement kernel (FP64).
+struct CpIterDev {
+  double sumw, sumw2, wmax, nbad, n, sigma, err, pad;
+};
+
+struct cp_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  cp_config cfg{};
+  CpHadParams P{};
+  int nb = 50;
+  // VEGAS grid, FP64
+  double* d_edges = nullptr;
+  // scratch: per-block slots and reduced outputs
+  double* d_slots = nullptr;
+  size_t slots_cap = 0;           // doubles
+  double* d_red = nullptr;        // CP_SLOT_HEAD + 3*CP_MAX_BINS doubles
+  CpIterDev* d_iters = nullptr;   // per-iteration records
+  int iters_cap = 0;
+  // SigmaProcess batch state (SoA FP32)
+  int64_t kin_n = 0, kin_cap = 0;
+  float *d_x1 = nullptr, *d_x2 = nullptr, *d_sH = nullptr, *d_tH = nullptr;
+  float *d_as = nullptr, *d_q2r = nullptr, *d_q2f = nullptr;
+  // launch shape of the persistent integrand kernels
+  int had_blocks = 0;
+  std::string err;
+};
+
+int cp_fail(cp_handle* h, int code, const std::string& msg);
+int cp_fail_cuda(cp_handle* h, cudaError_t e, const char* what);
+int cp_ensure_slots(cp_handle* h, size_t doubles);
+int cp_ensure_iters(cp_handle* h, int n);
+
+#define CP_CHECK_HANDLE(h) \
+  do { if (!(h)) return CP_ERR_INVALID; } while (0)
+#define CP_CUDA(h, call)                                        \
+  do {                                                          \
+    cudaError_t e_ = (call);                                    \
+    if (e_ != cudaSuccess) return cp_fail_cuda((h), e_, #call); \
+  } while (0)
+#define CP_LAUNCH_CHECK(h, what)                                \
+  do {                                                          \
+    cudaError_t e_ = cudaGetLastError();                        \
+    if (e_ != cudaSuccess) return cp_fail_cuda((h), e_, what);  \
+  } while (0)
+
+// ------------------------------------------------------------------------------------------
+// Device helpers
+// ------------------------------------------------------------------------------------------
+#if defined(__CUDACC__)
+
+// Kahan-compensated FP32 accumulation
+__device__ __forceinline__ void cp_kahan(float& s, float& c, float v)
+{
+  float y = v - c;
+  float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// Error-free sum (Knuth TwoSum): a + b = s + e exactly
+__device__ __forceinline__ void cp_two_sum(float a, float b, float& s, float& e)
+{
+  s = a + b;
+  float bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// Compensated warp reduction of (hi, lo) pairs; xor tree, deterministic. Result in all lanes.
+__device__ __forceinline__ void cp_warp_sum_comp(float& hi, float& lo)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    float oh = __shfl_xor_sync(0xffffffffu, hi, o);
+    float ol = __shfl_xor_sync(0xffffffffu, lo, o);
+    // order the pair so every lane adds the same two operands in the same order
+    int lane = threadIdx.x & 31;
+    float a = (lane & o) ? oh : hi, b = (lane & o) ? hi : oh;
+    float al = (lane & o) ? ol : lo, bl = (lane & o) ? lo : ol;
+    float s, e;
+    cp_two_sum(a, b, s, e);
+    hi = s;
+    lo = (al + bl) + e;
+  }
+}
+
+__device__ __forceinline__ double cp_warp_sum_d(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31;
+    v = (lane & o) ? (ov + v) : (v + ov);
+  }
+  return v;
+}
+
+__device__ __forceinline__ float cp_warp_max(float v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ double cp_warp_max_d(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Deterministic add of v into a warp-private histogram h[bin]: lanes that share a bin are
+// summed in lane order by the group's lowest lane, which alone writes.  Needs all 32 lanes.
+__device__ __forceinline__ void cp_warp_hist_add(float* h, int bin, float v)
+{
+  unsigned peers = __match_any_sync(0xffffffffu, bin);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(peers) - 1;
+  float sum = 0.f;
+  unsigned m = peers;
+  while (m) {
+    int l = __ffs(m) - 1;
+    sum += __shfl_sync(peers, v, l);
+    m &= m - 1;
+  }
+  if (lane == leader) h[bin] += sum;
+}
+
+// out[k] = sum over blocks of slots[b][k] (k != 2) or max (k == 2), fixed order, FP64.
+// One warp per output element.
+template <int UNUSED>
+__global__ void k_reduce_slots(const double* __restrict__ slots, int nblocks, int width, double* out)
+{
+  const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (k >= width) return;
+  double acc = 0.0;
+  if (k == 2) {
+    for (int b = lane; b < nblocks; b += 32) acc = fmax(acc, slots[(size_t)b * width + k]);
+    acc = cp_warp_max_d(acc);
+  } else {
+    for (int b = lane; b < nblocks; b += 32) acc += slots[(size_t)b * width + k];
+    acc = cp_warp_sum_d(acc);
+  }
+  if (lane == 0) out[k] = acc;
+}
+
+#endif

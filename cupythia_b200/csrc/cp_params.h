@@ -106,8 +106,10 @@ static inline int cp_build_had_params(const CpHadConfig& c, CpHadParams& P)
   double tauMin = 4.0 * c.pTmin * c.pTmin / s;
   double lnTauMin = log(tauMin);
   P.lnTauMin = (float)lnTauMin;
+  P.lnTauMinLo = (float)(lnTauMin - (double)P.lnTauMin);
   P.K0 = (float)(2.0 * M_PI * c.convert2mb * (-lnTauMin) / s);
   P.s = (float)s;
+  P.conv = (float)c.convert2mb;
   P.kR = (float)c.kR;
   P.kF = (float)c.kF;
   double L[4];

@@ -1,0 +1,304 @@
+// cp_vegas.cu -- the fused hadronic VEGAS iteration and its FP64 reduction / refinement.
+//
+// One persistent kernel per iteration: every thread draws its points' Philox words, maps them
+// through the VEGAS grid (edges staged in shared memory as FP32 (lo, width) pairs) and the
+// analytic (tau, y, z) base map, evaluates the FP32 integrand in registers, and accumulates
+//   sum w, sum w^2   Kahan-compensated FP32 per thread, compensated warp and block trees,
+//   max w, n_bad     per thread, then warp / block,
+//   sum w^2 per bin  warp-private shared-memory histograms, deterministic lane-order adds.
+// Each block writes one FP64 slot; a second kernel reduces the slots in a fixed order (FP64)
+// and a third refines the grid in FP64 on the device, so iterations chain on the stream
+// without host round trips (the reference round-trips through the host every iteration:
+// cuPythia/11_vegas_importance/vegas.cu:107-124).
+#include "cp_internal.cuh"
+
+struct HadLaunch {
+  uint64_t seed, point0, n;
+  uint32_t iter, stream;
+  int nb;
+  const double* edges;
+  double* slots;   // gridDim.x * (CP_SLOT_HEAD + 3 nb)
+  float* w_out;    // optional per-point weights
+  float* x_out;    // optional per-point mapped x (3 per point)
+};
+
+template <bool WRITE>
+__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const CpHadParams P, const HadLaunch L)
+{
+  __shared__ float2 sEdge[3][CP_MAX_BINS];
+  __shared__ float sHist[CP_WARPS][3][CP_MAX_BINS];
+  __shared__ float sRed[CP_WARPS][6];
+  const int nb = L.nb;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
+    int d = k / nb, b = k - d * nb;
+    const double* e = L.edges + d * (nb + 1);
+    double lo = e[b], hi = e[b + 1];
+    sEdge[d][b] = make_float2((float)lo, (float)(hi - lo));
+  }
+  for (int k = threadIdx.x; k < CP_WARPS * 3 * CP_MAX_BINS; k += CP_THREADS)
+    (&sHist[0][0][0])[k] = 0.f;
+  __syncthreads();
+
+  const float nbf = (float)nb;
+  const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
+  const uint64_t gtid = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x;
+  const uint64_t rounds = (L.n + stride - 1) / stride;
+  float s1 = 0.f, c1 = 0.f, s2 = 0.f, c2 = 0.f, wmax = 0.f;
+  uint32_t nbad = 0;
+  float* myHist = &sHist[warp][0][0];
+
+  for (uint64_t r = 0; r < rounds; ++r) {
+    const uint64_t p = r * stride + gtid;
+    const bool active = p < L.n;
+    float w = 0.f;
+    int bin[3] = {0, 0, 0};
+    if (active) {
+      uint32_t wd[4];
+      cp_point_words(L.seed, L.point0 + p, L.iter, L.stream, wd);
+      float x[3], jv = 1.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        float frac;
+        cp_bin_frac(wd[d], nb, bin[d], frac);
+        float2 e = sEdge[d][bin[d]];
+        x[d] = fmaf(frac, e.y, e.x);
+        jv *= nbf * e.y;
+      }
+      w = cp_had_weight(P, x[0], x[1], x[2], nullptr) * jv;
+      if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
+      cp_kahan(s1, c1, w);
+      cp_kahan(s2, c2, w * w);
+      wmax = fmaxf(wmax, w);
+      if (WRITE) {
+        if (L.w_out) L.w_out[p] = w;
+        if (L.x_out) { L.x_out[3 * p] = x[0]; L.x_out[3 * p + 1] = x[1]; L.x_out[3 * p + 2] = x[2]; }
+      }
+    }
+    const float w2 = w * w;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) cp_warp_hist_add(myHist + d * CP_MAX_BINS, bin[d], w2);
+  }
+
+  // compensated warp trees: Kahan sum s with compensation -c is the pair (s, -c)
+  float h1 = s1, l1 = -c1, h2 = s2, l2 = -c2;
+  cp_warp_sum_comp(h1, l1);
+  cp_warp_sum_comp(h2, l2);
+  float wm = cp_warp_max(wmax);
+  unsigned nb_w = __reduce_add_sync(0xffffffffu, nbad);
+  if (lane == 0) {
+    sRed[warp][0] = h1; sRed[warp][1] = l1; sRed[warp][2] = h2; sRed[warp][3] = l2;
+    sRed[warp][4] = wm; sRed[warp][5] = __uint_as_float(nb_w);
+  }
+  __syncthreads();
+  double* slot = L.slots + (size_t)blockIdx.x * (CP_SLOT_HEAD + 3 * nb);
+  if (threadIdx.x == 0) {
+    // block combine in warp order, FP32 compensated, then one FP64 store
+    float bh1 = 0.f, bl1 = 0.f, bh2 = 0.f, bl2 = 0.f, bm = 0.f;
+    unsigned bn = 0;
+    for (int k = 0; k < CP_WARPS; ++k) {
+      float s, e;
+      cp_two_sum(bh1, sRed[k][0], s, e); bh1 = s; bl1 += sRed[k][1] + e;
+      cp_two_sum(bh2, sRed[k][2], s, e); bh2 = s; bl2 += sRed[k][3] + e;
+      bm = fmaxf(bm, sRed[k][4]);
+      bn += __float_as_uint(sRed[k][5]);
+    }
+    slot[0] = (double)bh1 + (double)bl1;
+    slot[1] = (double)bh2 + (double)bl2;
+    slot[2] = (double)bm;
+    slot[3] = (double)bn;
+  }
+  for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
+    int d = k / nb, b = k - d * nb;
+    float s = 0.f;
+    for (int q = 0; q < CP_WARPS; ++q) s += sHist[q][d][b];
+    slot[CP_SLOT_HEAD + k] = (double)s;
+  }
+}
+
+// Iteration record and, if alpha > 0, Lepage's refinement of each dimension (FP64, one
+// thread per dimension): smooth (1,1)/(1,1,1)/(1,1), normalise, compress
+// r = ((d - 1) / ln d)^alpha, and rebin to equal shares of sum r.
+__global__ void k_refine(double* edges, const double* red, int nb, double n, double alpha,
+                         CpIterDev* rec)
+{
+  const int d = threadIdx.x;
+  if (d == 0 && rec) {
+    double sumw = red[0], sumw2 = red[1];
+    double mean = sumw / n;
+    double var = (sumw2 / n - mean * mean) / (n - 1.0);
+    rec->sumw = sumw; rec->sumw2 = sumw2; rec->wmax = red[2]; rec->nbad = red[3]; rec->n = n;
+    rec->sigma = mean; rec->err = sqrt(var > 0.0 ? var : 0.0);
+  }
+  if (!(alpha > 0.0) || d >= 3) return;
+  const double* h = red + CP_SLOT_HEAD + d * nb;
+  double* e = edges + d * (nb + 1);
+  double sm[CP_MAX_BINS], r[CP_MAX_BINS], ne[CP_MAX_BINS + 1];
+  double tot = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    double s;
+    if (i == 0) s = (h[0] + h[1]) / 2.0;
+    else if (i == nb - 1) s = (h[nb - 2] + h[nb - 1]) / 2.0;
+    else s = (h[i - 1] + h[i] + h[i + 1]) / 3.0;
+    sm[i] = s;
+    tot += s;
+  }
+  if (!(tot > 0.0)) return;
+  double rsum = 0.0;
+  for (int i = 0; i < nb; ++i) {
+    double di = sm[i] / tot, ri = 0.0;
+    if (di >= 1.0) ri = 1.0;
+    else if (di > 0.0) ri = pow((di - 1.0) / log(di), alpha);
+    r[i] = ri;
+    rsum += ri;
+  }
+  double step = rsum / (double)nb;
+  ne[0] = e[0];
+  ne[nb] = e[nb];
+  double acc = 0.0;
+  int j = 0;
+  for (int k = 1; k < nb; ++k) {
+    double need = step * (double)k;
+    while (j < nb - 1 && acc + r[j] < need) { acc += r[j]; ++j; }
+    double frac = r[j] > 0.0 ? (need - acc) / r[j] : 0.0;
+    frac = frac < 0.0 ? 0.0 : (frac > 1.0 ? 1.0 : frac);
+    ne[k] = e[j] + frac * (e[j + 1] - e[j]);
+  }
+  for (int k = 0; k <= nb; ++k) e[k] = ne[k];
+}
+
+// FP32 integrand at caller-supplied x
+__global__ void k_weight_at(const CpHadParams P, const float* __restrict__ x, int64_t n, float* w)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    w[i] = cp_had_weight(P, x[3 * i], x[3 * i + 1], x[3 * i + 2], nullptr);
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream,
+                      float* w_out, float* x_out)
+{
+  const int width = CP_SLOT_HEAD + 3 * h->nb;
+  int rc = cp_ensure_slots(h, (size_t)h->had_blocks * width);
+  if (rc) return rc;
+  HadLaunch L;
+  L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.stream = stream;
+  L.nb = h->nb; L.edges = h->d_edges; L.slots = h->d_slots; L.w_out = w_out; L.x_out = x_out;
+  if (w_out || x_out) k_had_accum<true><<<h->had_blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+  else k_had_accum<false><<<h->had_blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+  CP_LAUNCH_CHECK(h, "k_had_accum");
+  const int wpb = 8;
+  k_reduce_slots<0><<<(width + wpb - 1) / wpb, wpb * 32, 0, h->stream>>>(h->d_slots, h->had_blocks,
+                                                                        width, h->d_red);
+  CP_LAUNCH_CHECK(h, "k_reduce_slots");
+  return CP_OK;
+}
+
+static void fill_result(const CpIterDev& r, cp_result* out)
+{
+  out->sigma = r.sigma;
+  out->sigma_err = r.err;
+  out->sum_w = r.sumw;
+  out->sum_w2 = r.sumw2;
+  out->w_max = r.wmax;
+  out->n_points = (uint64_t)r.n;
+  out->n_bad = (uint64_t)r.nbad;
+  out->eta = r.wmax > 0 ? r.sigma / r.wmax : 0.0;
+}
+
+int cp_had_launch_shape(cp_handle* h)
+{
+  int per_sm = 0;
+  CP_CUDA(h, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_had_accum<false>, CP_THREADS, 0));
+  if (per_sm < 1) per_sm = 1;
+  h->had_blocks = h->num_sms * per_sm;
+  return CP_OK;
+}
+
+extern "C" int cp_vegas_iteration(cp_handle* h, uint64_t n_points, uint32_t iter, double alpha,
+                                  cp_result* out)
+{
+  CP_CHECK_HANDLE(h);
+  if (n_points < 2) return cp_fail(h, CP_ERR_INVALID, "cp_vegas_iteration: n_points < 2");
+  int rc = cp_ensure_iters(h, 1);
+  if (rc) return rc;
+  rc = had_launch(h, 0, n_points, iter, 0, nullptr, nullptr);
+  if (rc) return rc;
+  k_refine<<<1, 32, 0, h->stream>>>(h->d_edges, h->d_red, h->nb, (double)n_points, alpha, h->d_iters);
+  CP_LAUNCH_CHECK(h, "k_refine");
+  CpIterDev r;
+  CP_CUDA(h, cudaMemcpyAsync(&r, h->d_iters, sizeof r, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (out) fill_result(r, out);
+  if (r.nbad > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}
+
+extern "C" int cp_integrate(cp_handle* h, int n_iter, uint64_t n_points, double alpha, int skip,
+                            cp_result* per_iter, cp_result* combined)
+{
+  CP_CHECK_HANDLE(h);
+  if (n_iter < 1 || n_points < 2) return cp_fail(h, CP_ERR_INVALID, "cp_integrate: bad sizes");
+  int rc = cp_ensure_iters(h, n_iter);
+  if (rc) return rc;
+  for (int it = 0; it < n_iter; ++it) {
+    rc = had_launch(h, 0, n_points, (uint32_t)it, 0, nullptr, nullptr);
+    if (rc) return rc;
+    k_refine<<<1, 32, 0, h->stream>>>(h->d_edges, h->d_red, h->nb, (double)n_points, alpha,
+                                       h->d_iters + it);
+    CP_LAUNCH_CHECK(h, "k_refine");
+  }
+  CpIterDev* recs = new CpIterDev[n_iter];
+  cudaError_t e = cudaMemcpyAsync(recs, h->d_iters, sizeof(CpIterDev) * n_iter,
+                                  cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) { delete[] recs; return cp_fail_cuda(h, e, "cp_integrate readback"); }
+  double wsum = 0, w2 = 0, sw = 0, sw2 = 0, wmax = 0, nbad = 0, npts = 0;
+  for (int it = 0; it < n_iter; ++it) {
+    if (per_iter) fill_result(recs[it], per_iter + it);
+    nbad += recs[it].nbad;
+    if (it < skip) continue;
+    double err = recs[it].err;
+    if (err > 0) { wsum += recs[it].sigma / (err * err); w2 += 1.0 / (err * err); }
+    sw += recs[it].sumw; sw2 += recs[it].sumw2; npts += recs[it].n;
+    wmax = recs[it].wmax > wmax ? recs[it].wmax : wmax;
+  }
+  delete[] recs;
+  if (combined) {
+    combined->sigma = w2 > 0 ? wsum / w2 : 0;
+    combined->sigma_err = w2 > 0 ? 1.0 / sqrt(w2) : 0;
+    combined->sum_w = sw; combined->sum_w2 = sw2; combined->w_max = wmax;
+    combined->n_points = (uint64_t)npts; combined->n_bad = (uint64_t)nbad;
+    combined->eta = wmax > 0 ? combined->sigma / wmax : 0;
+  }
+  if (nbad > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}
+
+extern "C" int cp_point_weights(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter,
+                                float* w_dev, float* x_dev)
+{
+  CP_CHECK_HANDLE(h);
+  if (!w_dev && !x_dev) return cp_fail(h, CP_ERR_INVALID, "cp_point_weights: no output");
+  if (n == 0) return CP_OK;
+  int rc = had_launch(h, point0, n, iter, 0, w_dev, x_dev);
+  if (rc) return rc;
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}
+
+extern "C" int cp_weight_at(cp_handle* h, const float* x, int64_t n, float* w)
+{
+  CP_CHECK_HANDLE(h);
+  if (n < 0 || (n > 0 && (!x || !w))) return cp_fail(h, CP_ERR_INVALID, "cp_weight_at: bad args");
+  if (n == 0) return CP_OK;
+  int blocks = (int)((n + CP_THREADS - 1) / CP_THREADS);
+  if (blocks > h->num_sms * 16) blocks = h->num_sms * 16;
+  k_weight_at<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, x, n, w);
+  CP_LAUNCH_CHECK(h, "k_weight_at");
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}

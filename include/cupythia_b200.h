@@ -1,0 +1,178 @@
+/*
+ * cupythia_b200.h -- C ABI of the B200 (sm_100a) QCD 2->2 hard-process integrator.
+ *
+ * Plain pointers and sizes only.  "dev" pointers are CUDA device pointers on the handle's
+ * device; "host" pointers are ordinary host memory.  Every entry point returns CP_OK (0) or a
+ * nonzero CP_ERR_* code; cp_last_error() gives the message of the handle's last failure.
+ *
+ * Ownership: the caller owns every input and output buffer; the handle owns its scratch
+ * memory, its VEGAS grid and its flow weights.  Threading: one handle per host thread and
+ * device; all work of a handle is ordered on its CUDA stream (cp_set_stream).
+ *
+ * Each entry point names the reference interface it replaces (paths relative to the
+ * reference project root: cuPythia/ for the CUDA stages, pythia8317/ for Pythia).
+ */
+#ifndef CUPYTHIA_B200_H
+#define CUPYTHIA_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CP_ABI_VERSION 1
+
+/* status codes */
+#define CP_OK 0
+#define CP_ERR_INVALID 1  /* invalid argument or configuration                          */
+#define CP_ERR_CUDA 2     /* CUDA runtime error (message in cp_last_error)               */
+#define CP_ERR_NUMERIC 3  /* non-finite or negative weights were produced and zeroed     */
+#define CP_ERR_TIMEOUT 4  /* a bounded device-side wait expired                          */
+#define CP_ERR_CAPACITY 5 /* an output buffer was too small (count is still reported)   */
+#define CP_ERR_NOMEM 6    /* device allocation failed                                    */
+
+/* process switches (HardQCD:gg2gg ... of pythia8317/share/Pythia8/xmldoc/QCDHardProcesses.xml);
+ * Pythia process codes 111..115 (pythia8317/include/Pythia8/SigmaQCD.h:206,242,279,312,344) */
+#define CP_PROC_GG2GG 1
+#define CP_PROC_GG2QQBAR 2
+#define CP_PROC_QG2QG 4
+#define CP_PROC_QQ2QQ 8
+#define CP_PROC_QQBAR2GG 16
+#define CP_PROC_ALL 31
+
+#define CP_MAX_BINS 128   /* VEGAS bins per dimension */
+
+typedef struct cp_handle cp_handle;
+
+/* Physics and sampling configuration; field names follow the Pythia settings they mirror. */
+typedef struct cp_config {
+  double sqrt_s;       /* Beams:eCM, GeV                                   (13000)  */
+  double pt_hat_min;   /* PhaseSpace:pTHatMin, GeV                         (20)     */
+  double alphas_mz;    /* SigmaProcess:alphaSvalue, first-order running    (0.13)   */
+  double k_ren;        /* SigmaProcess:renormMultFac, muR^2 = k pT^2       (1)      */
+  double k_fac;        /* SigmaProcess:factorMultFac, muF^2 = k pT^2       (1)      */
+  double convert2mb;   /* GeV^-2 -> mb, SigmaProcess.cc:24                 (0.389380) */
+  int n_quark_in;      /* PDFinProcess:nQuarkIn (only 5 supported)         (5)      */
+  int n_quark_new;     /* HardQCD:nQuarkNew                                (3)      */
+  int proc_mask;       /* OR of CP_PROC_*                                  (ALL)    */
+  int n_bins;          /* VEGAS bins per dimension, <= CP_MAX_BINS         (50)     */
+  int device;          /* CUDA device ordinal                              (0)      */
+  int reserved;
+  uint64_t seed;       /* Philox key                                       (42)     */
+} cp_config;
+
+typedef struct cp_result {
+  double sigma;        /* estimate, mb                                              */
+  double sigma_err;    /* standard error, mb                                        */
+  double sum_w, sum_w2;
+  double w_max;
+  uint64_t n_points;
+  uint64_t n_bad;      /* non-finite / negative weights (zeroed)                    */
+  double eta;          /* <w> / w_max                                               */
+} cp_result;
+
+/* 64-byte unweighted event record: 2 incoming + 2 outgoing massless partons. */
+typedef struct cp_event {
+  int16_t id[4];       /* PDG ids: incoming a (+z), incoming b (-z), outgoing 3, 4  */
+  float pz_in[2];      /* incoming momenta along z, GeV (E = |pz|)                  */
+  float p3[4];         /* px, py, pz, E of outgoing 3, lab frame, GeV               */
+  float p4[4];         /* px, py, pz, E of outgoing 4                               */
+  float weight;        /* 1, or w / w_max for overweight events (> 1)               */
+  float pt_hat;        /* GeV                                                       */
+  uint32_t process;    /* Pythia process code 111..115                              */
+  uint32_t point;      /* low 32 bits of the point index that produced the event    */
+} cp_event;
+
+/* Gradient of the estimator (cp_adjoint). */
+typedef struct cp_grad {
+  double sigma, var;            /* estimator value and Var[w] of the batch           */
+  double dsigma[3], dvar[3];    /* d/d(alpha_s(mZ)), d/d(k_ren), d/d(pT_hat_min)     */
+  uint64_t n_points, n_bad;
+} cp_grad;
+
+/* ---------------------------------------------------------------- handles ---------- */
+int cp_abi_version(void);
+int cp_config_default(cp_config* cfg);
+/* replaces the per-stage cudaMalloc/setup of the cuPythia mains (e.g. 11_vegas_importance/vegas.cu:94-105) */
+int cp_create(const cp_config* cfg, cp_handle** out);
+int cp_destroy(cp_handle* h);
+const char* cp_last_error(const cp_handle* h);
+int cp_set_stream(cp_handle* h, void* cuda_stream);
+int cp_synchronize(cp_handle* h);
+int cp_device_sm_count(cp_handle* h, int* n_sm);
+
+/* ---------------------------------------------------------------- counter RNG ------ */
+/* Philox-4x32-10 words of points [point0, point0+n): key = seed, counter = (point, iter, stream);
+ * out (dev) holds 4n words.  Replaces the draw of cuPythia/common/rng.cuh:47-57 with the
+ * counter layout documented in the product's design notes. */
+int cp_philox_words(cp_handle* h, uint64_t seed, uint64_t point0, uint64_t n, uint32_t iter,
+                    uint32_t stream, uint32_t* out_dev);
+/* SplitMix64 uniforms in the reference's per-thread layout: out[t*k_per + i] =
+ * u01(splitmix64(seed + t*0x100000001B3 + i)) (cuPythia/03_fused_resident_me/fused_gg2gg.cu:43-46). */
+int cp_splitmix_uniforms(cp_handle* h, uint64_t seed, uint64_t n_threads, uint64_t k_per,
+                         double* out_dev);
+/* per-event keys splitmix64(base ^ e*0x9E3779B97F4A7C15), e in [e0, e0+n)
+ * (cuPythia/05_reproducible_events/repro_events.cu:43, cuPythia/pipeline/generate.cu:33) */
+int cp_event_keys(cp_handle* h, uint64_t base, uint64_t e0, uint64_t n, uint64_t* out_dev);
+
+/* ---------------------------------------------------------------- SigmaProcess ----- */
+/* Batched Sigma2Process::set2Kin (pythia8317/include/Pythia8/SigmaProcess.h:118,498-501 ->
+ * store2Kin, pythia8317/src/SigmaProcess.cc:846-925; massless): stores the batch and its
+ * uHat, pT^2, Q2Ren, Q2Fac and alpha_s.  Inputs are dev SoA arrays of n points. */
+int cp_set2kin_batch(cp_handle* h, const float* x1, const float* x2, const float* sH,
+                     const float* tH, int64_t n);
+/* Batched sigmaKin + sigmaHat of the flavour-independent processes 111, 112, 113, 115
+ * (pythia8317/src/SigmaQCD.cc:115-325): dsigmaHat/dtHat in GeV^-4, one value per point. */
+int cp_sigma_kin_batch(cp_handle* h, int process_code, float* out_dev);
+/* Batched sigmaHat(id1, id2) (SigmaProcess.h:139; Sigma2qq2qq::sigmaHat SigmaQCD.cc:272-286). */
+int cp_sigma_hat_batch(cp_handle* h, int process_code, int id1, int id2, float* out_dev);
+/* Batched sigmaPDF() (pythia8317/src/SigmaProcess.cc:423-480) summed over the processes of
+ * proc_mask: sum over pairs of CONVERT2MB sigmaHat xf_a(x1) xf_b(x2), mb GeV^-2. */
+int cp_sigma_pdf_batch(cp_handle* h, int proc_mask, float* out_dev);
+/* Accessors alphaSRen(), Q2Ren(), Q2Fac() of the stored batch (SigmaProcess.h:254-257). */
+int cp_scales_batch(cp_handle* h, float* alphas_dev, float* q2ren_dev, float* q2fac_dev);
+/* CTEQ5L x f(id, x, Q2) of a proton (PDF::xf, pythia8317/src/PartonDistributions.cc:122-180):
+ * out (dev) is n x 11 in id order -5..-1, 1..5, 21. */
+int cp_pdf_batch(cp_handle* h, const float* x_dev, const float* q2_dev, int64_t n, float* out_dev);
+
+/* ---------------------------------------------------------------- VEGAS ------------ */
+/* Grid: 3 dimensions (tau, y, cos theta) x (n_bins + 1) edges in [0, 1], FP64. */
+int cp_grid_reset(cp_handle* h);
+int cp_grid_set(cp_handle* h, const double* edges_host);
+int cp_grid_get(cp_handle* h, double* edges_host);
+/* One VEGAS iteration of n_points points (Philox stream 0, counter iteration = iter):
+ * fused draw -> map -> integrand -> Kahan block sums -> FP64 slot reduction -> per-bin w^2
+ * histograms, then, if alpha > 0, the FP64 grid refinement on the device.  Replaces the
+ * iteration body of cuPythia/11_vegas_importance/vegas.cu:107-124 (3-D, hadronic). */
+int cp_vegas_iteration(cp_handle* h, uint64_t n_points, uint32_t iter, double alpha,
+                       cp_result* out_host);
+/* n_iter iterations back to back on the device, one host read at the end; per_iter (host,
+ * n_iter entries, may be NULL) and the inverse-variance combination of the iterations with
+ * index >= skip. */
+int cp_integrate(cp_handle* h, int n_iter, uint64_t n_points, double alpha, int skip,
+                 cp_result* per_iter_host, cp_result* combined_host);
+/* Per-point weights (dev) of points [point0, point0+n) of iteration iter on the current grid,
+ * and optionally the mapped x (dev, 3n floats) the integrand was evaluated at. */
+int cp_point_weights(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, float* w_dev,
+                     float* x_dev);
+/* FP32 integrand at caller-given x in [0,1]^3 (dev, 3n floats): f * J_base, mb. */
+int cp_weight_at(cp_handle* h, const float* x_dev, int64_t n, float* w_dev);
+
+/* ---------------------------------------------------------------- partonic gg->gg --- */
+/* Fused resident gg->gg MC in FP64 (cuPythia/03_fused_resident_me/fused_gg2gg.cu:40-51):
+ * cos theta = (2u-1) cMax, u from Philox (point i: counter (i, 0, 0, 0), 53-bit uniform of
+ * words 0,1); sigma = <w>, w = dsigma/dtHat (2 cMax)(s/2) conv. */
+int cp_partonic_integrate(cp_handle* h, double sqrt_shat, double alphas, double cmax,
+                          double conv, uint64_t seed, uint64_t n_points, cp_result* out_host);
+/* Same integrand on the reference's SplitMix64 per-thread streams (n_threads x k_per draws). */
+int cp_partonic_splitmix(cp_handle* h, double sqrt_shat, double alphas, double cmax,
+                         double conv, uint64_t seed, uint64_t n_threads, uint64_t k_per,
+                         cp_result* out_host);
+/* Per-point FP64 weights of the Philox form, points [point0, point0+n). */
+int cp_partonic_weights(cp_handle* h, double sqrt_shat, double alphas, double cmax, double conv,
+                        uint64_t seed, uint64_t point0, uint64_t n, double* w_dev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -593,3 +593,39 @@ void cpo_had_adjoint_sums(const cpo_had_cfg* c, const double* edges, int nb, uin
 /* ======================= unweighting ======================= */
 /* von Neumann accept, cuPythia/07_unweighting_lhe/unweight_lhe.cu:54: accept if u wMax < w */
 int cpo_accept(double w, double wmax, uint32_t w3) { return cpo_u24(w3) * wmax < w; }
+
+/* ======================= batch helpers for the parity tests ======================= */
+typedef struct {
+  const cpo_had_cfg* c;
+  const float* x;
+  double* out;
+  int64_t i0, i1;
+} wx_job;
+
+static void* wx_thread(void* arg)
+{
+  wx_job* j = (wx_job*)arg;
+  for (int64_t i = j->i0; i < j->i1; ++i) {
+    double x[3] = {j->x[3 * i], j->x[3 * i + 1], j->x[3 * i + 2]};
+    j->out[i] = cpo_had_weight_x(j->c, x, NULL);
+  }
+  return NULL;
+}
+
+void cpo_had_weight_x_batch(const cpo_had_cfg* c, const float* x, int64_t n, double* out, int nthreads)
+{
+  nthreads = clamp_threads(nthreads, (uint64_t)n);
+  wx_job* jobs = (wx_job*)calloc((size_t)nthreads, sizeof(wx_job));
+  pthread_t* th = (pthread_t*)calloc((size_t)nthreads, sizeof(pthread_t));
+  int64_t per = n / nthreads, rem = n % nthreads, off = 0;
+  for (int t = 0; t < nthreads; ++t) {
+    jobs[t].c = c; jobs[t].x = x; jobs[t].out = out;
+    jobs[t].i0 = off; off += per + (t < rem ? 1 : 0); jobs[t].i1 = off;
+    if (nthreads > 1) pthread_create(&th[t], NULL, wx_thread, &jobs[t]);
+    else wx_thread(&jobs[t]);
+  }
+  if (nthreads > 1)
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  free(jobs);
+  free(th);
+}

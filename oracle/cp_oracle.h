@@ -136,6 +136,9 @@ void cpo_had_adjoint_sums(const cpo_had_cfg* c, const double* edges, int nb, uin
                           uint32_t iter, uint32_t stream, uint64_t p0, uint64_t n, double* g,
                           int nthreads);
 
+/* f * J_base at n points x (3n floats, as doubles), multi-threaded */
+void cpo_had_weight_x_batch(const cpo_had_cfg* c, const float* x, int64_t n, double* out, int nthreads);
+
 /* ---------------- unweighting ---------------- */
 /* Accept draw of a point: word 3 of its Philox block, as u24. */
 int cpo_accept(double w, double wmax, uint32_t w3);

@@ -19,7 +19,7 @@ int probe_pdf(double aSmZ, float lnx, float Q2, float* out8)
   if (cp_build_had_params(c, P)) return 1;
   CpCteqQ q[8];
   cp_cteq_q(P, Q2, q);
-  cp_cteq_x(P, q, lnx, out8);
+  cp_cteq_x(P, q, lnx, 0.f, out8);
   return 0;
 }
 void probe_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t* out)

@@ -1,0 +1,60 @@
+"""The FP32 integrand of the CUDA kernels (cupythia_b200/csrc/cp_integrand.cuh), compiled for the
+host, against the FP64 oracle: the FP32 formulation alone must hold 1e-5 relative per point."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+REL_TOL = 1e-5      # per-point weight tolerance in FP32
+TINY = 1e-12        # weights below TINY * mean underflow FP32 and carry no cross section
+
+
+@pytest.fixture(scope="module")
+def probe(tmp_path_factory):
+    so = str(tmp_path_factory.mktemp("probe") / "fp32_probe.so")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", os.path.join(HERE, "fp32_probe.cc"),
+                    "-o", so], check=True)
+    return C.CDLL(so)
+
+
+def _weights(probe, x, **kw):
+    out = np.zeros(len(x), np.float32)
+    args = dict(sqrtS=13000., pTmin=20., aSmZ=.13, kR=1., kF=1., conv=.389380)
+    args.update(kw)
+    rc = probe.probe_had_weights(*[C.c_double(args[k]) for k in ("sqrtS", "pTmin", "aSmZ", "kR", "kF", "conv")],
+                                 31, x.ctypes.data_as(C.c_void_p), len(x), out.ctypes.data_as(C.c_void_p))
+    assert rc == 0
+    return out
+
+
+@pytest.mark.parametrize("pTmin,aSmZ,kR", [(20., .13, 1.), (10., .11, .5), (50., .14, 2.)])
+def test_fp32_weights_within_tolerance(probe, orc, pTmin, aSmZ, kR):
+    rng = np.random.default_rng(7)
+    n = 40000
+    x = rng.random((n, 3)).astype(np.float32)
+    # edges of the cube, where the poles and the PDF endpoints sit
+    x[:2000, 2] = (1 - rng.random(2000) * 1e-4).astype(np.float32)
+    x[2000:4000, 2] = (rng.random(2000) * 1e-4).astype(np.float32)
+    x[4000:6000, 1] = (1 - rng.random(2000) * 1e-4).astype(np.float32)
+    x[6000:8000, 0] = (rng.random(2000) * 1e-4).astype(np.float32)
+    got = _weights(probe, x, pTmin=pTmin, aSmZ=aSmZ, kR=kR)
+    ref = orc.weight_x_batch(orc.had_cfg(pTmin=pTmin, aSmZ=aSmZ, kR=kR), x)
+    keep = ref > TINY * ref.mean()
+    rel = np.abs(got[keep] - ref[keep]) / ref[keep]
+    assert rel.max() < REL_TOL, (rel.max(), np.percentile(rel, 99))
+    assert np.all(np.isfinite(got))
+
+
+def test_probe_philox_matches_oracle(probe, orc):
+    out = (C.c_uint32 * 4)()
+    rng = np.random.default_rng(1)
+    for _ in range(100):
+        c = [int(v) for v in rng.integers(0, 2 ** 32, 6)]
+        probe.probe_philox(*[C.c_uint32(v) for v in c], out)
+        ref = (C.c_uint32 * 4)()
+        orc.lib().cpo_philox4x32_10((C.c_uint32 * 4)(*c[:4]), (C.c_uint32 * 2)(*c[4:]), ref)
+        assert list(out) == list(ref)
