@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from ._lib import (CP_PROC_ALL, CP_PROC_GG2GG, CP_PROC_GG2QQBAR, CP_PROC_QG2QG,  # noqa: F401
                    CP_PROC_QQ2QQ, CP_PROC_QQBAR2GG, CpError, cp_config, cp_event, cp_grad,
-                   cp_result)
+                   cp_result, cp_unweight_result)
 
 __all__ = ["Integrator", "CpError", "default_config", "CP_PROC_ALL"]
 
@@ -79,6 +79,12 @@ class Integrator:
 
     def set_stream(self, stream):
         self._check(self.lib.cp_set_stream(self.h, C.c_void_p(stream)))
+
+    def measure_peaks(self):
+        """(FP32 TFLOP/s, MUFU Tops/s) of the device from the library's microbenchmarks."""
+        f, m = C.c_double(), C.c_double()
+        self._check(self.lib.cp_measure_peaks(self.h, C.byref(f), C.byref(m)))
+        return f.value, m.value
 
     def sm_count(self):
         n = C.c_int()
@@ -155,6 +161,42 @@ class Integrator:
         self._check(self.lib.cp_weight_at(self.h, _ptr(x), x.shape[0], _ptr(w)))
         return w
 
+    def last_histogram(self):
+        out = (C.c_double * (4 + 3 * self.nb))()
+        self._check(self.lib.cp_last_histogram(self.h, out))
+        a = np.array(out[:])
+        return {"sum_w": a[0], "sum_w2": a[1], "w_max": a[2], "n_bad": a[3],
+                "hist": a[4:].reshape(3, self.nb)}
+
+    # ------------------------------------------------------------------ unweighting
+    def weight_quantile(self, q=0.999):
+        v = C.c_double()
+        self._check(self.lib.cp_weight_quantile(self.h, q, C.byref(v)))
+        return v.value
+
+    def set_wmax(self, w_max):
+        self._check(self.lib.cp_set_wmax(self.h, w_max))
+
+    def unweight(self, n_points, iteration=0, capacity=None, records=None):
+        """Production pass into a device buffer; returns (records tensor [n_acc, 64] uint8, stats)."""
+        torch = _torch()
+        if records is None:
+            capacity = capacity if capacity is not None else n_points
+            records = torch.empty((capacity, 64), dtype=torch.uint8, device=self.device)
+        capacity = records.shape[0]
+        r = cp_unweight_result()
+        rc = self.lib.cp_unweight(self.h, n_points, iteration, _ptr(records), capacity, C.byref(r))
+        self._check(rc)
+        return records[:min(r.n_accepted, capacity)], r.as_dict()
+
+    def generate_host(self, n_points, records_host, iteration=0, chunk=1 << 24):
+        """Production pass into a host uint8 tensor/array of shape [capacity, 64]."""
+        r = cp_unweight_result()
+        ptr = records_host.data_ptr() if hasattr(records_host, "data_ptr") else records_host.ctypes.data
+        self._check(self.lib.cp_generate_host(self.h, n_points, iteration, chunk, C.c_void_p(ptr),
+                                              records_host.shape[0], C.byref(r)))
+        return r.as_dict()
+
     # ------------------------------------------------------------------ partonic gg -> gg
     def partonic_integrate(self, n_points, sqrt_shat=100.0, alphas=0.13, cmax=0.9,
                            conv=0.3893793721, seed=42):
@@ -177,3 +219,13 @@ class Integrator:
         self._check(self.lib.cp_partonic_weights(self.h, sqrt_shat, alphas, cmax, conv, seed,
                                                  point0, n, _ptr(w)))
         return w
+
+
+EVENT_DTYPE = np.dtype([("id", "<i2", 4), ("pz_in", "<f4", 2), ("p3", "<f4", 4), ("p4", "<f4", 4),
+                        ("weight", "<f4"), ("pt_hat", "<f4"), ("process", "<u4"), ("point", "<u4")])
+
+
+def events_view(records):
+    """Structured numpy view (cp_event layout) of a [n, 64] uint8 record array or tensor."""
+    a = records.cpu().numpy() if hasattr(records, "cpu") else np.asarray(records)
+    return np.ascontiguousarray(a).view(EVENT_DTYPE).reshape(-1)

@@ -54,6 +54,18 @@ class cp_event(C.Structure):
     ]
 
 
+class cp_unweight_result(C.Structure):
+    _fields_ = [
+        ("sigma", C.c_double), ("sigma_err", C.c_double), ("sigma_unweighted", C.c_double),
+        ("w_max", C.c_double), ("w_max_seen", C.c_double), ("eta", C.c_double),
+        ("n_points", C.c_uint64), ("n_accepted", C.c_uint64), ("n_overweight", C.c_uint64),
+        ("n_bad", C.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class cp_grad(C.Structure):
     _fields_ = [
         ("sigma", C.c_double), ("var", C.c_double), ("dsigma", C.c_double * 3),
@@ -93,6 +105,12 @@ SIGNATURES = {
     "cp_integrate": [_P, _i, _u64, _d, _i, C.POINTER(cp_result), C.POINTER(cp_result)],
     "cp_point_weights": [_P, _u64, _u64, _u32, _P, _P],
     "cp_weight_at": [_P, _P, _i64, _P],
+    "cp_last_histogram": [_P, C.POINTER(_d)],
+    "cp_weight_quantile": [_P, _d, C.POINTER(_d)],
+    "cp_set_wmax": [_P, _d],
+    "cp_unweight": [_P, _u64, _u32, _P, _u64, C.POINTER(cp_unweight_result)],
+    "cp_generate_host": [_P, _u64, _u32, _u64, _P, _u64, C.POINTER(cp_unweight_result)],
+    "cp_measure_peaks": [_P, C.POINTER(_d), C.POINTER(_d)],
     "cp_partonic_integrate": [_P, _d, _d, _d, _d, _u64, _u64, C.POINTER(cp_result)],
     "cp_partonic_splitmix": [_P, _d, _d, _d, _d, _u64, _u64, _u64, C.POINTER(cp_result)],
     "cp_partonic_weights": [_P, _d, _d, _d, _d, _u64, _u64, _u64, _P],

@@ -119,7 +119,11 @@ extern "C" int cp_create(const cp_config* cfg, cp_handle** out)
   if (cudaSetDevice(h->device) != cudaSuccess) { delete h; return CP_ERR_CUDA; }
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
   bool ok = cudaMalloc(&h->d_edges, sizeof(double) * 3 * (CP_MAX_BINS + 1)) == cudaSuccess &&
-            cudaMalloc(&h->d_red, sizeof(double) * (CP_SLOT_HEAD + 3 * CP_MAX_BINS)) == cudaSuccess;
+            cudaMalloc(&h->d_red, sizeof(double) * (CP_SLOT_HEAD + 3 * CP_MAX_BINS)) == cudaSuccess &&
+            cudaMalloc(&h->d_qhist, sizeof(unsigned long long) * CP_QBINS) == cudaSuccess &&
+            cudaMalloc(&h->d_wmax, sizeof(double) * 2) == cudaSuccess &&
+            cudaMalloc(&h->d_counter, sizeof(unsigned long long) * 2) == cudaSuccess &&
+            cudaMemset(h->d_wmax, 0, sizeof(double) * 2) == cudaSuccess;
   if (!ok || cp_had_launch_shape(h) != CP_OK || cp_ensure_iters(h, 16) != CP_OK) {
     cp_destroy(h);
     return CP_ERR_NOMEM;
@@ -136,7 +140,7 @@ extern "C" int cp_destroy(cp_handle* h)
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
-                  h->d_tH, h->d_as, h->d_q2r, h->d_q2f};
+                  h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete h;

@@ -252,12 +252,21 @@ CP_HD float cp_channel_sum(const float mask[5], const CpBrackets& b, const float
 
 // ------------------------------------------------------------------------------------------
 // Weight f * J_base of a point x in [0,1]^3 (x0 -> tau, x1 -> y, x2 -> z), in mb.
+// cp_had_eval keeps the pieces the event record needs (PDFs, brackets, kinematics); kernels
+// that only need w call cp_had_weight and the compiler drops the rest.
 // ------------------------------------------------------------------------------------------
 struct CpKin {
   float tau, yMax, zMax, sH, omz, opz, lnx1, lnx2, pT2, alphaS;
 };
 
-CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, CpKin* kin)
+struct CpPoint {
+  CpKin k;
+  CpBrackets b;
+  float fa[8], fb[8];
+  float scale;   // K0 alpha_s^2 yMax zMax / tau: w = scale * channel sum
+};
+
+CP_HD float cp_had_eval(const CpHadParams& P, float x0, float x1, float x2, CpPoint& pt)
 {
   // ln tau = (1 - x0) ln tauMin as a (hi, lo) pair: both factors carry their rounding
   float omx0, omx0l;
@@ -287,18 +296,22 @@ CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, Cp
   float alphaS = cp_alphas(P, P.kR * pT2);
   CpCteqQ q[8];
   cp_cteq_q(P, P.kF * pT2, q);
-  float fa[8], fb[8];
-  cp_cteq_x(P, q, lnx1, lnx1L, fa);
-  cp_cteq_x(P, q, lnx2, lnx2L, fb);
-  CpBrackets b;
-  cp_brackets(P, tp, up, b);
-  float B = cp_channel_sum(P.mask, b, fa, fb);
-  if (kin) {
-    kin->tau = tau; kin->yMax = yMax; kin->zMax = zMax; kin->sH = sH; kin->omz = omz;
-    kin->opz = opz; kin->lnx1 = lnx1; kin->lnx2 = lnx2; kin->pT2 = pT2; kin->alphaS = alphaS;
-  }
-  if (!(zMax > 0.f)) return 0.f;
-  return P.K0 * (alphaS * alphaS) * B * yMax * zMax * invTau;
+  cp_cteq_x(P, q, lnx1, lnx1L, pt.fa);
+  cp_cteq_x(P, q, lnx2, lnx2L, pt.fb);
+  cp_brackets(P, tp, up, pt.b);
+  float B = cp_channel_sum(P.mask, pt.b, pt.fa, pt.fb);
+  pt.k.tau = tau; pt.k.yMax = yMax; pt.k.zMax = zMax; pt.k.sH = sH; pt.k.omz = omz;
+  pt.k.opz = opz; pt.k.lnx1 = lnx1; pt.k.lnx2 = lnx2; pt.k.pT2 = pT2; pt.k.alphaS = alphaS;
+  pt.scale = (zMax > 0.f) ? P.K0 * (alphaS * alphaS) * yMax * zMax * invTau : 0.f;
+  return pt.scale * B;
+}
+
+CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, CpKin* kin)
+{
+  CpPoint pt;
+  float w = cp_had_eval(P, x0, x1, x2, pt);
+  if (kin) *kin = pt.k;
+  return w;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -341,4 +354,172 @@ CP_HD void cp_bin_frac(uint32_t w, int nb, int& bin, float& frac)
   uint32_t m = (w >> 8) * (uint32_t)nb;      // < 2^24 * nb <= 2^31 for nb <= 128
   bin = (int)(m >> 24);
   frac = (float)(m & 0xFFFFFFu) * (1.f / 16777216.f);
+}
+
+// ------------------------------------------------------------------------------------------
+// Unweighted event record (the 64-byte cp_event of the C ABI).
+// Flavour choice follows SigmaProcess::pickInState (pythia8317/src/SigmaProcess.cc:486-508):
+// a process with probability proportional to its share of the channel sum, then an incoming
+// pair in initFlux order (SigmaProcess.cc:124-193) with probability proportional to its
+// pdfSigma; outgoing flavours follow each process's setIdColAcol (SigmaQCD.cc:135-342):
+// gg -> gg and q qbar -> g g give 21 21, gg -> q qbar gives q = 1 + int(nQuarkNew u), q qbar,
+// qg -> qg and qq -> qq keep the incoming flavours.
+// ------------------------------------------------------------------------------------------
+struct CpEventRec {
+  int16_t id[4];
+  float pz_in[2];
+  float p3[4];
+  float p4[4];
+  float weight;
+  float pt_hat;
+  uint32_t process;
+  uint32_t point;
+};
+
+// x f(id) from the raw array {d, u, g, ubar, dbar, s, c, b}
+CP_HD float cp_xf_id(const float f[8], int id)
+{
+  switch (id) {
+    case 1: return f[0];
+    case 2: return f[1];
+    case -1: return f[4];
+    case -2: return f[3];
+    case 3: case -3: return f[5];
+    case 4: case -4: return f[6];
+    case 5: case -5: return f[7];
+    default: return f[2];
+  }
+}
+
+CP_HD float cp_qq_pair_bracket(const CpBrackets& b, int id1, int id2)
+{
+  if (id2 == id1) return 0.5f * (b.qqT + b.qqU + b.qqTU);
+  if (id2 == -id1) return b.qqT + b.qqST;
+  return b.qqT;
+}
+
+// Process shares at one point: {gg2gg, gg2qqbar, qg2qg, qq2qq, qqbar2gg}
+CP_HD void cp_process_shares(const float mask[5], const CpBrackets& b, const float* A, const float* Bq, float c[5])
+{
+  float QA = A[0] + A[1] + A[3] + A[4] + 2.f * (A[5] + A[6] + A[7]);
+  float QB = Bq[0] + Bq[1] + Bq[3] + Bq[4] + 2.f * (Bq[5] + Bq[6] + Bq[7]);
+  float Dsame = A[0] * Bq[0] + A[1] * Bq[1] + A[3] * Bq[3] + A[4] * Bq[4] +
+                2.f * (A[5] * Bq[5] + A[6] * Bq[6] + A[7] * Bq[7]);
+  float Dopp = A[0] * Bq[4] + A[4] * Bq[0] + A[1] * Bq[3] + A[3] * Bq[1] +
+               2.f * (A[5] * Bq[5] + A[6] * Bq[6] + A[7] * Bq[7]);
+  float G = A[2] * Bq[2];
+  c[0] = mask[0] * G * b.gg2gg;
+  c[1] = mask[1] * G * b.gg2qqbar;
+  c[2] = mask[2] * b.qg2qg * (QA * Bq[2] + A[2] * QB);
+  c[3] = mask[3] * (QA * QB * b.qqT + Dsame * (0.5f * (b.qqU + b.qqTU - b.qqT)) + Dopp * b.qqST);
+  c[4] = mask[4] * Dopp * b.qqbar2gg;
+}
+
+// Picks (process, id1, id2, id3, id4) from uniforms r0 (process), r1 (pair), r3 (new flavour).
+CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, float r1, float r3,
+                            int& code, int id[4])
+{
+  float c[5];
+  cp_process_shares(P.mask, pt.b, pt.fa, pt.fb, c);
+  float tot = c[0] + c[1] + c[2] + c[3] + c[4];
+  float t = r0 * tot;
+  int k = 0;
+  while (k < 4 && (t >= c[k] || c[k] <= 0.f)) { t -= c[k]; ++k; }
+  if (c[k] <= 0.f) { k = 0; while (k < 4 && !(c[k] > 0.f)) ++k; }
+  code = 111 + k;
+  const float* A = pt.fa;
+  const float* B = pt.fb;
+  int a = 21, bb = 21;
+  if (k == 2) {
+    // (q, g) and (g, q) for q = -5..5, q != 0, in initFlux order
+    float tot2 = 0.f;
+    for (int q = -5; q <= 5; ++q)
+      if (q) tot2 += cp_xf_id(A, q) * B[2] + A[2] * cp_xf_id(B, q);
+    float u = r1 * tot2;
+    a = -5; bb = 21;
+    for (int q = -5; q <= 5; ++q) {
+      if (!q) continue;
+      float s1 = cp_xf_id(A, q) * B[2];
+      if (u < s1) { a = q; bb = 21; break; }
+      u -= s1;
+      float s2 = A[2] * cp_xf_id(B, q);
+      if (u < s2) { a = 21; bb = q; break; }
+      u -= s2;
+      a = 21; bb = q;   // rounding fall-through keeps the last pair
+    }
+  } else if (k == 3) {
+    float tot2 = 0.f;
+    for (int q1 = -5; q1 <= 5; ++q1)
+      for (int q2 = -5; q2 <= 5; ++q2)
+        if (q1 && q2) tot2 += cp_xf_id(A, q1) * cp_xf_id(B, q2) * cp_qq_pair_bracket(pt.b, q1, q2);
+    float u = r1 * tot2;
+    a = 5; bb = 5;
+    bool done = false;
+    for (int q1 = -5; q1 <= 5 && !done; ++q1)
+      for (int q2 = -5; q2 <= 5; ++q2) {
+        if (!q1 || !q2) continue;
+        float s = cp_xf_id(A, q1) * cp_xf_id(B, q2) * cp_qq_pair_bracket(pt.b, q1, q2);
+        a = q1; bb = q2;
+        if (u < s) { done = true; break; }
+        u -= s;
+      }
+  } else if (k == 4) {
+    float tot2 = 0.f;
+    for (int q = -5; q <= 5; ++q)
+      if (q) tot2 += cp_xf_id(A, q) * cp_xf_id(B, -q);
+    float u = r1 * tot2;
+    a = 5; bb = -5;
+    for (int q = -5; q <= 5; ++q) {
+      if (!q) continue;
+      float s = cp_xf_id(A, q) * cp_xf_id(B, -q);
+      a = q; bb = -q;
+      if (u < s) break;
+      u -= s;
+    }
+  }
+  id[0] = a; id[1] = bb;
+  if (k == 0 || k == 4) { id[2] = 21; id[3] = 21; }
+  else if (k == 1) {
+    int qn = 1 + (int)(P.nQuarkNew * r3);
+    if (qn > (int)P.nQuarkNew) qn = (int)P.nQuarkNew;
+    id[2] = qn; id[3] = -qn;
+  } else { id[2] = a; id[3] = bb; }
+}
+
+// Lab-frame four-momenta: parton 3 at cos(theta*) = z from beam A, azimuth phi; boost by the
+// rapidity y = (ln x1 - ln x2)/2 of the parton system (massless, PhaseSpace.cc 2 -> 2 kinematics).
+CP_HD void cp_make_event(const CpHadParams& P, const CpPoint& pt, float r0, float r1, float r2,
+                         float r3, float weight, uint32_t point, CpEventRec& ev)
+{
+  int code, id[4];
+  cp_pick_flavours(P, pt, r0, r1, r3, code, id);
+  for (int k = 0; k < 4; ++k) ev.id[k] = (int16_t)id[k];
+  const CpKin& k = pt.k;
+  float eBeam = 0.5f * cp_sqrtf(P.s);
+  float x1 = cp_expf(k.lnx1), x2 = cp_expf(k.lnx2);
+  ev.pz_in[0] = eBeam * x1;
+  ev.pz_in[1] = -eBeam * x2;
+  float pstar = 0.5f * cp_sqrtf(k.sH);
+  float z = 0.5f * (k.opz - k.omz);
+  float sinT = cp_sqrtf(k.omz * k.opz);
+  float pT = pstar * sinT;
+  float phi = 6.283185307f * r2;
+  float sphi, cphi;
+#if defined(__CUDA_ARCH__)
+  sincosf(phi, &sphi, &cphi);
+#else
+  sphi = sinf(phi); cphi = cosf(phi);
+#endif
+  float pzs = pstar * z;
+  float y = 0.5f * (k.lnx1 - k.lnx2);
+  float ey = cp_expf(y), iey = cp_expf(-y);
+  float ch = 0.5f * (ey + iey), sh = 0.5f * (ey - iey);
+  ev.p3[0] = pT * cphi; ev.p3[1] = pT * sphi;
+  ev.p3[2] = pzs * ch + pstar * sh; ev.p3[3] = pstar * ch + pzs * sh;
+  ev.p4[0] = -pT * cphi; ev.p4[1] = -pT * sphi;
+  ev.p4[2] = -pzs * ch + pstar * sh; ev.p4[3] = pstar * ch - pzs * sh;
+  ev.weight = weight;
+  ev.pt_hat = cp_sqrtf(k.pT2);
+  ev.process = (uint32_t)code;
+  ev.point = point;
 }

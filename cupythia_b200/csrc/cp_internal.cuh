@@ -3,16 +3,38 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <string.h>
 #include "../../include/cupythia_b200.h"
 #include "cp_params.h"
 
 #define CP_THREADS 256
 #ifndef CP_MIN_BLOCKS
-#define CP_MIN_BLOCKS 1   // resident blocks per SM the hot kernels are compiled for
+#define CP_MIN_BLOCKS 2   // resident blocks per SM the hot kernels are compiled for
 #endif
 #define CP_WARPS (CP_THREADS / 32)
 // per-block slot of the hadronic accumulation: sum w, sum w^2, max w, n_bad, then 3*nb hist
 #define CP_SLOT_HEAD 4
+
+// Weight histogram for the unweighting threshold: bin = IEEE-754 bits of w >> 18 (8 exponent
+// bits + 5 mantissa bits, monotone in w, about 2.2% wide), restricted to 2^-64 <= w < 2^64.
+#define CP_QBINS 4096
+#define CP_QBIN_OFFSET ((127 - 64) << 5)
+__host__ __device__ __forceinline__ int cp_qbin(float w)
+{
+  if (!(w > 0.f)) return -1;
+  uint32_t bits;
+  memcpy(&bits, &w, 4);
+  int b = (int)(bits >> 18) - CP_QBIN_OFFSET;
+  return b < 0 ? 0 : (b >= CP_QBINS ? CP_QBINS - 1 : b);
+}
+// upper edge of a bin
+__host__ __device__ __forceinline__ float cp_qbin_hi(int b)
+{
+  uint32_t bits = (uint32_t)(b + 1 + CP_QBIN_OFFSET) << 18;
+  float f;
+  memcpy(&f, &bits, 4);
+  return f;
+}
 
 // Per-iteration record written by the device refinement kernel (FP64).
 struct CpIterDev {
@@ -40,6 +62,11 @@ struct cp_handle {
   float *d_as = nullptr, *d_q2r = nullptr, *d_q2f = nullptr;
   // launch shape of the persistent integrand kernels
   int had_blocks = 0;
+  // weight histogram of the last iteration and the unweighting threshold (device)
+  unsigned long long* d_qhist = nullptr;   // CP_QBINS
+  double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
+  unsigned long long* d_counter = nullptr; // accepted-event counter
+  uint64_t last_n = 0;
   std::string err;
 };
 

@@ -1,0 +1,293 @@
+// cp_unweight.cu -- production pass: unweighting and on-device compaction into 64-byte records.
+//
+// One persistent kernel draws, maps and evaluates each point exactly like the VEGAS pass,
+// accepts it when u * w_max < w (cuPythia/07_unweighting_lhe/unweight_lhe.cu:54; overweight
+// events w > w_max are kept with weight w / w_max, as Pythia keeps them,
+// pythia8317/src/ProcessContainer.cc:383-385), and writes accepted events straight into a
+// dense array: one ballot per warp, one global atomic per warp, then each accepting lane stores
+// its 64-byte record as four 16-byte stores.  The reference instead writes flags and runs a
+// separate library compaction pass (cuPythia/10_cub_compaction/cub_compaction.cu:76-80,
+// cuPythia/pipeline/generate.cu:97-104).
+//
+// Random numbers: the accept draw is word 3 of the point's Philox block (stream 0); accepted
+// points draw a second block from stream 1 for the process / pair / azimuth / new-flavour picks.
+#include <vector>
+#include "cp_internal.cuh"
+
+#define CP_UNW_SLOT 8   // sum w, sum w^2, max w, n_bad, n_acc, sum event weight, n_over, unused
+
+struct UnwLaunch {
+  uint64_t seed, point0, n;
+  uint32_t iter;
+  int nb;
+  const double* edges;
+  const double* wmax;          // device threshold
+  CpEventRec* out;
+  uint64_t capacity;
+  unsigned long long* counter; // events written so far (may exceed capacity: reported)
+  double* slots;
+};
+
+static_assert(sizeof(CpEventRec) == 64, "event record must be 64 bytes");
+static_assert(sizeof(CpEventRec) == sizeof(cp_event), "C ABI record layout");
+
+__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_unweight(const CpHadParams P, const UnwLaunch L)
+{
+  __shared__ float2 sEdge[3][CP_MAX_BINS];
+  __shared__ double sRed[CP_WARPS][7];
+  const int nb = L.nb;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
+    int d = k / nb, b = k - d * nb;
+    const double* e = L.edges + d * (nb + 1);
+    double lo = e[b], hi = e[b + 1];
+    sEdge[d][b] = make_float2((float)lo, (float)(hi - lo));
+  }
+  __syncthreads();
+  const float wmax = (float)L.wmax[0];
+  const float nbf = (float)nb;
+  const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
+  const uint64_t gtid = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x;
+  const uint64_t rounds = (L.n + stride - 1) / stride;
+  float s1 = 0.f, c1 = 0.f, s2 = 0.f, c2 = 0.f, se = 0.f, ce = 0.f, wm = 0.f;
+  uint32_t nbad = 0, nacc = 0, nover = 0;
+
+  for (uint64_t r = 0; r < rounds; ++r) {
+    const uint64_t p = r * stride + gtid;
+    bool accept = false;
+    float w = 0.f;
+    CpPoint pt;
+    uint32_t wd[4] = {0, 0, 0, 0};
+    if (p < L.n) {
+      cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
+      float x[3], jv = 1.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int bin;
+        float frac;
+        cp_bin_frac(wd[d], nb, bin, frac);
+        float2 e = sEdge[d][bin];
+        x[d] = fmaf(frac, e.y, e.x);
+        jv *= nbf * e.y;
+      }
+      w = cp_had_eval(P, x[0], x[1], x[2], pt) * jv;
+      if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
+      cp_kahan(s1, c1, w);
+      cp_kahan(s2, c2, w * w);
+      wm = fmaxf(wm, w);
+      accept = cp_u24(wd[3]) * wmax < w;
+    }
+    const unsigned ball = __ballot_sync(0xffffffffu, accept);
+    if (ball == 0u) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(L.counter, (unsigned long long)__popc(ball));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (accept) {
+      const uint64_t slot = base + __popc(ball & ((1u << lane) - 1u));
+      float ew = w > wmax ? w / wmax : 1.f;
+      ++nacc;
+      nover += w > wmax ? 1u : 0u;
+      cp_kahan(se, ce, ew);
+      if (slot < L.capacity) {
+        uint32_t w2[4];
+        cp_point_words(L.seed, L.point0 + p, L.iter, 1, w2);
+        CpEventRec ev;
+        cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), ew,
+                      (uint32_t)(L.point0 + p), ev);
+        const uint4* src = reinterpret_cast<const uint4*>(&ev);
+        uint4* dst = reinterpret_cast<uint4*>(L.out + slot);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dst[q] = src[q];
+      }
+    }
+  }
+  // block reduction (FP32 compensated per thread, FP64 across warps)
+  double v[7] = {(double)s1 - (double)c1, (double)s2 - (double)c2, (double)wm, (double)nbad,
+                 (double)nacc, (double)se - (double)ce, (double)nover};
+#pragma unroll
+  for (int k = 0; k < 7; ++k) v[k] = (k == 2) ? cp_warp_max_d(v[k]) : cp_warp_sum_d(v[k]);
+  if (lane == 0)
+    for (int k = 0; k < 7; ++k) sRed[warp][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double* slot = L.slots + (size_t)blockIdx.x * CP_UNW_SLOT;
+    for (int k = 0; k < 7; ++k) {
+      double a = (k == 2) ? 0.0 : 0.0;
+      for (int q = 0; q < CP_WARPS; ++q) a = (k == 2) ? fmax(a, sRed[q][k]) : a + sRed[q][k];
+      slot[k] = a;
+    }
+    slot[7] = 0.0;
+  }
+}
+
+__global__ void k_set_wmax(double* wmax, double v) { wmax[0] = v; }
+
+static int unw_blocks(cp_handle* h)
+{
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_had_unweight, CP_THREADS, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+  }
+  return h->num_sms * per_sm;
+}
+
+// Enqueue one production pass on h->stream (no host synchronisation).
+static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, cp_event* out,
+                            uint64_t capacity, double* red_dst)
+{
+  const int blocks = unw_blocks(h);
+  int rc = cp_ensure_slots(h, (size_t)blocks * CP_UNW_SLOT);
+  if (rc) return rc;
+  UnwLaunch L;
+  L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.nb = h->nb;
+  L.edges = h->d_edges; L.wmax = h->d_wmax; L.out = reinterpret_cast<CpEventRec*>(out);
+  L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
+  k_had_unweight<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+  CP_LAUNCH_CHECK(h, "k_had_unweight");
+  k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
+  CP_LAUNCH_CHECK(h, "k_reduce_slots");
+  return CP_OK;
+}
+
+static void fill_unw(const double* red, double n, double wmax, cp_unweight_result* o)
+{
+  double mean = red[0] / n, var = (red[1] / n - mean * mean) / (n - 1.0);
+  o->sigma = mean;
+  o->sigma_err = sqrt(var > 0 ? var : 0);
+  o->sigma_unweighted = wmax * red[5] / n;
+  o->w_max = wmax;
+  o->w_max_seen = red[2];
+  o->n_points = (uint64_t)n;
+  o->n_accepted = (uint64_t)red[4];
+  o->n_overweight = (uint64_t)red[6];
+  o->n_bad = (uint64_t)red[3];
+  o->eta = red[4] / n;
+}
+
+extern "C" int cp_set_wmax(cp_handle* h, double w_max)
+{
+  CP_CHECK_HANDLE(h);
+  if (!(w_max > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_set_wmax: w_max must be positive");
+  k_set_wmax<<<1, 1, 0, h->stream>>>(h->d_wmax, w_max);
+  CP_LAUNCH_CHECK(h, "k_set_wmax");
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}
+
+extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_event* records_dev,
+                           uint64_t capacity, cp_unweight_result* out)
+{
+  CP_CHECK_HANDLE(h);
+  if (n_points < 2) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: n_points < 2");
+  if (capacity && !records_dev) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: null records");
+  if (((uintptr_t)records_dev & 15) != 0) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: records must be 16-byte aligned");
+  double wm[2];
+  CP_CUDA(h, cudaMemcpyAsync(wm, h->d_wmax, sizeof wm, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: no threshold (cp_weight_quantile or cp_set_wmax)");
+  CP_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), h->stream));
+  int rc = unweight_enqueue(h, 0, n_points, iter, records_dev, capacity, h->d_red);
+  if (rc) return rc;
+  double red[8];
+  unsigned long long cnt = 0;
+  CP_CUDA(h, cudaMemcpyAsync(red, h->d_red, sizeof red, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaMemcpyAsync(&cnt, h->d_counter, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (out) fill_unw(red, (double)n_points, wm[0], out);
+  if (cnt > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_unweight: record buffer too small (n_accepted reported)");
+  if (red[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}
+
+// Chunked production into HOST memory: chunk k is computed into one of two device buffers
+// while chunk k-1 is copied to the host on a second stream, so the PCIe transfer of the
+// records overlaps the integrand.  records_host should be pinned for the copies to overlap.
+extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t chunk,
+                                cp_event* records_host, uint64_t capacity, cp_unweight_result* out)
+{
+  CP_CHECK_HANDLE(h);
+  if (n_points < 2 || chunk < 2) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: bad sizes");
+  if (capacity && !records_host) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: null records");
+  double wm[2];
+  CP_CUDA(h, cudaMemcpyAsync(wm, h->d_wmax, sizeof wm, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: no threshold");
+  if (chunk > n_points) chunk = n_points;
+  const uint64_t nchunks = (n_points + chunk - 1) / chunk;
+  // a chunk accepts at most every point; size the staging buffers for the chunk
+  const uint64_t stage_cap = chunk;
+  cp_event* stage[2] = {nullptr, nullptr};
+  double* red = nullptr;
+  unsigned long long* cnt = nullptr;
+  cudaStream_t copy = nullptr;
+  cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+  std::vector<unsigned long long> hcnt(nchunks, 0);
+  std::vector<double> hred(nchunks * 8, 0.0);
+  int rc = CP_OK;
+  uint64_t written = 0;
+  cudaError_t e = cudaSuccess;
+  do {
+    if ((e = cudaMalloc(&stage[0], sizeof(cp_event) * stage_cap)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&stage[1], sizeof(cp_event) * stage_cap)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&red, sizeof(double) * 8 * nchunks)) != cudaSuccess) break;
+    if ((e = cudaMalloc(&cnt, sizeof(unsigned long long) * nchunks)) != cudaSuccess) break;
+    if ((e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking)) != cudaSuccess) break;
+    for (int b = 0; b < 2; ++b) {
+      if ((e = cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming)) != cudaSuccess) break;
+      if ((e = cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming)) != cudaSuccess) break;
+    }
+    if (e != cudaSuccess) break;
+    if ((e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * nchunks, h->stream)) != cudaSuccess) break;
+    for (uint64_t c = 0; c < nchunks && rc == CP_OK; ++c) {
+      const int b = (int)(c & 1);
+      const uint64_t p0 = c * chunk, n = (p0 + chunk <= n_points) ? chunk : n_points - p0;
+      if (c >= 2 && (e = cudaStreamWaitEvent(h->stream, copied[b], 0)) != cudaSuccess) break;
+      unsigned long long* saved = h->d_counter;
+      h->d_counter = cnt + c;
+      rc = unweight_enqueue(h, p0, n, iter, stage[b], stage_cap, red + 8 * c);
+      h->d_counter = saved;
+      if (rc) break;
+      if ((e = cudaEventRecord(done[b], h->stream)) != cudaSuccess) break;
+      // the host needs this chunk's count to place its records
+      if ((e = cudaMemcpyAsync(&hcnt[c], cnt + c, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               h->stream)) != cudaSuccess) break;
+      if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) break;
+      uint64_t take = hcnt[c] < stage_cap ? hcnt[c] : stage_cap;
+      if (written + take > capacity) take = capacity > written ? capacity - written : 0;
+      if ((e = cudaStreamWaitEvent(copy, done[b], 0)) != cudaSuccess) break;
+      if (take && (e = cudaMemcpyAsync(records_host + written, stage[b], sizeof(cp_event) * take,
+                                       cudaMemcpyDeviceToHost, copy)) != cudaSuccess) break;
+      if ((e = cudaEventRecord(copied[b], copy)) != cudaSuccess) break;
+      written += take;
+    }
+    if (e != cudaSuccess || rc) break;
+    if ((e = cudaStreamSynchronize(copy)) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(hred.data(), red, sizeof(double) * 8 * nchunks, cudaMemcpyDeviceToHost,
+                             h->stream)) != cudaSuccess) break;
+    e = cudaStreamSynchronize(h->stream);
+  } while (0);
+  if (copy) cudaStreamSynchronize(copy);
+  for (int b = 0; b < 2; ++b) {
+    if (done[b]) cudaEventDestroy(done[b]);
+    if (copied[b]) cudaEventDestroy(copied[b]);
+  }
+  if (copy) cudaStreamDestroy(copy);
+  if (stage[0]) cudaFree(stage[0]);
+  if (stage[1]) cudaFree(stage[1]);
+  if (red) cudaFree(red);
+  if (cnt) cudaFree(cnt);
+  if (e != cudaSuccess) return cp_fail_cuda(h, e, "cp_generate_host");
+  if (rc) return rc;
+  double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint64_t total_acc = 0;
+  for (uint64_t c = 0; c < nchunks; ++c) {
+    for (int k = 0; k < 8; ++k) tot[k] = (k == 2) ? (hred[8 * c + k] > tot[k] ? hred[8 * c + k] : tot[k]) : tot[k] + hred[8 * c + k];
+    total_acc += hcnt[c];
+  }
+  if (out) fill_unw(tot, (double)n_points, wm[0], out);
+  if (total_acc > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_generate_host: record buffer too small");
+  if (tot[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}

@@ -20,6 +20,7 @@ struct HadLaunch {
   double* slots;   // gridDim.x * (CP_SLOT_HEAD + 3 nb)
   float* w_out;    // optional per-point weights
   float* x_out;    // optional per-point mapped x (3 per point)
+  unsigned long long* qhist;   // weight histogram (CP_QBINS), integer adds
 };
 
 template <bool WRITE>
@@ -28,6 +29,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
   __shared__ float2 sEdge[3][CP_MAX_BINS];
   __shared__ float sHist[CP_WARPS][3][CP_MAX_BINS];
   __shared__ float sRed[CP_WARPS][6];
+  __shared__ unsigned sQ[CP_QBINS];
   const int nb = L.nb;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
@@ -38,6 +40,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
   }
   for (int k = threadIdx.x; k < CP_WARPS * 3 * CP_MAX_BINS; k += CP_THREADS)
     (&sHist[0][0][0])[k] = 0.f;
+  for (int k = threadIdx.x; k < CP_QBINS; k += CP_THREADS) sQ[k] = 0u;
   __syncthreads();
 
   const float nbf = (float)nb;
@@ -70,6 +73,8 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
       cp_kahan(s1, c1, w);
       cp_kahan(s2, c2, w * w);
       wmax = fmaxf(wmax, w);
+      int qb = cp_qbin(w);
+      if (qb >= 0) atomicAdd(&sQ[qb], 1u);
       if (WRITE) {
         if (L.w_out) L.w_out[p] = w;
         if (L.x_out) { L.x_out[3 * p] = x[0]; L.x_out[3 * p + 1] = x[1]; L.x_out[3 * p + 2] = x[2]; }
@@ -114,6 +119,29 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
     for (int q = 0; q < CP_WARPS; ++q) s += sHist[q][d][b];
     slot[CP_SLOT_HEAD + k] = (double)s;
   }
+  for (int k = threadIdx.x; k < CP_QBINS; k += CP_THREADS)
+    if (sQ[k]) atomicAdd(&L.qhist[k], (unsigned long long)sQ[k]);
+}
+
+// Smallest bin edge w such that at most (1 - q) n of the weights lie above it (q-quantile,
+// rounded up to the bin's upper edge); stored as the unweighting threshold.
+__global__ void k_quantile(const unsigned long long* __restrict__ qhist, double q, double* wmax)
+{
+  __shared__ unsigned long long sh[CP_QBINS];
+  for (int k = threadIdx.x; k < CP_QBINS; k += blockDim.x) sh[k] = qhist[k];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  unsigned long long tot = 0;
+  for (int k = 0; k < CP_QBINS; ++k) tot += sh[k];
+  double allowed = (1.0 - q) * (double)tot;
+  unsigned long long above = 0;
+  int b = CP_QBINS - 1;
+  for (; b > 0; --b) {
+    if ((double)(above + sh[b]) > allowed) break;
+    above += sh[b];
+  }
+  wmax[0] = (double)cp_qbin_hi(b);
+  wmax[1] = q;
 }
 
 // Iteration record and, if alpha > 0, Lepage's refinement of each dimension (FP64, one
@@ -187,6 +215,9 @@ static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, 
   HadLaunch L;
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.stream = stream;
   L.nb = h->nb; L.edges = h->d_edges; L.slots = h->d_slots; L.w_out = w_out; L.x_out = x_out;
+  L.qhist = h->d_qhist;
+  CP_CUDA(h, cudaMemsetAsync(h->d_qhist, 0, sizeof(unsigned long long) * CP_QBINS, h->stream));
+  h->last_n = n;
   if (w_out || x_out) k_had_accum<true><<<h->had_blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
   else k_had_accum<false><<<h->had_blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
   CP_LAUNCH_CHECK(h, "k_had_accum");
@@ -300,5 +331,31 @@ extern "C" int cp_weight_at(cp_handle* h, const float* x, int64_t n, float* w)
   k_weight_at<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, x, n, w);
   CP_LAUNCH_CHECK(h, "k_weight_at");
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}
+
+extern "C" int cp_last_histogram(cp_handle* h, double* out)
+{
+  CP_CHECK_HANDLE(h);
+  if (!out) return cp_fail(h, CP_ERR_INVALID, "cp_last_histogram: null output");
+  CP_CUDA(h, cudaMemcpyAsync(out, h->d_red, sizeof(double) * (CP_SLOT_HEAD + 3 * h->nb),
+                             cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}
+
+extern "C" int cp_weight_quantile(cp_handle* h, double q, double* w_q)
+{
+  CP_CHECK_HANDLE(h);
+  if (!(q > 0.0 && q < 1.0)) return cp_fail(h, CP_ERR_INVALID, "cp_weight_quantile: q must be in (0, 1)");
+  if (h->last_n == 0) return cp_fail(h, CP_ERR_INVALID, "cp_weight_quantile: run an iteration first");
+  k_quantile<<<1, 256, 0, h->stream>>>(h->d_qhist, q, h->d_wmax);
+  CP_LAUNCH_CHECK(h, "k_quantile");
+  if (w_q) {
+    double v[2];
+    CP_CUDA(h, cudaMemcpyAsync(v, h->d_wmax, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+    CP_CUDA(h, cudaStreamSynchronize(h->stream));
+    *w_q = v[0];
+  }
   return CP_OK;
 }

@@ -83,6 +83,16 @@ typedef struct cp_event {
   uint32_t point;      /* low 32 bits of the point index that produced the event    */
 } cp_event;
 
+/* Result of a production (unweighting) pass. */
+typedef struct cp_unweight_result {
+  double sigma, sigma_err;       /* weighted estimate of the pass, mb                    */
+  double sigma_unweighted;       /* w_max * (sum of event weights) / n_points, mb        */
+  double w_max;                  /* threshold used                                       */
+  double w_max_seen;             /* largest weight of the pass                           */
+  double eta;                    /* n_accepted / n_points                                */
+  uint64_t n_points, n_accepted, n_overweight, n_bad;
+} cp_unweight_result;
+
 /* Gradient of the estimator (cp_adjoint). */
 typedef struct cp_grad {
   double sigma, var;            /* estimator value and Var[w] of the batch           */
@@ -158,6 +168,31 @@ int cp_point_weights(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, f
 /* FP32 integrand at caller-given x in [0,1]^3 (dev, 3n floats): f * J_base, mb. */
 int cp_weight_at(cp_handle* h, const float* x_dev, int64_t n, float* w_dev);
 
+/* Reduced sums of the last VEGAS pass (host, 4 + 3 n_bins doubles): sum w, sum w^2, max w,
+ * n_bad, then the per-bin sums of w^2 of each dimension (the refinement's input). */
+int cp_last_histogram(cp_handle* h, double* out_host);
+
+/* ---------------------------------------------------------------- unweighting ------ */
+/* q-quantile of the weights of the last VEGAS pass (integer weight histogram, ~2% bins,
+ * rounded up), stored as the handle's unweighting threshold; the production run uses
+ * q = 0.999.  Replaces the host w_max scans of cuPythia/07_unweighting_lhe/unweight_lhe.cu:59-63
+ * and cuPythia/pipeline/generate.cu:71-76. */
+int cp_weight_quantile(cp_handle* h, double q, double* w_q_host);
+/* Sets the unweighting threshold explicitly. */
+int cp_set_wmax(cp_handle* h, double w_max);
+/* Production pass over points [0, n_points) of counter iteration iter: fused draw -> map ->
+ * integrand -> accept (u w_max < w; overweight events kept with weight w / w_max) -> compaction
+ * of accepted events into records_dev (capacity records).  Replaces the unweighting kernels
+ * (cuPythia/07_unweighting_lhe/unweight_lhe.cu:42-57, cuPythia/pipeline/generate.cu:56-62) and
+ * the flag + library compaction (cuPythia/10_cub_compaction/cub_compaction.cu:36-46,76-80).
+ * Returns CP_ERR_CAPACITY (with the counts filled in) when more events were accepted than fit. */
+int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_event* records_dev,
+                uint64_t capacity, cp_unweight_result* out_host);
+/* The same production pass delivering the records to HOST memory (pinned for overlap), in
+ * chunks of `chunk` points whose device-to-host copies overlap the next chunk's compute. */
+int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t chunk,
+                     cp_event* records_host, uint64_t capacity, cp_unweight_result* out_host);
+
 /* ---------------------------------------------------------------- partonic gg->gg --- */
 /* Fused resident gg->gg MC in FP64 (cuPythia/03_fused_resident_me/fused_gg2gg.cu:40-51):
  * cos theta = (2u-1) cMax, u from Philox (point i: counter (i, 0, 0, 0), 53-bit uniform of
@@ -171,6 +206,12 @@ int cp_partonic_splitmix(cp_handle* h, double sqrt_shat, double alphas, double c
 /* Per-point FP64 weights of the Philox form, points [point0, point0+n). */
 int cp_partonic_weights(cp_handle* h, double sqrt_shat, double alphas, double cmax, double conv,
                         uint64_t seed, uint64_t point0, uint64_t n, double* w_dev);
+
+/* ---------------------------------------------------------------- measurement ------ */
+/* FP32 FMA and MUFU (ex2) throughput of the device from dependency-free microbenchmarks:
+ * TFLOP/s (2 per FMA) and Tops/s.  No reference counterpart: the integrand's roofline
+ * denominators (it is SIMT FP32 / SFU work). */
+int cp_measure_peaks(cp_handle* h, double* fp32_tflops_host, double* mufu_tops_host);
 
 #ifdef __cplusplus
 }

@@ -163,7 +163,8 @@ def test_iteration_sums_and_histogram_match_oracle(integ, orc):
     assert r["n_bad"] == 0
     assert abs(r["sum_w"] / w.sum() - 1) < 1e-6
     assert abs(r["sum_w2"] / (w * w).sum() - 1) < 1e-6
-    # refined grid == oracle refinement of the oracle histogram of the same points
+    h = integ.last_histogram()
+    # per-bin sums of w^2 against the FP64 oracle on the same points
     L = orc.lib()
     e = grid.reshape(-1).copy()
     sums = np.zeros(2)
@@ -172,8 +173,11 @@ def test_iteration_sums_and_histogram_match_oracle(integ, orc):
     L.cpo_had_accumulate(C.byref(cfg), orc.dptr(e), integ.nb, integ.cfg.seed, 5, 0, n,
                          orc.dptr(sums), orc.dptr(hist), 8)
     assert abs(sums[0] / r["sum_w"] - 1) < 2e-6
-    L.cpo_vegas_refine(orc.dptr(e), orc.dptr(hist), 3, integ.nb, 1.5)
-    assert np.max(np.abs(integ.grid.reshape(-1) - e)) < 1e-5
+    assert np.allclose(h["hist"].reshape(-1), hist, rtol=1e-4, atol=1e-12 * hist.max())
+    # the device refinement of the device histogram == the oracle refinement of the same input
+    e2 = grid.reshape(-1).copy()
+    L.cpo_vegas_refine(orc.dptr(e2), orc.dptr(np.ascontiguousarray(h["hist"].reshape(-1))), 3, integ.nb, 1.5)
+    assert np.max(np.abs(integ.grid.reshape(-1) - e2)) < 1e-12
     integ.reset_grid()
 
 
