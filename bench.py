@@ -221,7 +221,7 @@ def run_ours(a):
     e2e_sec = allmax(pg, max(e0.elapsed_time(e1) / 1e3, wall), dev)
     e2e_all = allsum(pg, e2e_events, dev)
 
-    # ---- roofline of the dominant kernel (k_had_unweight): FP32-pipe work per point
+    # ---- roofline of the dominant kernel (k_unw_accept): FP32-pipe work per point
     peaks, src = measured_peaks()
     fp32_peak = fp32_peak_tflops(it, stream)
     ops = FP32_FLOP_PER_POINT
@@ -243,8 +243,8 @@ def run_ours(a):
         "adapt_seconds": adapt_s,
         "e2e": {"value": e2e_all / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": GRID_BYTES,
                 "d2h_bytes_per_step": int(d2h / e2e_steps)},
-        "gpu_launches": 2 * a.steps,
-        "roofline": {"bound": "fp32", "kernel": "k_had_unweight", "achieved": achieved,
+        "gpu_launches": 3 * a.steps,
+        "roofline": {"bound": "fp32", "kernel": "k_unw_accept", "achieved": achieved,
                      "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks)",
                      "flop_per_point": ops, "traffic": None, "ms_per_launch": unit_ms,
@@ -260,7 +260,7 @@ def run_ours(a):
 
 
 # FP32 FLOP per point of the fused integrand (FADD + FMUL + 2 FFMA, thread level), from the ncu
-# SASS counters of k_had_unweight on a 2^22-point pass; see profiles/.
+# SASS counters of k_unw_accept on a 2^22-point pass; see profiles/.
 FP32_FLOP_PER_POINT = 1500.0
 
 

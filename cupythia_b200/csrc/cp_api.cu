@@ -123,7 +123,9 @@ extern "C" int cp_create(const cp_config* cfg, cp_handle** out)
             cudaMalloc(&h->d_qhist, sizeof(unsigned long long) * CP_QBINS) == cudaSuccess &&
             cudaMalloc(&h->d_wmax, sizeof(double) * 2) == cudaSuccess &&
             cudaMalloc(&h->d_counter, sizeof(unsigned long long) * 2) == cudaSuccess &&
-            cudaMemset(h->d_wmax, 0, sizeof(double) * 2) == cudaSuccess;
+            cudaMemset(h->d_wmax, 0, sizeof(double) * 2) == cudaSuccess &&
+            cudaMalloc(&h->d_cteq, sizeof(CpCteqPoly) * 8) == cudaSuccess &&
+            cudaMemcpy(h->d_cteq, h->P.cteq, sizeof(CpCteqPoly) * 8, cudaMemcpyHostToDevice) == cudaSuccess;
   if (!ok || cp_had_launch_shape(h) != CP_OK || cp_ensure_iters(h, 16) != CP_OK) {
     cp_destroy(h);
     return CP_ERR_NOMEM;
@@ -140,7 +142,7 @@ extern "C" int cp_destroy(cp_handle* h)
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
-                  h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter};
+                  h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete h;
@@ -309,11 +311,15 @@ __global__ void k_set2kin(const CpHadParams P, int64_t n, const float* __restric
 }
 
 // which: 0 = sigmaKin of code (flavour independent), 1 = sigmaHat(id1, id2), 2 = sigmaPDF(mask)
-__global__ void k_sigma(const CpHadParams P, int64_t n, int which, int code, int id1, int id2, int mask,
-                        const float* __restrict__ x1, const float* __restrict__ x2,
-                        const float* __restrict__ sH, const float* __restrict__ tH,
-                        const float* __restrict__ as, const float* __restrict__ q2f, float* out)
+__global__ void k_sigma(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n, int which, int code,
+                        int id1, int id2, int mask, const float* __restrict__ x1,
+                        const float* __restrict__ x2, const float* __restrict__ sH,
+                        const float* __restrict__ tH, const float* __restrict__ as,
+                        const float* __restrict__ q2f, float* out)
 {
+  __shared__ CpCteqPoly cteq[8];
+  cp_stage_cteq(cteq, cteq_g);
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     float s = sH[i], t = tH[i], u = -(s + t);
@@ -326,11 +332,8 @@ __global__ void k_sigma(const CpHadParams P, int64_t n, int which, int code, int
     if (which == 2) {
       float m[5];
       for (int k = 0; k < 5; ++k) m[k] = (mask >> k) & 1 ? 1.f : 0.f;
-      CpCteqQ q[8];
-      cp_cteq_q(P, q2f[i], q);
       float fa[8], fb[8];
-      cp_cteq_x(P, q, logf(x1[i]), 0.f, fa);
-      cp_cteq_x(P, q, logf(x2[i]), 0.f, fb);
+      cp_cteq_pair(cteq, q2f[i], logf(x1[i]), 0.f, logf(x2[i]), 0.f, fa, fb);
       v = P.conv * pref * cp_channel_sum(m, b, fa, fb);
     } else {
       float br = 0.f;
@@ -349,15 +352,17 @@ __global__ void k_sigma(const CpHadParams P, int64_t n, int which, int code, int
   }
 }
 
-__global__ void k_pdf(const CpHadParams P, int64_t n, const float* __restrict__ x,
+__global__ void k_pdf(const CpCteqPoly* cteq_g, int64_t n, const float* __restrict__ x,
                       const float* __restrict__ q2, float* out)
 {
+  __shared__ CpCteqPoly cteq[8];
+  cp_stage_cteq(cteq, cteq_g);
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    CpCteqQ q[8];
-    cp_cteq_q(P, q2[i], q);
-    float f[8];
-    cp_cteq_x(P, q, logf(x[i]), 0.f, f);
+    float f[8], g[8];
+    float lx = logf(x[i]);
+    cp_cteq_pair(cteq, q2[i], lx, 0.f, lx, 0.f, f, g);
     // id order -5..-1, 1..5, 21; f = {d, u, g, ubar, dbar, s, c, b}
     float* o = out + 11 * i;
     o[0] = f[7]; o[1] = f[6]; o[2] = f[5]; o[3] = f[3]; o[4] = f[4];
@@ -390,7 +395,7 @@ static int sigma_launch(cp_handle* h, int which, int code, int id1, int id2, int
 {
   if (h->kin_n == 0) return CP_OK;
   if (!out) return cp_fail(h, CP_ERR_INVALID, "null output");
-  k_sigma<<<grid_for(h, h->kin_n), 256, 0, h->stream>>>(h->P, h->kin_n, which, code, id1, id2, mask,
+  k_sigma<<<grid_for(h, h->kin_n), 256, 0, h->stream>>>(h->P, h->d_cteq, h->kin_n, which, code, id1, id2, mask,
                                                          h->d_x1, h->d_x2, h->d_sH, h->d_tH, h->d_as,
                                                          h->d_q2f, out);
   CP_LAUNCH_CHECK(h, "k_sigma");
@@ -439,7 +444,7 @@ extern "C" int cp_pdf_batch(cp_handle* h, const float* x, const float* q2, int64
   CP_CHECK_HANDLE(h);
   if (n < 0 || (n > 0 && (!x || !q2 || !out))) return cp_fail(h, CP_ERR_INVALID, "cp_pdf_batch: bad arguments");
   if (!n) return CP_OK;
-  k_pdf<<<grid_for(h, n), 256, 0, h->stream>>>(h->P, n, x, q2, out);
+  k_pdf<<<grid_for(h, n), 256, 0, h->stream>>>(h->d_cteq, n, x, q2, out);
   CP_LAUNCH_CHECK(h, "k_pdf");
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return CP_OK;

@@ -92,36 +92,6 @@ CP_HD float cp_alphas(const CpHadParams& P, float Q2)
   return (12.f * CP_PI_F) / (b0 * (lnQ2 - lnL2));
 }
 
-// Q-dependent CTEQ5L coefficients, shared by both beams.
-struct CpCteqQ {
-  float A, B, af1, af2, p, af5, af6, af7, af8, qfac;
-};
-
-CP_HD void cp_cteq_q(const CpHadParams& P, float Q2, CpCteqQ q[8])
-{
-  // Q2 clamp of PartonDistributions.cc:925
-  if (Q2 > 1e8f) Q2 = 1e8f;
-  if (Q2 < 1.f) Q2 = 1.f;
-  float Q = cp_sqrtf(Q2);
-  float lnQ = 0.5f * cp_logf(Q2);
-  float invQ = 1.f / Q;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const CpCteqPoly& c = P.cteq[i];
-    float sb1 = cp_logf(lnQ - c.lnAlpha) - 1.2f;
-    q[i].A = cp_poly(c.A, sb1);
-    q[i].B = cp_poly(c.B, sb1);
-    q[i].af1 = cp_poly(c.af1, sb1);
-    q[i].af2 = cp_poly(c.af2, sb1);
-    q[i].p = cp_poly(c.p, sb1);
-    q[i].af5 = cp_poly(c.af5, sb1);
-    q[i].af6 = cp_poly(c.af6, sb1);
-    q[i].af7 = cp_poly(c.af7, sb1);
-    q[i].af8 = cp_poly(c.af8, sb1);
-    q[i].qfac = (Q > c.qlim) ? (1.f - c.qmin * invQ) : 0.f;
-  }
-}
-
 // Error-free transformations on FP32 (Knuth TwoSum, FMA TwoProd) used to carry the few
 // quantities whose FP32 rounding would otherwise be amplified (ln tau, ln x, the CTEQ5L exponent).
 CP_HD void cp_twosum(float a, float b, float& s, float& e)
@@ -139,68 +109,125 @@ CP_HD void cp_acc2(float& s, float& c, float v)
   c += e;
 }
 
-// Proton x f for one beam from ln x = lnx + lnxLo (<= 0, lnxLo a sub-ulp correction):
-// out = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.
-CP_HD void cp_cteq_x(const CpHadParams& P, const CpCteqQ q[8], float lnx, float lnxLo, float out[8])
+// x-dependent quantities of one beam, from ln x = lnx + lnxLo (<= 0, lnxLo a sub-ulp correction)
+struct CpBeamX {
+  float x, omx, lny, uh, ul, x1L;
+};
+
+CP_HD CpBeamX cp_beam_x(float lnx, float lnxLo)
 {
   // x clamp of PartonDistributions.cc:926
   const float lnxMin = -13.815510558f;   // ln 1e-6
   if (lnx < lnxMin) { lnx = lnxMin; lnxLo = 0.f; }
+  CpBeamX b;
   float x = cp_expf(lnx);
   float omx = -cp_expm1f(lnx);           // 1 - x
   x = cp_fmaf(x, lnxLo, x);
   omx = cp_fmaf(-x, lnxLo, omx);
   if (omx < 1e-10f) { omx = 1e-10f; x = 1.f - 1e-10f; lnx = -1e-10f; lnxLo = 0.f; }
   float y = -lnx;                        // y = -ln x, correction -lnxLo
-  float lny = cp_logf(y) - lnxLo / y;
+  b.lny = cp_logf(y) - lnxLo / y;
   // u = ln(x / 1e-5) = ln x + ln 1e5 as a (hi, lo) pair
   const float LN1E5_HI = 11.512925148f, LN1E5_LO = 3.1696e-07f;
-  float uh, ul;
-  cp_twosum(lnx, LN1E5_HI, uh, ul);
-  ul += LN1E5_LO + lnxLo;
-  float x1L = cp_logf(omx);
-  float sumUbarDbar = 0.f;
-#pragma unroll
+  cp_twosum(lnx, LN1E5_HI, b.uh, b.ul);
+  b.ul += LN1E5_LO + lnxLo;
+  b.x1L = cp_logf(omx);
+  b.x = x;
+  b.omx = omx;
+  return b;
+}
+
+// Q-dependent coefficients of parametrisation i, shared by both beams
+struct CpCteqQ {
+  float A, B, af1, af2, p, af5, af6, af7, af8, qfac;
+};
+
+CP_HD CpCteqQ cp_cteq_coef(const CpCteqPoly& c, float lnQ, float Q, float invQ)
+{
+  CpCteqQ q;
+  float sb1 = cp_logf(lnQ - c.lnAlpha) - 1.2f;
+  q.A = cp_poly(c.A, sb1);
+  q.B = cp_poly(c.B, sb1);
+  q.af1 = cp_poly(c.af1, sb1);
+  q.af2 = cp_poly(c.af2, sb1);
+  q.p = cp_poly(c.p, sb1);
+  q.af5 = cp_poly(c.af5, sb1);
+  q.af6 = cp_poly(c.af6, sb1);
+  q.af7 = cp_poly(c.af7, sb1);
+  q.af8 = cp_poly(c.af8, sb1);
+  q.qfac = (Q > c.qlim) ? (1.f - c.qmin * invQ) : 0.f;
+  return q;
+}
+
+// "answer" of xfUpdate (PartonDistributions.cc:1031-1046) for one parametrisation and beam:
+// x exp(exponent) (1 - Qmin/Q), with
+//   exponent = A + B x + C u + af1 (y^p - 1) U + part3 + ut1 ln(1-x) + af2 L,  C = af1 af8,
+// summed with the products' FMA residuals and the additions' TwoSum errors kept in a second
+// float, and exp(hi + lo) = exp(hi) (1 + lo).
+CP_HD float cp_cteq_answer(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX& b)
+{
+  // y^p - 1 with the rounding residual of p ln y carried into first order
+  float ah = a.p * b.lny;
+  float al = cp_fmaf(a.p, b.lny, -ah);
+  float ym1 = cp_expm1f(ah);
+  ym1 = cp_fmaf(1.f + ym1, al, ym1);
+  float U = cp_fmaf(a.af8, b.uh, 1.f);
+  float part3 = b.x * b.omx * (a.af5 + a.af6 * b.omx + a.af7 * b.x * b.omx);
+  float L = c.useX1L ? b.x1L : cp_logf(b.omx + c.eut2);
+  float Ch = a.af1 * a.af8, Cl = cp_fmaf(a.af1, a.af8, -Ch);
+  float t3 = Ch * b.uh, t3l = cp_fmaf(Ch, b.uh, -t3) + Ch * b.ul + Cl * b.uh;
+  float qv = a.af1 * ym1;
+  float t4 = qv * U, t4l = cp_fmaf(qv, U, -t4);
+  float t2 = a.B * b.x, t2l = cp_fmaf(a.B, b.x, -t2);
+  float t6 = c.ut1 * b.x1L, t6l = cp_fmaf(c.ut1, b.x1L, -t6);
+  float t7 = a.af2 * L, t7l = cp_fmaf(a.af2, L, -t7);
+  float eh = a.A, el = (t2l + t3l) + (t4l + t6l + t7l);
+  cp_acc2(eh, el, t3);
+  cp_acc2(eh, el, t4);
+  cp_acc2(eh, el, t2);
+  cp_acc2(eh, el, part3);
+  cp_acc2(eh, el, t6);
+  cp_acc2(eh, el, t7);
+  float ex = cp_expf(eh);
+  return b.x * cp_fmaf(ex, el, ex) * a.qfac;
+}
+
+// CTEQ5L of a proton for both beams at one factorisation scale (PDF::xf + CTEQ5L::xfUpdate):
+// fa, fb = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.  The 8 parametrisations run as a rolled loop
+// over coefficient records `cteq` (staged in shared memory by the kernels) to keep the code
+// small; each result lands in its register through predicated selects.
+CP_HD void cp_cteq_pair(const CpCteqPoly* cteq, float Q2, float lnxA, float lnxAL, float lnxB,
+                        float lnxBL, float fa[8], float fb[8])
+{
+  // Q2 clamp of PartonDistributions.cc:925
+  if (Q2 > 1e8f) Q2 = 1e8f;
+  if (Q2 < 1.f) Q2 = 1.f;
+  const float Q = cp_sqrtf(Q2);
+  const float lnQ = 0.5f * cp_logf(Q2);
+  const float invQ = 1.f / Q;
+  const CpBeamX A = cp_beam_x(lnxA, lnxAL), B = cp_beam_x(lnxB, lnxBL);
+#pragma unroll 1
   for (int i = 0; i < 8; ++i) {
-    const CpCteqPoly& c = P.cteq[i];
-    const CpCteqQ& a = q[i];
-    // y^p - 1 with the rounding residual of p ln y carried into first order
-    float ah = a.p * lny;
-    float al = cp_fmaf(a.p, lny, -ah);
-    float ym1 = cp_expm1f(ah);
-    ym1 = cp_fmaf(1.f + ym1, al, ym1);
-    float U = cp_fmaf(a.af8, uh, 1.f);
-    float part3 = x * omx * (a.af5 + a.af6 * omx + a.af7 * x * omx);
-    float L = c.useX1L ? x1L : cp_logf(omx + c.eut2);
-    // exponent = A + B x + C u + af1 (y^p - 1) U + part3 + ut1 ln(1-x) + af2 L, C = af1 af8,
-    // summed with the product residuals and addition errors carried in a second float
-    float Ch = a.af1 * a.af8, Cl = cp_fmaf(a.af1, a.af8, -Ch);
-    float t3 = Ch * uh, t3l = cp_fmaf(Ch, uh, -t3) + Ch * ul + Cl * uh;
-    float qv = a.af1 * ym1;
-    float t4 = qv * U, t4l = cp_fmaf(qv, U, -t4);
-    float t2 = a.B * x, t2l = cp_fmaf(a.B, x, -t2);
-    float t6 = c.ut1 * x1L, t6l = cp_fmaf(c.ut1, x1L, -t6);
-    float t7 = a.af2 * L, t7l = cp_fmaf(a.af2, L, -t7);
-    float eh = a.A, el = (t2l + t3l) + (t4l + t6l + t7l);
-    cp_acc2(eh, el, t3);
-    cp_acc2(eh, el, t4);
-    cp_acc2(eh, el, t2);
-    cp_acc2(eh, el, part3);
-    cp_acc2(eh, el, t6);
-    cp_acc2(eh, el, t7);
-    float answer = x * cp_fmaf(cp_expf(eh), el, cp_expf(eh)) * a.qfac;
-    if (i == 3) sumUbarDbar = x * answer;
-    else if (i == 4) {
-      float inv = 1.f / (1.f + answer);
-      out[3] = sumUbarDbar * inv;
-      out[4] = sumUbarDbar * answer * inv;
-    } else {
-      out[i] = x * answer;
-    }
+    const CpCteqPoly& c = cteq[i];
+    const CpCteqQ a = cp_cteq_coef(c, lnQ, Q, invQ);
+    float ra = cp_cteq_answer(c, a, A), rb = cp_cteq_answer(c, a, B);
+    // parametrisation 4 is the dbar/ubar ratio; the others are x * answer
+    if (i != 4) { ra *= A.x; rb *= B.x; }
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (k == i) { fa[k] = ra; fb[k] = rb; }
   }
+  // ubar and dbar from (ubar + dbar) and dbar/ubar: PartonDistributions.cc:1053-1054
+  float ia = 1.f / (1.f + fa[4]), ib = 1.f / (1.f + fb[4]);
+  float sa = fa[3], sb = fb[3];
+  fa[3] = sa * ia; fa[4] = sa * fa[4] * ia;
+  fb[3] = sb * ib; fb[4] = sb * fb[4] * ib;
   // max(0, .) of PDF::xf (PartonDistributions.cc:133-180)
 #pragma unroll
-  for (int k = 0; k < 8; ++k) out[k] = out[k] > 0.f ? out[k] : 0.f;
+  for (int k = 0; k < 8; ++k) {
+    fa[k] = fa[k] > 0.f ? fa[k] : 0.f;
+    fb[k] = fb[k] > 0.f ? fb[k] : 0.f;
+  }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -266,7 +293,8 @@ struct CpPoint {
   float scale;   // K0 alpha_s^2 yMax zMax / tau: w = scale * channel sum
 };
 
-CP_HD float cp_had_eval(const CpHadParams& P, float x0, float x1, float x2, CpPoint& pt)
+CP_HD float cp_had_eval(const CpHadParams& P, const CpCteqPoly* cteq, float x0, float x1, float x2,
+                        CpPoint& pt)
 {
   // ln tau = (1 - x0) ln tauMin as a (hi, lo) pair: both factors carry their rounding
   float omx0, omx0l;
@@ -294,10 +322,7 @@ CP_HD float cp_had_eval(const CpHadParams& P, float x0, float x1, float x2, CpPo
   float lnx2 = lnTau * x1;
   float lnx2L = cp_fmaf(lnTau, x1, -lnx2) + lnTauL * x1;
   float alphaS = cp_alphas(P, P.kR * pT2);
-  CpCteqQ q[8];
-  cp_cteq_q(P, P.kF * pT2, q);
-  cp_cteq_x(P, q, lnx1, lnx1L, pt.fa);
-  cp_cteq_x(P, q, lnx2, lnx2L, pt.fb);
+  cp_cteq_pair(cteq, P.kF * pT2, lnx1, lnx1L, lnx2, lnx2L, pt.fa, pt.fb);
   cp_brackets(P, tp, up, pt.b);
   float B = cp_channel_sum(P.mask, pt.b, pt.fa, pt.fb);
   pt.k.tau = tau; pt.k.yMax = yMax; pt.k.zMax = zMax; pt.k.sH = sH; pt.k.omz = omz;
@@ -306,10 +331,11 @@ CP_HD float cp_had_eval(const CpHadParams& P, float x0, float x1, float x2, CpPo
   return pt.scale * B;
 }
 
-CP_HD float cp_had_weight(const CpHadParams& P, float x0, float x1, float x2, CpKin* kin)
+CP_HD float cp_had_weight(const CpHadParams& P, const CpCteqPoly* cteq, float x0, float x1, float x2,
+                          CpKin* kin)
 {
   CpPoint pt;
-  float w = cp_had_eval(P, x0, x1, x2, pt);
+  float w = cp_had_eval(P, cteq, x0, x1, x2, pt);
   if (kin) *kin = pt.k;
   return w;
 }

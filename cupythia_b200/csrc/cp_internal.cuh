@@ -50,6 +50,8 @@ struct cp_handle {
   int nb = 50;
   // VEGAS grid, FP64
   double* d_edges = nullptr;
+  // CTEQ5L coefficient records (device copy of P.cteq, staged into shared memory by kernels)
+  CpCteqPoly* d_cteq = nullptr;
   // scratch: per-block slots and reduced outputs
   double* d_slots = nullptr;
   size_t slots_cap = 0;           // doubles
@@ -151,6 +153,14 @@ __device__ __forceinline__ double cp_warp_max_d(double v)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+
+// Copies the 8 CTEQ5L coefficient records from global into shared memory (block-wide).
+__device__ __forceinline__ void cp_stage_cteq(CpCteqPoly* dst, const CpCteqPoly* src)
+{
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+  for (int k = threadIdx.x; k < (int)(8 * sizeof(CpCteqPoly) / 4); k += blockDim.x) d[k] = s[k];
 }
 
 // Deterministic add of v into a warp-private histogram h[bin]: lanes that share a bin are

@@ -1,11 +1,13 @@
 // cp_unweight.cu -- production pass: unweighting and on-device compaction into 64-byte records.
 //
-// One persistent kernel draws, maps and evaluates each point exactly like the VEGAS pass,
-// accepts it when u * w_max < w (cuPythia/07_unweighting_lhe/unweight_lhe.cu:54; overweight
-// events w > w_max are kept with weight w / w_max, as Pythia keeps them,
-// pythia8317/src/ProcessContainer.cc:383-385), and writes accepted events straight into a
-// dense array: one ballot per warp, one global atomic per warp, then each accepting lane stores
-// its 64-byte record as four 16-byte stores.  The reference instead writes flags and runs a
+// K1 draws, maps and evaluates each point exactly like the VEGAS pass, accepts it when
+// u * w_max < w (cuPythia/07_unweighting_lhe/unweight_lhe.cu:54; overweight events w > w_max
+// are kept with weight w / w_max, as Pythia keeps them, pythia8317/src/ProcessContainer.cc:
+// 383-385) and reserves a slot in the dense record array (one ballot and one global atomic per
+// warp).  K2 then runs over the reserved slots only, with every lane busy, re-evaluates those
+// points and writes their 64-byte records as four 16-byte stores.  Keeping the record builder
+// out of K1 keeps K1's code small (its instruction-cache footprint, not arithmetic, limited the
+// fused version) and its lanes converged.  The reference instead writes flags and runs a
 // separate library compaction pass (cuPythia/10_cub_compaction/cub_compaction.cu:76-80,
 // cuPythia/pipeline/generate.cu:97-104).
 //
@@ -21,31 +23,60 @@ struct UnwLaunch {
   uint32_t iter;
   int nb;
   const double* edges;
+  const CpCteqPoly* cteq;
   const double* wmax;          // device threshold
   CpEventRec* out;
   uint64_t capacity;
-  unsigned long long* counter; // events written so far (may exceed capacity: reported)
+  unsigned long long* counter; // events accepted so far (may exceed capacity: reported)
   double* slots;
 };
 
 static_assert(sizeof(CpEventRec) == 64, "event record must be 64 bytes");
 static_assert(sizeof(CpEventRec) == sizeof(cp_event), "C ABI record layout");
 
-__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_unweight(const CpHadParams P, const UnwLaunch L)
+struct CpMapped {
+  float x[3], jv;
+};
+
+__device__ __forceinline__ CpMapped cp_map_point(const float2 (*sEdge)[CP_MAX_BINS], int nb, const uint32_t wd[4])
 {
-  __shared__ float2 sEdge[3][CP_MAX_BINS];
-  __shared__ double sRed[CP_WARPS][7];
-  const int nb = L.nb;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  CpMapped m;
+  m.jv = 1.f;
+  const float nbf = (float)nb;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int bin;
+    float frac;
+    cp_bin_frac(wd[d], nb, bin, frac);
+    float2 e = sEdge[d][bin];
+    m.x[d] = fmaf(frac, e.y, e.x);
+    m.jv *= nbf * e.y;
+  }
+  return m;
+}
+
+__device__ __forceinline__ void cp_stage_edges(float2 (*sEdge)[CP_MAX_BINS], const double* edges, int nb)
+{
   for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
     int d = k / nb, b = k - d * nb;
-    const double* e = L.edges + d * (nb + 1);
+    const double* e = edges + d * (nb + 1);
     double lo = e[b], hi = e[b + 1];
     sEdge[d][b] = make_float2((float)lo, (float)(hi - lo));
   }
+}
+
+// K1: weight, accept, reserve a record slot (one ballot and one atomic per warp) and store the
+// point's in-call index and event weight in that slot; K2 fills in the rest of the record.
+__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const CpHadParams P, const UnwLaunch L)
+{
+  __shared__ float2 sEdge[3][CP_MAX_BINS];
+  __shared__ CpCteqPoly sCteq[8];
+  __shared__ double sRed[CP_WARPS][7];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  cp_stage_edges(sEdge, L.edges, L.nb);
+  cp_stage_cteq(sCteq, L.cteq);
   __syncthreads();
   const float wmax = (float)L.wmax[0];
-  const float nbf = (float)nb;
   const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
   const uint64_t gtid = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x;
   const uint64_t rounds = (L.n + stride - 1) / stride;
@@ -56,21 +87,11 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_unweight(cons
     const uint64_t p = r * stride + gtid;
     bool accept = false;
     float w = 0.f;
-    CpPoint pt;
-    uint32_t wd[4] = {0, 0, 0, 0};
     if (p < L.n) {
+      uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
-      float x[3], jv = 1.f;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        int bin;
-        float frac;
-        cp_bin_frac(wd[d], nb, bin, frac);
-        float2 e = sEdge[d][bin];
-        x[d] = fmaf(frac, e.y, e.x);
-        jv *= nbf * e.y;
-      }
-      w = cp_had_eval(P, x[0], x[1], x[2], pt) * jv;
+      CpMapped m = cp_map_point(sEdge, L.nb, wd);
+      w = cp_had_weight(P, sCteq, m.x[0], m.x[1], m.x[2], nullptr) * m.jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
       cp_kahan(s1, c1, w);
       cp_kahan(s2, c2, w * w);
@@ -84,24 +105,17 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_unweight(cons
     base = __shfl_sync(0xffffffffu, base, 0);
     if (accept) {
       const uint64_t slot = base + __popc(ball & ((1u << lane) - 1u));
-      float ew = w > wmax ? w / wmax : 1.f;
+      const float ew = w > wmax ? w / wmax : 1.f;
       ++nacc;
       nover += w > wmax ? 1u : 0u;
       cp_kahan(se, ce, ew);
       if (slot < L.capacity) {
-        uint32_t w2[4];
-        cp_point_words(L.seed, L.point0 + p, L.iter, 1, w2);
-        CpEventRec ev;
-        cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), ew,
-                      (uint32_t)(L.point0 + p), ev);
-        const uint4* src = reinterpret_cast<const uint4*>(&ev);
-        uint4* dst = reinterpret_cast<uint4*>(L.out + slot);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dst[q] = src[q];
+        // weight, pt_hat, process, point: the last 16 bytes of the record
+        uint4* dst = reinterpret_cast<uint4*>(L.out + slot) + 3;
+        *dst = make_uint4(__float_as_uint(ew), 0u, 0u, (uint32_t)p);
       }
     }
   }
-  // block reduction (FP32 compensated per thread, FP64 across warps)
   double v[7] = {(double)s1 - (double)c1, (double)s2 - (double)c2, (double)wm, (double)nbad,
                  (double)nacc, (double)se - (double)ce, (double)nover};
 #pragma unroll
@@ -112,11 +126,42 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_unweight(cons
   if (threadIdx.x == 0) {
     double* slot = L.slots + (size_t)blockIdx.x * CP_UNW_SLOT;
     for (int k = 0; k < 7; ++k) {
-      double a = (k == 2) ? 0.0 : 0.0;
+      double a = 0.0;
       for (int q = 0; q < CP_WARPS; ++q) a = (k == 2) ? fmax(a, sRed[q][k]) : a + sRed[q][k];
       slot[k] = a;
     }
     slot[7] = 0.0;
+  }
+}
+
+// K2: dense pass over the reserved slots: re-evaluate the accepted point, pick process and
+// flavours, build the lab-frame kinematics, store the full 64-byte record.
+__global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, const UnwLaunch L)
+{
+  __shared__ float2 sEdge[3][CP_MAX_BINS];
+  __shared__ CpCteqPoly sCteq[8];
+  cp_stage_edges(sEdge, L.edges, L.nb);
+  cp_stage_cteq(sCteq, L.cteq);
+  __syncthreads();
+  const unsigned long long acc = *L.counter;
+  const uint64_t nrec = acc < L.capacity ? acc : L.capacity;
+  for (uint64_t k = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x; k < nrec;
+       k += (uint64_t)gridDim.x * CP_THREADS) {
+    const uint4 tail = reinterpret_cast<const uint4*>(L.out + k)[3];
+    const uint64_t point = L.point0 + tail.w;
+    uint32_t wd[4], w2[4];
+    cp_point_words(L.seed, point, L.iter, 0, wd);
+    cp_point_words(L.seed, point, L.iter, 1, w2);
+    CpMapped m = cp_map_point(sEdge, L.nb, wd);
+    CpPoint pt;
+    cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt);
+    CpEventRec ev;
+    cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]),
+                  __uint_as_float(tail.x), (uint32_t)point, ev);
+    const uint4* src = reinterpret_cast<const uint4*>(&ev);
+    uint4* dst = reinterpret_cast<uint4*>(L.out + k);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) dst[q] = src[q];
   }
 }
 
@@ -126,7 +171,7 @@ static int unw_blocks(cp_handle* h)
 {
   static int per_sm = -1;
   if (per_sm < 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_had_unweight, CP_THREADS, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unw_accept, CP_THREADS, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
   }
@@ -140,14 +185,20 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   const int blocks = unw_blocks(h);
   int rc = cp_ensure_slots(h, (size_t)blocks * CP_UNW_SLOT);
   if (rc) return rc;
+  if (n > (1ull << 32)) return cp_fail(h, CP_ERR_INVALID, "at most 2^32 points per production call");
   UnwLaunch L;
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.nb = h->nb;
-  L.edges = h->d_edges; L.wmax = h->d_wmax; L.out = reinterpret_cast<CpEventRec*>(out);
+  L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;
+  L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
-  k_had_unweight<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
-  CP_LAUNCH_CHECK(h, "k_had_unweight");
+  k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+  CP_LAUNCH_CHECK(h, "k_unw_accept");
   k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
+  if (capacity) {
+    k_unw_build<<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
+    CP_LAUNCH_CHECK(h, "k_unw_build");
+  }
   return CP_OK;
 }
 

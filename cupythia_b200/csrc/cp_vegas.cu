@@ -17,6 +17,7 @@ struct HadLaunch {
   uint32_t iter, stream;
   int nb;
   const double* edges;
+  const CpCteqPoly* cteq;
   double* slots;   // gridDim.x * (CP_SLOT_HEAD + 3 nb)
   float* w_out;    // optional per-point weights
   float* x_out;    // optional per-point mapped x (3 per point)
@@ -30,7 +31,9 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
   __shared__ float sHist[CP_WARPS][3][CP_MAX_BINS];
   __shared__ float sRed[CP_WARPS][6];
   __shared__ unsigned sQ[CP_QBINS];
+  __shared__ CpCteqPoly sCteq[8];
   const int nb = L.nb;
+  cp_stage_cteq(sCteq, L.cteq);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
     int d = k / nb, b = k - d * nb;
@@ -68,7 +71,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
         x[d] = fmaf(frac, e.y, e.x);
         jv *= nbf * e.y;
       }
-      w = cp_had_weight(P, x[0], x[1], x[2], nullptr) * jv;
+      w = cp_had_weight(P, sCteq, x[0], x[1], x[2], nullptr) * jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
       cp_kahan(s1, c1, w);
       cp_kahan(s2, c2, w * w);
@@ -196,11 +199,15 @@ __global__ void k_refine(double* edges, const double* red, int nb, double n, dou
 }
 
 // FP32 integrand at caller-supplied x
-__global__ void k_weight_at(const CpHadParams P, const float* __restrict__ x, int64_t n, float* w)
+__global__ void k_weight_at(const CpHadParams P, const CpCteqPoly* cteq_g, const float* __restrict__ x,
+                            int64_t n, float* w)
 {
+  __shared__ CpCteqPoly sCteq[8];
+  cp_stage_cteq(sCteq, cteq_g);
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    w[i] = cp_had_weight(P, x[3 * i], x[3 * i + 1], x[3 * i + 2], nullptr);
+    w[i] = cp_had_weight(P, sCteq, x[3 * i], x[3 * i + 1], x[3 * i + 2], nullptr);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -216,6 +223,7 @@ static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, 
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.stream = stream;
   L.nb = h->nb; L.edges = h->d_edges; L.slots = h->d_slots; L.w_out = w_out; L.x_out = x_out;
   L.qhist = h->d_qhist;
+  L.cteq = h->d_cteq;
   CP_CUDA(h, cudaMemsetAsync(h->d_qhist, 0, sizeof(unsigned long long) * CP_QBINS, h->stream));
   h->last_n = n;
   if (w_out || x_out) k_had_accum<true><<<h->had_blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
@@ -328,7 +336,7 @@ extern "C" int cp_weight_at(cp_handle* h, const float* x, int64_t n, float* w)
   if (n == 0) return CP_OK;
   int blocks = (int)((n + CP_THREADS - 1) / CP_THREADS);
   if (blocks > h->num_sms * 16) blocks = h->num_sms * 16;
-  k_weight_at<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, x, n, w);
+  k_weight_at<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, h->d_cteq, x, n, w);
   CP_LAUNCH_CHECK(h, "k_weight_at");
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return CP_OK;

