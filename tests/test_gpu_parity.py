@@ -158,7 +158,8 @@ def test_iteration_sums_and_histogram_match_oracle(integ, orc):
     integ.integrate(3, 1 << 20, alpha=1.5)
     grid = integ.grid.copy()
     n = 1 << 17
-    w = integ.point_weights(0, n, 5).cpu().numpy().astype(np.float64)
+    w, xw = integ.point_weights(0, n, 5, with_x=True)
+    w = w.cpu().numpy().astype(np.float64)
     r = integ.iteration(n, 5, alpha=1.5)
     assert r["n_bad"] == 0
     assert abs(r["sum_w"] / w.sum() - 1) < 1e-6
@@ -166,8 +167,7 @@ def test_iteration_sums_and_histogram_match_oracle(integ, orc):
     h = integ.last_histogram()
     # per-bin sums of w^2 against FP64 weights at the x the kernel evaluated (the FP64 map of the
     # same words differs from the FP32 one by an ulp of x, which the t-channel pole amplifies)
-    w2, x = integ.point_weights(0, n, 5, with_x=True)
-    x = x.cpu().numpy()
+    x = xw.cpu().numpy()
     words = integ.philox_words(integ.cfg.seed, 0, n, 5, 0)
     m = (words[:, :3] >> 8).astype(np.uint64) * integ.nb
     bins = (m >> 24).astype(np.int64)
