@@ -10,6 +10,7 @@
 // and a third refines the grid in FP64 on the device, so iterations chain on the stream
 // without host round trips (the reference round-trips through the host every iteration:
 // cuPythia/11_vegas_importance/vegas.cu:107-124).
+#include <mutex>
 #include "cp_internal.cuh"
 
 struct HadLaunch {
@@ -366,4 +367,101 @@ extern "C" int cp_weight_quantile(cp_handle* h, double q, double* w_q)
     *w_q = v[0];
   }
   return CP_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free VEGAS pass.
+//
+// For callers that must not allocate device memory: code running inside a CUDA graph that is
+// being captured, under a caller-owned memory pool or a fixed memory budget, or embedded in a
+// host framework that owns every device allocation (a Pythia plugin sharing the GPU with its
+// host program).  This entry point creates no handle and calls no cudaMalloc / cudaFree: its
+// scratch (the per-block partial sums, the weight histogram and the CTEQ5L coefficient
+// records) lives in the file-scope array below, which every GPU that loads this library keeps
+// until the process exits.
+//
+// Limits: the partial sums hold at most CP_NOALLOC_MAX_BLOCKS blocks of CP_SLOT_HEAD + 3 *
+// CP_MAX_BINS doubles, so n_bins above CP_MAX_BINS is rejected; the grid is capped at
+// CP_NOALLOC_MAX_BLOCKS blocks (296 are used on a B200).  Total: 1,623,296 bytes per device.
+// Every call shares the array and it keeps the last call's contents; the weight histogram is
+// cleared at the start of each call and every partial-sum slot is rewritten.  Calls that overlap
+// on the GPU (different streams, or several host threads) race on the array and must not be
+// issued; calls in one stream are ordered and safe.
+// ------------------------------------------------------------------------------------------
+#define CP_NOALLOC_MAX_BLOCKS 512
+#define CP_NOALLOC_SLOT_DOUBLES (CP_NOALLOC_MAX_BLOCKS * (CP_SLOT_HEAD + 3 * CP_MAX_BINS))
+#define CP_NOALLOC_CTEQ_DOUBLES 160   // 8 CpCteqPoly records (1056 bytes), rounded up
+#define CP_NOALLOC_DOUBLES (CP_NOALLOC_CTEQ_DOUBLES + CP_QBINS + CP_NOALLOC_SLOT_DOUBLES)
+
+static __device__ __align__(256) double cp_noalloc_scratch[CP_NOALLOC_DOUBLES];
+static_assert(sizeof(CpCteqPoly) * 8 <= CP_NOALLOC_CTEQ_DOUBLES * sizeof(double), "CTEQ records fit");
+
+namespace {
+struct NoallocDevice {
+  double* scratch = nullptr;   // device address of cp_noalloc_scratch on this device
+  int blocks = 0;
+  int ready = 0;
+};
+const int CP_NOALLOC_MAX_DEVICES = 64;
+NoallocDevice g_noalloc[CP_NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mutex;
+}  // namespace
+
+extern "C" int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, uint32_t iter,
+                                     const double* edges_dev, double* sums_dev, void* cuda_stream)
+{
+  if (!cfg || !edges_dev || !sums_dev) return CP_ERR_INVALID;
+  if (cfg->n_bins < 2 || cfg->n_bins > CP_MAX_BINS) return CP_ERR_INVALID;   // beyond the scratch
+  if (n_points < 2) return CP_ERR_INVALID;
+  if (cfg->device < 0 || cfg->device >= CP_NOALLOC_MAX_DEVICES) return CP_ERR_INVALID;
+  CpHadConfig hc{cfg->sqrt_s, cfg->pt_hat_min, cfg->alphas_mz, cfg->k_ren, cfg->k_fac,
+                 cfg->convert2mb, cfg->n_quark_in, cfg->n_quark_new, cfg->proc_mask};
+  CpHadParams P;
+  if (cp_build_had_params(hc, P) || (cfg->proc_mask & ~CP_PROC_ALL) || cfg->proc_mask == 0)
+    return CP_ERR_INVALID;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return CP_ERR_CUDA;
+  if (prev != cfg->device && cudaSetDevice(cfg->device) != cudaSuccess) return CP_ERR_CUDA;
+  cudaStream_t stream = (cudaStream_t)cuda_stream;
+  int rc = CP_OK;
+  NoallocDevice& D = g_noalloc[cfg->device];
+  {
+    // once per device, with that device current: the array's device address, the launch shape
+    // and the (configuration-independent) CTEQ5L coefficient records
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!D.ready) {
+      void* ptr = nullptr;
+      int nsm = 0, per_sm = 0;
+      if (cudaGetSymbolAddress(&ptr, cp_noalloc_scratch) != cudaSuccess || !ptr ||
+          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_had_accum<false>, CP_THREADS, 0) != cudaSuccess ||
+          cudaMemcpy(ptr, P.cteq, sizeof(CpCteqPoly) * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = CP_ERR_CUDA;
+      } else {
+        D.scratch = (double*)ptr;
+        int blocks = nsm * (per_sm > 0 ? per_sm : 1);
+        D.blocks = blocks < CP_NOALLOC_MAX_BLOCKS ? blocks : CP_NOALLOC_MAX_BLOCKS;
+        D.ready = 1;
+      }
+    }
+  }
+  if (rc == CP_OK) {
+    double* base = D.scratch;
+    unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base + CP_NOALLOC_CTEQ_DOUBLES);
+    double* slots = base + CP_NOALLOC_CTEQ_DOUBLES + CP_QBINS;
+    const int nb = cfg->n_bins, width = CP_SLOT_HEAD + 3 * nb;
+    HadLaunch L;
+    L.seed = cfg->seed; L.point0 = 0; L.n = n_points; L.iter = iter; L.stream = 0;
+    L.nb = nb; L.edges = edges_dev; L.cteq = reinterpret_cast<const CpCteqPoly*>(base);
+    L.slots = slots; L.w_out = nullptr; L.x_out = nullptr; L.qhist = qhist;
+    if (cudaMemsetAsync(qhist, 0, sizeof(unsigned long long) * CP_QBINS, stream) != cudaSuccess) {
+      rc = CP_ERR_CUDA;
+    } else {
+      k_had_accum<false><<<D.blocks, CP_THREADS, 0, stream>>>(P, L);
+      k_reduce_slots<0><<<(width + 7) / 8, 8 * 32, 0, stream>>>(slots, D.blocks, width, sums_dev);
+      if (cudaGetLastError() != cudaSuccess) rc = CP_ERR_CUDA;
+    }
+  }
+  if (prev != cfg->device) cudaSetDevice(prev);
+  return rc;
 }

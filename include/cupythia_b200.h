@@ -172,6 +172,20 @@ int cp_weight_at(cp_handle* h, const float* x_dev, int64_t n, float* w_dev);
  * n_bad, then the per-bin sums of w^2 of each dimension (the refinement's input). */
 int cp_last_histogram(cp_handle* h, double* out_host);
 
+/* One VEGAS pass (the body of cp_vegas_iteration, without refinement) that allocates nothing.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc: code inside a CUDA
+ * graph being captured, under a caller-owned memory pool or fixed memory budget, or embedded in
+ * a host program that owns every device allocation.  No handle is created; the scratch (block
+ * partial sums for up to 512 blocks, the weight histogram, the CTEQ5L records: 1,623,296 bytes)
+ * is a file-scope device array that every GPU loading this library keeps until exit.
+ * Inputs: cfg (host), the grid edges_dev (3 x (n_bins + 1) doubles).  Output: sums_dev (4 + 3
+ * n_bins doubles, the layout of cp_last_histogram).  n_bins > CP_MAX_BINS is rejected
+ * (CP_ERR_INVALID).  The first call on a device sets up (symbol address, coefficient copy) and
+ * should come before any stream capture.  The array keeps the last call's contents and the
+ * weight histogram is cleared per call; calls that overlap on the GPU race on it. */
+int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, uint32_t iter,
+                          const double* edges_dev, double* sums_dev, void* cuda_stream);
+
 /* ---------------------------------------------------------------- unweighting ------ */
 /* q-quantile of the weights of the last VEGAS pass (integer weight histogram, ~2% bins,
  * rounded up), stored as the handle's unweighting threshold; the production run uses
