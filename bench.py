@@ -261,7 +261,7 @@ def run_ours(a):
 
 # FP32 FLOP per point of the fused integrand (FADD + FMUL + 2 FFMA, thread level), from the ncu
 # SASS counters of k_unw_accept on a 2^22-point pass; see profiles/.
-FP32_FLOP_PER_POINT = 1500.0
+FP32_FLOP_PER_POINT = 3278.0
 
 
 def fp32_peak_tflops(it, stream):

@@ -168,6 +168,38 @@ class Integrator:
         return {"sum_w": a[0], "sum_w2": a[1], "w_max": a[2], "n_bad": a[3],
                 "hist": a[4:].reshape(3, self.nb)}
 
+    # ------------------------------------------------------------------ adjoint
+    def adjoint(self, n_points, iteration=0, stream=0):
+        """Gradients of sigma and Var[w] (see cp_adjoint); edge gradients as (3, nb+1) arrays."""
+        g = cp_grad()
+        ne = 3 * (self.nb + 1)
+        ds = np.zeros(ne)
+        dv = np.zeros(ne)
+        self._check(self.lib.cp_adjoint(self.h, n_points, iteration, stream, C.byref(g),
+                                        ds.ctypes.data_as(C.c_void_p), dv.ctypes.data_as(C.c_void_p)))
+        return {"sigma": g.sigma, "var": g.var, "dsigma": list(g.dsigma), "dvar": list(g.dvar),
+                "params": ["alphas_mz", "k_ren", "pt_hat_min"], "n_bad": g.n_bad,
+                "dsigma_dedges": ds.reshape(3, -1), "dvar_dedges": dv.reshape(3, -1)}
+
+    def adapt_gradient(self, steps, n_points, lr=0.4, iteration0=0):
+        """Variance-gradient adaptation: `steps` device gradient steps, halving lr whenever the
+        batch variance (measured at the pre-step grid of each step) rises. Returns the history."""
+        hist = []
+        prev = None
+        for s in range(steps):
+            r = self.gradient_step(n_points, iteration=iteration0 + s, lr=lr)
+            rel = r["var"] / r["sigma"] ** 2
+            if prev is not None and rel > prev:
+                lr *= 0.5
+            prev = rel
+            hist.append({"step": s, "lr": lr, "rel_var": rel, "sigma": r["sigma"]})
+        return hist
+
+    def gradient_step(self, n_points, iteration=0, lr=0.5):
+        g = cp_grad()
+        self._check(self.lib.cp_vegas_gradient_step(self.h, n_points, iteration, lr, C.byref(g)))
+        return {"sigma": g.sigma, "var": g.var}
+
     # ------------------------------------------------------------------ unweighting
     def weight_quantile(self, q=0.999):
         v = C.c_double()

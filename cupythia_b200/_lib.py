@@ -110,6 +110,8 @@ SIGNATURES = {
     "cp_set_wmax": [_P, _d],
     "cp_unweight": [_P, _u64, _u32, _P, _u64, C.POINTER(cp_unweight_result)],
     "cp_generate_host": [_P, _u64, _u32, _u64, _P, _u64, C.POINTER(cp_unweight_result)],
+    "cp_adjoint": [_P, _u64, _u32, _u32, C.POINTER(cp_grad), _P, _P],
+    "cp_vegas_gradient_step": [_P, _u64, _u32, _d, C.POINTER(cp_grad)],
     "cp_measure_peaks": [_P, C.POINTER(_d), C.POINTER(_d)],
     "cp_vegas_pass_noalloc": [C.POINTER(cp_config), _u64, _u32, _P, _P, _P],
     "cp_partonic_integrate": [_P, _d, _d, _d, _d, _u64, _u64, C.POINTER(cp_result)],

@@ -180,16 +180,17 @@ __device__ __forceinline__ void cp_warp_hist_add(float* h, int bin, float v)
   if (lane == leader) h[bin] += sum;
 }
 
-// out[k] = sum over blocks of slots[b][k] (k != 2) or max (k == 2), fixed order, FP64.
+// out[k] = sum over blocks of slots[b][k], or their max for k == max_col; fixed order, FP64.
 // One warp per output element.
 template <int UNUSED>
-__global__ void k_reduce_slots(const double* __restrict__ slots, int nblocks, int width, double* out)
+__global__ void k_reduce_slots(const double* __restrict__ slots, int nblocks, int width, double* out,
+                               int max_col = 2)
 {
   const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (k >= width) return;
   double acc = 0.0;
-  if (k == 2) {
+  if (k == max_col) {
     for (int b = lane; b < nblocks; b += 32) acc = fmax(acc, slots[(size_t)b * width + k]);
     acc = cp_warp_max_d(acc);
   } else {

@@ -221,6 +221,19 @@ int cp_partonic_splitmix(cp_handle* h, double sqrt_shat, double alphas, double c
 int cp_partonic_weights(cp_handle* h, double sqrt_shat, double alphas, double cmax, double conv,
                         uint64_t seed, uint64_t point0, uint64_t n, double* w_dev);
 
+/* ---------------------------------------------------------------- adjoint ---------- */
+/* Gradients of the estimator over points [0, n_points) of counter (iter, stream): d sigma and
+ * d Var[w] with respect to alpha_s(mZ), k_ren and pT_hat_min (out), and to the 3 x (n_bins + 1)
+ * grid edges (host arrays, may be NULL), exact at fixed random numbers (forward mode, FP32).
+ * No reference counterpart (the reference has no derivative code); checked against central
+ * finite differences of cp_vegas_iteration / cp_point_weights and the FP64 CPU adjoint. */
+int cp_adjoint(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream, cp_grad* out_host,
+               double* dsigma_dedges_host, double* dvar_dedges_host);
+/* One variance-gradient grid update on the device: the adjoint over n_points points, then
+ * ln(bin width) -= lr * G / max|G|, G = dVar/dln(width), per dimension (the most sensitive bin
+ * changes by exp(+-lr)); the alternative to the classic refinement of cp_vegas_iteration. */
+int cp_vegas_gradient_step(cp_handle* h, uint64_t n_points, uint32_t iter, double lr, cp_grad* out_host);
+
 /* ---------------------------------------------------------------- measurement ------ */
 /* FP32 FMA and MUFU (ex2) throughput of the device from dependency-free microbenchmarks:
  * TFLOP/s (2 per FMA) and Tops/s.  No reference counterpart: the integrand's roofline

@@ -1,6 +1,7 @@
 // fp32_probe.cc -- host build of the device integrand header (cupythia_b200/csrc/cp_integrand.cuh)
 // used by the CPU test suite to check the FP32 formulation against the FP64 oracle without a GPU.
 #include "../cupythia_b200/csrc/cp_params.h"
+#include "../cupythia_b200/csrc/cp_dual.cuh"
 
 extern "C" {
 int probe_had_weights(double sqrtS, double pTmin, double aSmZ, double kR, double kF, double conv,
@@ -19,6 +20,29 @@ int probe_pdf(double aSmZ, float lnx, float Q2, float* out8)
   if (cp_build_had_params(c, P)) return 1;
   float other[8];
   cp_cteq_pair(P.cteq, Q2, lnx, 0.f, lnx, 0.f, out8, other);
+  return 0;
+}
+// value and derivatives (d/dx0, d/dx1, d/dx2, d/dalpha_s(mZ), d/dk_ren, d/dpT_hat_min) of f * J_base
+// at one point, from the dual-number integrand of the adjoint kernel
+int probe_had_grad(double sqrtS, double pTmin, double aSmZ, double kR, const float* x, double* out7)
+{
+  CpHadConfig c{sqrtS, pTmin, aSmZ, kR, 1.0, 0.389380, 5, 3, 31};
+  CpHadParams P;
+  if (cp_build_had_params(c, P)) return 1;
+  typedef CpDual<6> D;
+  CpHadParamsT<D> Q;
+  Q.lnTauMin = cp_dconst<6>((float)log(4.0 * pTmin * pTmin / (sqrtS * sqrtS)));
+  Q.lnTauMin.d[5] = (float)(2.0 / pTmin);
+  Q.kR = cp_dconst<6>((float)kR);
+  Q.kR.d[4] = 1.f;
+  const double b0[4] = {27.0, 25.0, 23.0, 21.0};
+  for (int k = 0; k < 4; ++k) {
+    Q.lnL2[k] = cp_dconst<6>(P.lnL2[k]);
+    Q.lnL2[k].d[3] = (float)(12.0 * M_PI / (b0[k] * aSmZ * aSmZ));
+  }
+  D w = cp_had_weight_t<D>(P, Q, P.cteq, cp_dvar<6>(x[0], 0), cp_dvar<6>(x[1], 1), cp_dvar<6>(x[2], 2));
+  out7[0] = w.v;
+  for (int k = 0; k < 6; ++k) out7[1 + k] = w.d[k];
   return 0;
 }
 void probe_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t* out)

@@ -58,3 +58,26 @@ def test_probe_philox_matches_oracle(probe, orc):
         ref = (C.c_uint32 * 4)()
         orc.lib().cpo_philox4x32_10((C.c_uint32 * 4)(*c[:4]), (C.c_uint32 * 2)(*c[4:]), ref)
         assert list(out) == list(ref)
+
+
+def test_dual_number_gradients_match_complex_step(probe, orc):
+    """The adjoint kernel's forward-mode integrand (cp_dual.cuh) against the FP64 complex-step
+    derivatives of the oracle, at the same FP32 points."""
+    L = orc.lib()
+    probe.probe_had_grad.argtypes = [C.c_double] * 4 + [C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(9)
+    cfg = orc.had_cfg()
+    worst = 0.0
+    for _ in range(400):
+        x = rng.uniform(0.02, 0.98, 3).astype(np.float32)
+        got = np.zeros(7)
+        assert probe.probe_had_grad(13000., 20., .13, 1., x.ctypes.data, got.ctypes.data) == 0
+        ref = (C.c_double * 7)()
+        L.cpo_had_weight_grad(C.byref(cfg), orc.dptr(x.astype(np.float64)), ref)
+        ref = np.array(ref[:])
+        assert abs(got[0] / ref[0] - 1) < 1e-4
+        # derivative scale: |w| per unit of each variable (x in [0,1], alpha_s ~ 0.1, k ~ 1, pT ~ 20)
+        scale = np.abs(ref[0]) * np.array([1, 1, 1, 1 / 0.13, 1.0, 1 / 20.0])
+        err = np.abs(got[1:] - ref[1:]) / (np.abs(ref[1:]) + 1e-3 * scale)
+        worst = max(worst, err.max())
+    assert worst < 2e-3, worst
