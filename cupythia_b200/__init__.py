@@ -200,6 +200,43 @@ class Integrator:
         self._check(self.lib.cp_vegas_gradient_step(self.h, n_points, iteration, lr, C.byref(g)))
         return {"sigma": g.sigma, "var": g.var}
 
+    # ------------------------------------------------------------------ learned proposal
+    def flow_init(self, seed=7):
+        self._check(self.lib.cp_flow_init(self.h, seed))
+
+    @property
+    def flow_params(self):
+        n = self.lib.cp_flow_num_params()
+        out = np.zeros(n, np.float32)
+        self._check(self.lib.cp_flow_get_params(self.h, out.ctypes.data_as(C.c_void_p), n))
+        return out
+
+    @flow_params.setter
+    def flow_params(self, p):
+        p = np.ascontiguousarray(np.asarray(p, np.float32))
+        self._check(self.lib.cp_flow_set_params(self.h, p.ctypes.data_as(C.c_void_p), p.size))
+
+    def flow_sample(self, point0, n, iteration=0, stream=0):
+        torch = _torch()
+        out = torch.empty((n, 4), dtype=torch.float32, device=self.device)
+        self._check(self.lib.cp_flow_sample(self.h, point0, n, iteration, stream, _ptr(out)))
+        return out
+
+    def flow_enable(self, on=True):
+        self._check(self.lib.cp_flow_enable(self.h, 1 if on else 0))
+
+    def flow_train(self, steps, batch=65536, lr=1e-3):
+        loss = np.zeros(steps)
+        self._check(self.lib.cp_flow_train(self.h, steps, batch, lr, loss.ctypes.data_as(C.c_void_p)))
+        return loss
+
+    def flow_loss_grad(self, batch, iteration):
+        n = self.lib.cp_flow_num_params()
+        g = np.zeros(n, np.float32)
+        loss = C.c_double()
+        self._check(self.lib.cp_flow_loss_grad(self.h, batch, iteration, g.ctypes.data_as(C.c_void_p), C.byref(loss)))
+        return g, loss.value
+
     # ------------------------------------------------------------------ unweighting
     def weight_quantile(self, q=0.999):
         v = C.c_double()

@@ -112,6 +112,14 @@ SIGNATURES = {
     "cp_generate_host": [_P, _u64, _u32, _u64, _P, _u64, C.POINTER(cp_unweight_result)],
     "cp_adjoint": [_P, _u64, _u32, _u32, C.POINTER(cp_grad), _P, _P],
     "cp_vegas_gradient_step": [_P, _u64, _u32, _d, C.POINTER(cp_grad)],
+    "cp_flow_num_params": [],
+    "cp_flow_init": [_P, _u64],
+    "cp_flow_get_params": [_P, _P, _i],
+    "cp_flow_set_params": [_P, _P, _i],
+    "cp_flow_sample": [_P, _u64, _u64, _u32, _u32, _P],
+    "cp_flow_enable": [_P, _i],
+    "cp_flow_train": [_P, _i, _u64, _d, _P],
+    "cp_flow_loss_grad": [_P, _u64, _u32, _P, _P],
     "cp_measure_peaks": [_P, C.POINTER(_d), C.POINTER(_d)],
     "cp_vegas_pass_noalloc": [C.POINTER(cp_config), _u64, _u32, _P, _P, _P],
     "cp_partonic_integrate": [_P, _d, _d, _d, _d, _u64, _u64, C.POINTER(cp_result)],

@@ -1,0 +1,611 @@
+// cp_flow_train.cu -- training of the learned proposal on weights the integrator generates.
+//
+// Objective: the relative second moment of the weights, L = <w^2> / <w>^2 (= 1 + Var[w]/sigma^2),
+// minimised over the flow parameters theta at fixed VEGAS grid.  With w = f(x(x_v; theta)) J,
+// x_v the VEGAS-mapped point (fixed by the random numbers), f the integrand and J the VEGAS
+// Jacobian times |dx/dx_v|, the pathwise gradient is
+//   dL/dtheta = 2/(B sigma^2) sum_points w^2 (d ln f/dx . dx/dtheta + d ln J/dtheta),
+// so one step is: flow forward (saving each coupling's input) -> integrand value and d ln f/dx
+// (forward-mode FP32 duals, the adjoint machinery) -> backward through sigmoid and couplings
+// with each coupling's MLP recomputed on the tensor cores -> weight-gradient GEMMs on the tensor
+// cores -> Adam (FP32 master weights) -> BF16 fragment repack.
+#include "cp_dual.cuh"
+#include "cp_flow.cuh"
+#include "cp_internal.cuh"
+
+int cp_flow_ensure(cp_handle* h);
+int cp_flow_repack(cp_handle* h);
+
+struct FlowTrainBufs {
+  float* zs;           // [B][4][3] input z of each coupling
+  float4* vj;          // [B] (v0, v1, v2, ln J)
+  float4* wg;          // [B] (w, d ln F / dv)
+  uint16_t* X;         // [4][B][16]  bf16 MLP inputs
+  uint16_t* H1;        // [4][B][64]  bf16 post-ReLU hidden 1
+  uint16_t* H2;        // [4][B][64]  bf16 post-ReLU hidden 2
+  uint16_t* D1;        // [4][B][64]  bf16 d pre-activation 1
+  uint16_t* D2;        // [4][B][64]  bf16 d pre-activation 2
+  uint16_t* DO;        // [4][B][16]  bf16 d outputs (s_raw, t)
+  double* sums;        // [2] sum w, sum w^2 of the batch
+  double* loss;        // per-step relative second moment
+};
+
+__device__ __forceinline__ float cp_bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float cp_bf_hi(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+
+// ------------------------------------------------------------------------------------------
+// 1. forward, saving the input z of every coupling
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(CP_THREADS) k_flow_fwd_train(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g,
+                                                               const double* __restrict__ edges, int nb,
+                                                               uint64_t seed, uint32_t iter, uint32_t stream, uint64_t n,
+                                                               float* __restrict__ zs, float4* __restrict__ vj)
+{
+  extern __shared__ uint2 sPk[];
+  float* sBias = reinterpret_cast<float*>(sPk + CP_FLOW_NC * CP_FLOW_P_FWD);
+  __shared__ float2 sEdge[3][CP_MAX_BINS];
+  for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
+    const int d = k / nb, b = k - d * nb;
+    sEdge[d][b] = make_float2((float)edges[d * (nb + 1) + b], (float)(edges[d * (nb + 1) + b + 1] - edges[d * (nb + 1) + b]));
+  }
+  for (int c = 0; c < CP_FLOW_NC; ++c)
+    for (int e = threadIdx.x; e < CP_FLOW_P_FWD; e += CP_THREADS) sPk[c * CP_FLOW_P_FWD + e] = pk_g[c * CP_FLOW_P_PER + e];
+  for (int j = threadIdx.x; j < CP_FLOW_NC * CP_FLOW_NB; j += CP_THREADS) sBias[j] = bias_g[j];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
+  const uint64_t rounds = (n + stride - 1) / stride;
+  for (uint64_t r = 0; r < rounds; ++r) {
+    const uint64_t p = r * stride + (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x;
+    const bool active = p < n;
+    float z[3], jv = 1.f, logdet = 0.f;
+    uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
+    if (active) cp_point_words(seed, p, iter, stream, w);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int bin;
+      logdet += cp_flow_logit(cp_flow_vegas_in(sEdge[d], nb, w[d], jv, bin), z[d]);
+    }
+    logdet += logf(jv);
+#pragma unroll 1
+    for (int c = 0; c < CP_FLOW_NC; ++c) {
+      if (active)
+        for (int d = 0; d < 3; ++d) zs[(p * CP_FLOW_NC + c) * 3 + d] = z[d];
+      const CpCoupling k = cp_coupling(c);
+      const float* b = sBias + c * CP_FLOW_NB;
+      float o0[4], o1[4], o[4];
+      cp_flow_mlp_tile(sPk + c * CP_FLOW_P_FWD, b, b + 64, b + 128, z[k.cin[0]], z[k.cin[1]], k.nin, 0, o0);
+      cp_flow_mlp_tile(sPk + c * CP_FLOW_P_FWD, b, b + 64, b + 128, z[k.cin[0]], z[k.cin[1]], k.nin, 16, o1);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) o[q] = lane >= 16 ? o1[q] : o0[q];
+      for (int j = 0; j < k.nt; ++j) {
+        const float s = CP_FLOW_S * tanhf(o[j] / CP_FLOW_S);
+        z[k.tr[j]] = fmaf(z[k.tr[j]], expf(s), o[k.nt + j]);
+        logdet += s;
+      }
+    }
+    float v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) logdet += cp_flow_sigmoid(z[d], v[d]);
+    if (active) vj[p] = make_float4(v[0], v[1], v[2], logdet);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// 2. integrand value and d ln f / dx at the flow's points (3-tangent duals), batch sums
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_flow_igrad(const CpHadParams P, const CpCteqPoly* __restrict__ cteq_g,
+                                                    uint64_t n, float lnTauMin, const float4* __restrict__ vj,
+                                                    float4* __restrict__ wg, double* __restrict__ slots)
+{
+  __shared__ CpCteqPoly sCteq[8];
+  __shared__ double sRed[4][2];
+  cp_stage_cteq(sCteq, cteq_g);
+  __syncthreads();
+  typedef CpDual<3> D3;
+  CpHadParamsT<D3> Q;
+  Q.lnTauMin = cp_dconst<3>(lnTauMin);
+  Q.kR = cp_dconst<3>(P.kR);
+  for (int k = 0; k < 4; ++k) Q.lnL2[k] = cp_dconst<3>(P.lnL2[k]);
+  double s1 = 0.0, s2 = 0.0;
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+    const float4 f = vj[p];
+    D3 F = cp_had_weight_t<D3>(P, Q, sCteq, cp_dvar<3>(f.x, 0), cp_dvar<3>(f.y, 1), cp_dvar<3>(f.z, 2));
+    float w = F.v * expf(f.w);
+    float g[3] = {0.f, 0.f, 0.f};
+    if (F.v > 0.f && isfinite(w)) {
+      for (int d = 0; d < 3; ++d) g[d] = F.d[d] / F.v;
+    } else {
+      w = 0.f;
+    }
+    wg[p] = make_float4(w, g[0], g[1], g[2]);
+    s1 += w;
+    s2 += (double)w * w;
+  }
+  s1 = cp_warp_sum_d(s1);
+  s2 = cp_warp_sum_d(s2);
+  if ((threadIdx.x & 31) == 0) { sRed[threadIdx.x >> 5][0] = s1; sRed[threadIdx.x >> 5][1] = s2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += sRed[q][0]; b += sRed[q][1]; }
+    slots[2 * blockIdx.x] = a;
+    slots[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// 3. backward through the couplings (MLPs recomputed), writing the GEMM operands
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_store_rowfrag(uint16_t* base, int ld, uint64_t row0, uint64_t n, int gid, int tig,
+                                                 const uint32_t h[4][4])
+{
+  // writes a 16 x 64 bf16 tile held as A fragments (rows row0 + gid, row0 + gid + 8)
+  const uint64_t ra = row0 + gid, rb = row0 + gid + 8;
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+    const int c0 = 16 * kt + 2 * tig;
+    if (ra < n) {
+      *reinterpret_cast<uint32_t*>(base + ra * ld + c0) = h[kt][0];
+      *reinterpret_cast<uint32_t*>(base + ra * ld + c0 + 8) = h[kt][2];
+    }
+    if (rb < n) {
+      *reinterpret_cast<uint32_t*>(base + rb * ld + c0) = h[kt][1];
+      *reinterpret_cast<uint32_t*>(base + rb * ld + c0 + 8) = h[kt][3];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g, uint64_t n,
+                                                  const float* __restrict__ zs, const float4* __restrict__ vj,
+                                                  const float4* __restrict__ wg, const double* __restrict__ sums,
+                                                  FlowTrainBufs out)
+{
+  extern __shared__ uint2 sPk[];   // all CP_FLOW_P_PER fragments of the 4 couplings, then biases
+  float* sBias = reinterpret_cast<float*>(sPk + CP_FLOW_NC * CP_FLOW_P_PER);
+  for (int e = threadIdx.x; e < CP_FLOW_NC * CP_FLOW_P_PER; e += blockDim.x) sPk[e] = pk_g[e];
+  for (int j = threadIdx.x; j < CP_FLOW_NC * CP_FLOW_NB; j += blockDim.x) sBias[j] = bias_g[j];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+  const double sig = sums[0] / (double)n;
+  const float cnorm = (float)(2.0 / ((double)n * sig * sig));
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  const uint64_t rounds = (n + 32 * warps - 1) / (32 * warps);
+  for (uint64_t r = 0; r < rounds; ++r) {
+    const uint64_t base = (r * warps + (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32;
+    const uint64_t p = base + lane;
+    const bool active = p < n;
+    float dz[3] = {0.f, 0.f, 0.f}, cJ = 0.f;
+    if (active) {
+      const float4 f = vj[p], g = wg[p];
+      cJ = cnorm * g.x * g.x;
+      const float v[3] = {f.x, f.y, f.z}, gv[3] = {g.y, g.z, g.w};
+      // sigmoid: dv/dz = v (1 - v); d ln(v (1 - v))/dz = 1 - 2 v
+      for (int d = 0; d < 3; ++d) dz[d] = cJ * gv[d] * v[d] * (1.f - v[d]) + cJ * (1.f - 2.f * v[d]);
+    }
+#pragma unroll 1
+    for (int c = CP_FLOW_NC - 1; c >= 0; --c) {
+      const CpCoupling k = cp_coupling(c);
+      const uint2* pk = sPk + c * CP_FLOW_P_PER;
+      const float* b = sBias + c * CP_FLOW_NB;
+      float zin[3] = {0.f, 0.f, 0.f};
+      if (active)
+        for (int d = 0; d < 3; ++d) zin[d] = zs[(p * CP_FLOW_NC + c) * 3 + d];
+      const float in0 = zin[k.cin[0]], in1 = k.nin > 1 ? zin[k.cin[1]] : 0.f;
+      const uint64_t off = (uint64_t)c * n;
+#pragma unroll 1
+      for (int tile = 0; tile < 2; ++tile) {
+        const int tb = 16 * tile;
+        const uint64_t row0 = base + tb;
+        // ---- recompute the MLP forward of this tile (A fragments kept for the ReLU masks)
+        float r0a = __shfl_sync(0xffffffffu, in0, tb + gid), r0b = __shfl_sync(0xffffffffu, in1, tb + gid);
+        float r8a = __shfl_sync(0xffffffffu, in0, tb + gid + 8), r8b = __shfl_sync(0xffffffffu, in1, tb + gid + 8);
+        uint32_t a[4] = {tig == 0 ? cp_bf2(r0a, r0b) : 0u, tig == 0 ? cp_bf2(r8a, r8b) : 0u, 0u, 0u};
+        if (tig == 0) {
+          if (row0 + gid < n) *reinterpret_cast<uint32_t*>(out.X + (off + row0 + gid) * 16) = a[0];
+          if (row0 + gid + 8 < n) *reinterpret_cast<uint32_t*>(out.X + (off + row0 + gid + 8) * 16) = a[1];
+        }
+        float acc[8][4];
+        uint32_t h1[4][4], h2[4][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+          const float b0 = b[nt * 8 + 2 * tig], b1 = b[nt * 8 + 2 * tig + 1];
+          acc[nt][0] = b0; acc[nt][1] = b1; acc[nt][2] = b0; acc[nt][3] = b1;
+          cp_mma_bf16(acc[nt], a, pk[CP_FLOW_P_W1 + nt * 32 + lane]);
+        }
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+          h1[kt][0] = cp_bf2(fmaxf(acc[2 * kt][0], 0.f), fmaxf(acc[2 * kt][1], 0.f));
+          h1[kt][1] = cp_bf2(fmaxf(acc[2 * kt][2], 0.f), fmaxf(acc[2 * kt][3], 0.f));
+          h1[kt][2] = cp_bf2(fmaxf(acc[2 * kt + 1][0], 0.f), fmaxf(acc[2 * kt + 1][1], 0.f));
+          h1[kt][3] = cp_bf2(fmaxf(acc[2 * kt + 1][2], 0.f), fmaxf(acc[2 * kt + 1][3], 0.f));
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+          const float b0 = b[64 + nt * 8 + 2 * tig], b1 = b[64 + nt * 8 + 2 * tig + 1];
+          acc[nt][0] = b0; acc[nt][1] = b1; acc[nt][2] = b0; acc[nt][3] = b1;
+#pragma unroll
+          for (int kt = 0; kt < 4; ++kt) cp_mma_bf16(acc[nt], h1[kt], pk[CP_FLOW_P_W2 + (kt * 8 + nt) * 32 + lane]);
+        }
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+          h2[kt][0] = cp_bf2(fmaxf(acc[2 * kt][0], 0.f), fmaxf(acc[2 * kt][1], 0.f));
+          h2[kt][1] = cp_bf2(fmaxf(acc[2 * kt][2], 0.f), fmaxf(acc[2 * kt][3], 0.f));
+          h2[kt][2] = cp_bf2(fmaxf(acc[2 * kt + 1][0], 0.f), fmaxf(acc[2 * kt + 1][1], 0.f));
+          h2[kt][3] = cp_bf2(fmaxf(acc[2 * kt + 1][2], 0.f), fmaxf(acc[2 * kt + 1][3], 0.f));
+        }
+        cp_store_rowfrag(out.H1 + off * 64, 64, row0, n, gid, tig, h1);
+        cp_store_rowfrag(out.H2 + off * 64, 64, row0, n, gid, tig, h2);
+        float c3[4] = {b[128 + 2 * tig], b[128 + 2 * tig + 1], b[128 + 2 * tig], b[128 + 2 * tig + 1]};
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) cp_mma_bf16(c3, h2[kt], pk[CP_FLOW_P_W3 + kt * 32 + lane]);
+        // ---- this tile's rows: outputs to the point lanes, coupling backward there
+        const int rr = (lane - tb) & 15, src = 4 * (rr & 7);
+        const bool hi = rr >= 8, mine = lane >= tb && lane < tb + 16;
+        float o[4];
+        {
+          float x0 = __shfl_sync(0xffffffffu, c3[0], src), x1 = __shfl_sync(0xffffffffu, c3[1], src);
+          float x2 = __shfl_sync(0xffffffffu, c3[2], src), x3 = __shfl_sync(0xffffffffu, c3[3], src);
+          float y0 = __shfl_sync(0xffffffffu, c3[0], src + 1), y1 = __shfl_sync(0xffffffffu, c3[1], src + 1);
+          float y2 = __shfl_sync(0xffffffffu, c3[2], src + 1), y3 = __shfl_sync(0xffffffffu, c3[3], src + 1);
+          o[0] = hi ? x2 : x0; o[1] = hi ? x3 : x1; o[2] = hi ? y2 : y0; o[3] = hi ? y3 : y1;
+        }
+        float dO[4] = {0.f, 0.f, 0.f, 0.f};
+        float dzT[2] = {0.f, 0.f};
+        if (mine && active) {
+          for (int j = 0; j < k.nt; ++j) {
+            const float th = tanhf(o[j] / CP_FLOW_S), s = CP_FLOW_S * th, e = expf(s);
+            const int d = k.tr[j];
+            const float dzo = dz[d];
+            const float ds = fmaf(dzo * zin[d], e, cJ);
+            dO[j] = ds * (1.f - th * th);
+            dO[k.nt + j] = dzo;
+            dzT[j] = dzo * e;
+          }
+        }
+        // dO as an A fragment: columns 0..3, rows gid and gid + 8
+        // (a shuffle sends the value the source lane holds, so fetch all four and select here)
+        float g0[4], g8[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          g0[q] = __shfl_sync(0xffffffffu, dO[q], tb + gid);
+          g8[q] = __shfl_sync(0xffffffffu, dO[q], tb + gid + 8);
+        }
+        const bool odd = tig & 1;
+        uint32_t ad[4] = {tig < 2 ? cp_bf2(odd ? g0[2] : g0[0], odd ? g0[3] : g0[1]) : 0u,
+                          tig < 2 ? cp_bf2(odd ? g8[2] : g8[0], odd ? g8[3] : g8[1]) : 0u, 0u, 0u};
+        if (tig < 2) {
+          if (row0 + gid < n) *reinterpret_cast<uint32_t*>(out.DO + (off + row0 + gid) * 16 + 2 * tig) = ad[0];
+          if (row0 + gid + 8 < n) *reinterpret_cast<uint32_t*>(out.DO + (off + row0 + gid + 8) * 16 + 2 * tig) = ad[1];
+        }
+        // dH2 = dO W3^T, masked by the ReLU of layer 2
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+          acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+          cp_mma_bf16(acc[nt], ad, pk[CP_FLOW_P_W3T + nt * 32 + lane]);
+          const uint32_t m01 = h2[nt >> 1][(nt & 1) ? 2 : 0], m23 = h2[nt >> 1][(nt & 1) ? 3 : 1];
+          if (cp_bf_lo(m01) <= 0.f) acc[nt][0] = 0.f;
+          if (cp_bf_hi(m01) <= 0.f) acc[nt][1] = 0.f;
+          if (cp_bf_lo(m23) <= 0.f) acc[nt][2] = 0.f;
+          if (cp_bf_hi(m23) <= 0.f) acc[nt][3] = 0.f;
+        }
+        uint32_t d2[4][4];
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+          d2[kt][0] = cp_bf2(acc[2 * kt][0], acc[2 * kt][1]);
+          d2[kt][1] = cp_bf2(acc[2 * kt][2], acc[2 * kt][3]);
+          d2[kt][2] = cp_bf2(acc[2 * kt + 1][0], acc[2 * kt + 1][1]);
+          d2[kt][3] = cp_bf2(acc[2 * kt + 1][2], acc[2 * kt + 1][3]);
+        }
+        cp_store_rowfrag(out.D2 + off * 64, 64, row0, n, gid, tig, d2);
+        // dH1 = dH2 W2^T, masked by the ReLU of layer 1
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) {
+          acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+          for (int kt = 0; kt < 4; ++kt) cp_mma_bf16(acc[nt], d2[kt], pk[CP_FLOW_P_W2T + (kt * 8 + nt) * 32 + lane]);
+          const uint32_t m01 = h1[nt >> 1][(nt & 1) ? 2 : 0], m23 = h1[nt >> 1][(nt & 1) ? 3 : 1];
+          if (cp_bf_lo(m01) <= 0.f) acc[nt][0] = 0.f;
+          if (cp_bf_hi(m01) <= 0.f) acc[nt][1] = 0.f;
+          if (cp_bf_lo(m23) <= 0.f) acc[nt][2] = 0.f;
+          if (cp_bf_hi(m23) <= 0.f) acc[nt][3] = 0.f;
+        }
+        uint32_t d1[4][4];
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+          d1[kt][0] = cp_bf2(acc[2 * kt][0], acc[2 * kt][1]);
+          d1[kt][1] = cp_bf2(acc[2 * kt][2], acc[2 * kt][3]);
+          d1[kt][2] = cp_bf2(acc[2 * kt + 1][0], acc[2 * kt + 1][1]);
+          d1[kt][3] = cp_bf2(acc[2 * kt + 1][2], acc[2 * kt + 1][3]);
+        }
+        cp_store_rowfrag(out.D1 + off * 64, 64, row0, n, gid, tig, d1);
+        // dX = dH1 W1^T: columns 0..1 are the gradients of the two input features
+        float cx[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) cp_mma_bf16(cx, d1[kt], pk[CP_FLOW_P_W1T + kt * 32 + lane]);
+        const float e0 = __shfl_sync(0xffffffffu, cx[0], src), e1 = __shfl_sync(0xffffffffu, cx[1], src);
+        const float e2 = __shfl_sync(0xffffffffu, cx[2], src), e3 = __shfl_sync(0xffffffffu, cx[3], src);
+        if (mine && active) {
+          const float dx0 = hi ? e2 : e0, dx1 = hi ? e3 : e1;
+          for (int j = 0; j < k.nt; ++j) dz[k.tr[j]] = dzT[j];
+          dz[k.cin[0]] += dx0;
+          if (k.nin > 1) dz[k.cin[1]] += dx1;
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// 4. weight gradients G[M][N] += sum_p A[p][0:M]^T B[p][0:N] on the tensor cores
+//    (A, B bf16 row-major with leading dims lda = M, ldb = N; M in {16, 64}, N in {16, 64})
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_ldsm_x4_t(uint32_t r[4], const void* p)
+{
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+
+template <int M, int N>
+__global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
+                                                    uint64_t n, float* __restrict__ G, int ldg, int nvalid, int chunk)
+{
+  constexpr int MT = M / 16, NT = N / 8, TPW = (MT * NT + 3) / 4;
+  __shared__ __align__(16) uint16_t sA[16 * M];
+  __shared__ __align__(16) uint16_t sB[16 * N];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
+  const int mi = lane >> 3, rw = lane & 7;
+  float acc[TPW][4];
+#pragma unroll
+  for (int j = 0; j < TPW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const uint64_t p_begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t p_end = p_begin + chunk < n ? p_begin + chunk : n;
+  for (uint64_t p0 = p_begin; p0 < p_end; p0 += 16) {
+    for (int e = threadIdx.x; e < 16 * M / 8; e += blockDim.x) {
+      const int row = e / (M / 8), col = (e % (M / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (p0 + row < p_end) v = *reinterpret_cast<const uint4*>(A + (p0 + row) * M + col);
+      *reinterpret_cast<uint4*>(&sA[row * M + col]) = v;
+    }
+    for (int e = threadIdx.x; e < 16 * N / 8; e += blockDim.x) {
+      const int row = e / (N / 8), col = (e % (N / 8)) * 8;
+      uint4 v = make_uint4(0, 0, 0, 0);
+      if (p0 + row < p_end) v = *reinterpret_cast<const uint4*>(B + (p0 + row) * N + col);
+      *reinterpret_cast<uint4*>(&sB[row * N + col]) = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < TPW; ++j) {
+      const int t = warp + 4 * j;
+      if (t < MT * NT) {
+        const int mt = t / NT, nt = t % NT;
+        uint32_t a[4], bq[2];
+        // A^T of m-tile mt: 8x8 blocks (points 0-7 | 8-15) x (m +0 | +8), delivered transposed
+        cp_ldsm_x4_t(a, &sA[((mi >> 1) * 8 + rw) * M + mt * 16 + (mi & 1) * 8]);
+        // B of n-tile nt: blocks (points 0-7 | 8-15) x (n tile), delivered transposed
+        {
+          const uint32_t ad = (uint32_t)__cvta_generic_to_shared(&sB[((mi & 1) * 8 + rw) * N + nt * 8]);
+          asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+                       : "=r"(bq[0]), "=r"(bq[1]) : "r"(ad));
+        }
+        cp_mma_bf16(acc[j], a, make_uint2(bq[0], bq[1]));
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < TPW; ++j) {
+    const int t = warp + 4 * j;
+    if (t >= MT * NT) continue;
+    const int mt = t / NT, nt = t % NT;
+    const int m0 = mt * 16 + gid, n0 = nt * 8 + 2 * tig;
+    if (n0 < nvalid) { atomicAdd(&G[m0 * ldg + n0], acc[j][0]); atomicAdd(&G[(m0 + 8) * ldg + n0], acc[j][2]); }
+    if (n0 + 1 < nvalid) { atomicAdd(&G[m0 * ldg + n0 + 1], acc[j][1]); atomicAdd(&G[(m0 + 8) * ldg + n0 + 1], acc[j][3]); }
+  }
+}
+
+// column sums of a bf16 [n][ld] array (bias gradients)
+__global__ void k_flow_colsum(const uint16_t* __restrict__ D, uint64_t n, int ld, int ncols, float* __restrict__ out)
+{
+  const int col = threadIdx.x % ncols;
+  const int lanes = blockDim.x / ncols;
+  float s = 0.f;
+  for (uint64_t p = (uint64_t)blockIdx.x * lanes + threadIdx.x / ncols; p < n; p += (uint64_t)gridDim.x * lanes)
+    s += __uint_as_float(((uint32_t)D[p * ld + col]) << 16);
+  if ((int)threadIdx.x < lanes * ncols) atomicAdd(&out[col], s);
+}
+
+// ------------------------------------------------------------------------------------------
+// 5. Adam on the FP32 master weights (padding entries stay zero)
+// ------------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ bool cp_flow_param_used(int i)
+{
+  const int c = i / CP_FLOW_PER, o = i % CP_FLOW_PER;
+  const CpCoupling k = cp_coupling(c);
+  const int nout = 2 * k.nt;
+  if (o < CP_FLOW_B1) return o / 64 < k.nin;
+  if (o < CP_FLOW_B2) return true;
+  if (o < CP_FLOW_W3) return true;
+  if (o < CP_FLOW_B3) return ((o - CP_FLOW_W3) % 8) < nout;
+  return (o - CP_FLOW_B3) < nout;
+}
+
+__global__ void k_flow_adam(float* __restrict__ P, float* __restrict__ G, float* __restrict__ Mo, float* __restrict__ Vo,
+                            float lr, float b1t, float b2t)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= CP_FLOW_NPARAM) return;
+  const float g = G[i];
+  G[i] = 0.f;
+  if (!cp_flow_param_used(i)) { P[i] = 0.f; return; }
+  const float m = 0.9f * Mo[i] + 0.1f * g, v = 0.999f * Vo[i] + 0.001f * g * g;
+  Mo[i] = m;
+  Vo[i] = v;
+  P[i] -= lr * (m / (1.f - b1t)) / (sqrtf(v / (1.f - b2t)) + 1e-8f);
+}
+
+__global__ void k_flow_loss(const double* slots, int nblk, uint64_t n, double* sums, double* loss)
+{
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < nblk; ++k) { a += slots[2 * k]; b += slots[2 * k + 1]; }
+  sums[0] = a;
+  sums[1] = b;
+  const double m = a / (double)n;
+  loss[0] = (b / (double)n) / (m * m);
+}
+
+// ------------------------------------------------------------------------------------------
+// host
+// ------------------------------------------------------------------------------------------
+struct FlowTrainMem {
+  void* base = nullptr;
+  uint64_t cap = 0;
+};
+
+static size_t train_bytes(uint64_t B)
+{
+  return B * (sizeof(float) * 12 + sizeof(float4) * 2 + 2 * CP_FLOW_NC * (16 + 64 * 4 + 16)) + 4096;
+}
+
+static FlowTrainBufs carve(void* base, uint64_t B)
+{
+  char* q = static_cast<char*>(base);
+  FlowTrainBufs t;
+  t.vj = reinterpret_cast<float4*>(q); q += sizeof(float4) * B;
+  t.wg = reinterpret_cast<float4*>(q); q += sizeof(float4) * B;
+  t.zs = reinterpret_cast<float*>(q); q += sizeof(float) * 12 * B;
+  t.X = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 16 * B;
+  t.H1 = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 64 * B;
+  t.H2 = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 64 * B;
+  t.D1 = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 64 * B;
+  t.D2 = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 64 * B;
+  t.DO = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 16 * B;
+  q = reinterpret_cast<char*>(((uintptr_t)q + 255) & ~(uintptr_t)255);
+  t.sums = reinterpret_cast<double*>(q); q += 64;
+  t.loss = reinterpret_cast<double*>(q);
+  return t;
+}
+
+static size_t bwd_smem() { return sizeof(uint2) * CP_FLOW_NC * CP_FLOW_P_PER + sizeof(float) * CP_FLOW_NC * CP_FLOW_NB; }
+static size_t fwd_smem() { return sizeof(uint2) * CP_FLOW_NC * CP_FLOW_P_FWD + sizeof(float) * CP_FLOW_NC * CP_FLOW_NB; }
+
+// One training step over a batch of B points (counter iteration = step, Philox stream 2).
+static int flow_train_step(cp_handle* h, const FlowTrainBufs& t, uint64_t B, uint32_t step, float lr, double* loss_dev)
+{
+  const int nb = h->nb;
+  k_flow_fwd_train<<<h->num_sms * 2, CP_THREADS, fwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, h->d_edges, nb,
+                                                                           h->cfg.seed, step, 2, B, t.zs, t.vj);
+  CP_LAUNCH_CHECK(h, "k_flow_fwd_train");
+  const int gblk = h->num_sms * 4;
+  int rc = cp_ensure_slots(h, (size_t)2 * gblk);
+  if (rc) return rc;
+  const float lnTauMin = (float)log(4.0 * h->cfg.pt_hat_min * h->cfg.pt_hat_min / (h->cfg.sqrt_s * h->cfg.sqrt_s));
+  k_flow_igrad<<<gblk, 128, 0, h->stream>>>(h->P, h->d_cteq, B, lnTauMin, t.vj, t.wg, h->d_slots);
+  CP_LAUNCH_CHECK(h, "k_flow_igrad");
+  k_flow_loss<<<1, 1, 0, h->stream>>>(h->d_slots, gblk, B, t.sums, loss_dev);
+  CP_LAUNCH_CHECK(h, "k_flow_loss");
+  k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, B, t.zs, t.vj, t.wg, t.sums, t);
+  CP_LAUNCH_CHECK(h, "k_flow_bwd");
+  float* G = h->d_flow + CP_FLOW_NPARAM;
+  const int chunk = 4096;
+  const int cblk = (int)((B + chunk - 1) / chunk);
+  for (int c = 0; c < CP_FLOW_NC; ++c) {
+    float* g = G + c * CP_FLOW_PER;
+    k_flow_wgrad<16, 64><<<cblk, 128, 0, h->stream>>>(t.X + (uint64_t)c * B * 16, t.D1 + (uint64_t)c * B * 64, B,
+                                                      g + CP_FLOW_W1, 64, 64, chunk);
+    k_flow_wgrad<64, 64><<<cblk, 128, 0, h->stream>>>(t.H1 + (uint64_t)c * B * 64, t.D2 + (uint64_t)c * B * 64, B,
+                                                      g + CP_FLOW_W2, 64, 64, chunk);
+    // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
+    k_flow_wgrad<64, 16><<<cblk, 128, 0, h->stream>>>(t.H2 + (uint64_t)c * B * 64, t.DO + (uint64_t)c * B * 16, B,
+                                                      g + CP_FLOW_W3, 8, 8, chunk);
+    CP_LAUNCH_CHECK(h, "k_flow_wgrad");
+    k_flow_colsum<<<64, 256, 0, h->stream>>>(t.D1 + (uint64_t)c * B * 64, B, 64, 64, g + CP_FLOW_B1);
+    k_flow_colsum<<<64, 256, 0, h->stream>>>(t.D2 + (uint64_t)c * B * 64, B, 64, 64, g + CP_FLOW_B2);
+    k_flow_colsum<<<64, 256, 0, h->stream>>>(t.DO + (uint64_t)c * B * 16, B, 16, 8, g + CP_FLOW_B3);
+    CP_LAUNCH_CHECK(h, "k_flow_colsum");
+  }
+  return CP_OK;
+}
+
+// Trains the flow for n_steps batches of `batch` points on the current VEGAS grid; loss_host
+// (n_steps doubles, may be NULL) receives <w^2>/<w>^2 of each batch before its update.
+extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host)
+{
+  CP_CHECK_HANDLE(h);
+  if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
+  if (n_steps < 1 || batch < 64 || batch > (1ull << 24) || (batch & 31))
+    return cp_fail(h, CP_ERR_INVALID, "cp_flow_train: batch must be a multiple of 32 in [64, 2^24]");
+  static bool attr = false;
+  if (!attr) {
+    CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
+    CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
+    attr = true;
+  }
+  void* mem = nullptr;
+  const size_t bytes = train_bytes(batch);
+  CP_CUDA(h, cudaMalloc(&mem, bytes + sizeof(double) * (size_t)n_steps));
+  FlowTrainBufs t = carve(mem, batch);
+  double* losses = reinterpret_cast<double*>(static_cast<char*>(mem) + bytes);
+  int rc = CP_OK;
+  cudaError_t e = cudaMemsetAsync(mem, 0, bytes, h->stream);
+  if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_train memset");
+  float* G = h->d_flow + CP_FLOW_NPARAM;
+  if (!rc) e = cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream);
+  for (int s = 0; s < n_steps && rc == CP_OK; ++s) {
+    rc = flow_train_step(h, t, batch, (uint32_t)(h->flow_t + s), (float)lr, losses + s);
+    if (rc) break;
+    const long step = h->flow_t + s + 1;
+    k_flow_adam<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(
+        h->d_flow, G, G + CP_FLOW_NPARAM, G + 2 * CP_FLOW_NPARAM, (float)lr,
+        (float)pow(0.9, (double)step), (float)pow(0.999, (double)step));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { rc = cp_fail_cuda(h, e, "k_flow_adam"); break; }
+    rc = cp_flow_repack(h);
+  }
+  if (!rc) {
+    h->flow_t += n_steps;
+    if (loss_host) e = cudaMemcpyAsync(loss_host, losses, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_train readback");
+  } else {
+    cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(mem);
+  return rc;
+}
+
+// Loss gradient of one batch without updating (for the gradient checks): grad_host receives
+// cp_flow_num_params() floats (dL/dtheta of L = <w^2>/<w>^2), loss_host the batch loss.
+extern "C" int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, float* grad_host, double* loss_host)
+{
+  CP_CHECK_HANDLE(h);
+  if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
+  if (batch < 64 || batch > (1ull << 24) || (batch & 31)) return cp_fail(h, CP_ERR_INVALID, "bad batch");
+  static bool attr = false;
+  if (!attr) {
+    CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
+    CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
+    attr = true;
+  }
+  void* mem = nullptr;
+  const size_t bytes = train_bytes(batch);
+  CP_CUDA(h, cudaMalloc(&mem, bytes + sizeof(double)));
+  FlowTrainBufs t = carve(mem, batch);
+  double* loss = reinterpret_cast<double*>(static_cast<char*>(mem) + bytes);
+  float* G = h->d_flow + CP_FLOW_NPARAM;
+  cudaError_t e = cudaMemsetAsync(mem, 0, bytes, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream);
+  int rc = e == cudaSuccess ? flow_train_step(h, t, batch, iter, 0.f, loss) : cp_fail_cuda(h, e, "memset");
+  if (!rc) {
+    e = cudaMemcpyAsync(grad_host, G, sizeof(float) * CP_FLOW_NPARAM, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && loss_host) e = cudaMemcpyAsync(loss_host, loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_loss_grad readback");
+  } else {
+    cudaStreamSynchronize(h->stream);
+  }
+  cudaFree(mem);
+  return rc;
+}

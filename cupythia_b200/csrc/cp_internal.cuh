@@ -69,6 +69,15 @@ struct cp_handle {
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
   unsigned long long* d_counter = nullptr; // accepted-event counter
   uint64_t last_n = 0;
+  // learned proposal: FP32 master/grad/Adam moments (4 x n_param), packed BF16 fragments,
+  // staged biases, per-point (v, ln J) buffer; flow_on routes the passes through the flow
+  float* d_flow = nullptr;
+  uint2* d_flow_pk = nullptr;
+  float* d_flow_bias = nullptr;
+  float4* d_flow_buf = nullptr;
+  uint64_t flow_buf_cap = 0;
+  int flow_on = 0;
+  long flow_t = 0;
   std::string err;
 };
 
@@ -76,6 +85,8 @@ int cp_fail(cp_handle* h, int code, const std::string& msg);
 int cp_fail_cuda(cp_handle* h, cudaError_t e, const char* what);
 int cp_ensure_slots(cp_handle* h, size_t doubles);
 int cp_ensure_iters(cp_handle* h, int n);
+int cp_flow_buffer(cp_handle* h, uint64_t n);
+int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out);
 
 #define CP_CHECK_HANDLE(h) \
   do { if (!(h)) return CP_ERR_INVALID; } while (0)
@@ -153,6 +164,20 @@ __device__ __forceinline__ double cp_warp_max_d(double v)
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+
+// VEGAS map of a continuous coordinate v in [0, 1] (the flow's output): bin, x, width.
+__device__ __forceinline__ void cp_map_v(const float2* edges_d, int nb, float v, int& bin, float& x, float& width)
+{
+  const float t = v * (float)nb;
+  int b = (int)t;
+  b = b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+  float frac = t - (float)b;
+  frac = frac < 0.f ? 0.f : (frac > 1.f ? 1.f : frac);
+  const float2 e = edges_d[b];
+  bin = b;
+  x = fmaf(frac, e.y, e.x);
+  width = e.y;
 }
 
 // Copies the 8 CTEQ5L coefficient records from global into shared memory (block-wide).

@@ -29,6 +29,7 @@ struct UnwLaunch {
   uint64_t capacity;
   unsigned long long* counter; // events accepted so far (may exceed capacity: reported)
   double* slots;
+  const float4* flow;          // flow output (v, ln J) per in-call point, or null
 };
 
 static_assert(sizeof(CpEventRec) == 64, "event record must be 64 bytes");
@@ -52,6 +53,19 @@ __device__ __forceinline__ CpMapped cp_map_point(const float2 (*sEdge)[CP_MAX_BI
     m.x[d] = fmaf(frac, e.y, e.x);
     m.jv *= nbf * e.y;
   }
+  return m;
+}
+
+// map of a point: the flow's v if present, else the Philox words
+__device__ __forceinline__ CpMapped cp_map_any(const float2 (*sEdge)[CP_MAX_BINS], int nb, const uint32_t wd[4],
+                                               const float4* flow, uint64_t p)
+{
+  if (!flow) return cp_map_point(sEdge, nb, wd);
+  // the flow already applied the VEGAS map and its own transform: x and the total ln J
+  CpMapped m;
+  const float4 f = flow[p];
+  m.x[0] = f.x; m.x[1] = f.y; m.x[2] = f.z;
+  m.jv = expf(f.w);
   return m;
 }
 
@@ -90,7 +104,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
     if (p < L.n) {
       uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
-      CpMapped m = cp_map_point(sEdge, L.nb, wd);
+      CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
       w = cp_had_weight(P, sCteq, m.x[0], m.x[1], m.x[2], nullptr) * m.jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
       cp_kahan(s1, c1, w);
@@ -152,7 +166,7 @@ __global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, c
     uint32_t wd[4], w2[4];
     cp_point_words(L.seed, point, L.iter, 0, wd);
     cp_point_words(L.seed, point, L.iter, 1, w2);
-    CpMapped m = cp_map_point(sEdge, L.nb, wd);
+    CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, tail.w);
     CpPoint pt;
     cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt);
     CpEventRec ev;
@@ -191,6 +205,14 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;
   L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
+  L.flow = nullptr;
+  if (h->flow_on) {
+    rc = cp_flow_buffer(h, n);
+    if (rc) return rc;
+    rc = cp_flow_forward_enqueue(h, point0, n, iter, 0, h->d_flow_buf);
+    if (rc) return rc;
+    L.flow = h->d_flow_buf;
+  }
   k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
   CP_LAUNCH_CHECK(h, "k_unw_accept");
   k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);

@@ -23,6 +23,7 @@ struct HadLaunch {
   float* w_out;    // optional per-point weights
   float* x_out;    // optional per-point mapped x (3 per point)
   unsigned long long* qhist;   // weight histogram (CP_QBINS), integer adds
+  const float4* flow;          // flow output (v, ln J) per point, or null: map the Philox words
 };
 
 template <bool WRITE>
@@ -61,16 +62,25 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
     float w = 0.f;
     int bin[3] = {0, 0, 0};
     if (active) {
+      float x[3], jv = 1.f;
       uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, L.stream, wd);
-      float x[3], jv = 1.f;
+      if (L.flow) {
+        // the flow already applied the VEGAS map and its own transform: x and the total ln J
+        const float4 f = L.flow[p];
+        x[0] = f.x; x[1] = f.y; x[2] = f.z;
+        jv = expf(f.w);
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        float frac;
-        cp_bin_frac(wd[d], nb, bin[d], frac);
-        float2 e = sEdge[d][bin[d]];
-        x[d] = fmaf(frac, e.y, e.x);
-        jv *= nbf * e.y;
+        for (int d = 0; d < 3; ++d) bin[d] = (int)(((wd[d] >> 8) * (uint32_t)nb) >> 24);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          float frac;
+          cp_bin_frac(wd[d], nb, bin[d], frac);
+          float2 e = sEdge[d][bin[d]];
+          x[d] = fmaf(frac, e.y, e.x);
+          jv *= nbf * e.y;
+        }
       }
       w = cp_had_weight(P, sCteq, x[0], x[1], x[2], nullptr) * jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
@@ -225,6 +235,14 @@ static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, 
   L.nb = h->nb; L.edges = h->d_edges; L.slots = h->d_slots; L.w_out = w_out; L.x_out = x_out;
   L.qhist = h->d_qhist;
   L.cteq = h->d_cteq;
+  L.flow = nullptr;
+  if (h->flow_on) {
+    rc = cp_flow_buffer(h, n);
+    if (rc) return rc;
+    rc = cp_flow_forward_enqueue(h, point0, n, iter, stream, h->d_flow_buf);
+    if (rc) return rc;
+    L.flow = h->d_flow_buf;
+  }
   CP_CUDA(h, cudaMemsetAsync(h->d_qhist, 0, sizeof(unsigned long long) * CP_QBINS, h->stream));
   h->last_n = n;
   if (w_out || x_out) k_had_accum<true><<<h->had_blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
@@ -453,7 +471,7 @@ extern "C" int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, ui
     HadLaunch L;
     L.seed = cfg->seed; L.point0 = 0; L.n = n_points; L.iter = iter; L.stream = 0;
     L.nb = nb; L.edges = edges_dev; L.cteq = reinterpret_cast<const CpCteqPoly*>(base);
-    L.slots = slots; L.w_out = nullptr; L.x_out = nullptr; L.qhist = qhist;
+    L.slots = slots; L.w_out = nullptr; L.x_out = nullptr; L.qhist = qhist; L.flow = nullptr;
     if (cudaMemsetAsync(qhist, 0, sizeof(unsigned long long) * CP_QBINS, stream) != cudaSuccess) {
       rc = CP_ERR_CUDA;
     } else {

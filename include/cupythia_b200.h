@@ -234,6 +234,30 @@ int cp_adjoint(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream, 
  * changes by exp(+-lr)); the alternative to the classic refinement of cp_vegas_iteration. */
 int cp_vegas_gradient_step(cp_handle* h, uint64_t n_points, uint32_t iter, double lr, cp_grad* out_host);
 
+/* ---------------------------------------------------------------- learned proposal -- */
+/* A RealNVP-style flow on [0,1]^3 in front of the VEGAS map: logit, 4 affine couplings (MLP
+ * in -> 64 -> 64 -> out, ReLU, BF16 weights and activations on the tensor cores, FP32
+ * accumulation), sigmoid.  No reference counterpart (the reference has no learned proposal).
+ * FP32 master parameters: cp_flow_num_params() floats in the layout of cupythia_b200/csrc/cp_flow.cuh. */
+int cp_flow_num_params(void);
+/* Xavier-uniform weights from the counter RNG with key `seed` (7 in the production recipe),
+ * zero biases, zero output layer (the untrained flow is the identity). */
+int cp_flow_init(cp_handle* h, uint64_t seed);
+int cp_flow_get_params(cp_handle* h, float* params_host, int n);
+int cp_flow_set_params(cp_handle* h, const float* params_host, int n);
+/* Flow samples of points [point0, point0+n), counter (iter, stream): out (dev, 16-byte aligned)
+ * holds (v0, v1, v2, ln|dv/du|) per point. */
+int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float* out_dev);
+/* Routes cp_vegas_iteration / cp_integrate / cp_point_weights / cp_unweight / cp_generate_host
+ * through the flow (on = 1) or the Philox words directly (on = 0). */
+int cp_flow_enable(cp_handle* h, int on);
+/* n_steps Adam steps (learning rate lr) on batches of `batch` points (counter stream 2) drawn
+ * through the current flow and VEGAS grid, minimising <w^2>/<w>^2; loss_host (n_steps doubles,
+ * may be NULL) receives each batch's value before its update. */
+int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host);
+/* The training gradient of one batch (counter iteration iter, stream 2) without an update. */
+int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, float* grad_host, double* loss_host);
+
 /* ---------------------------------------------------------------- measurement ------ */
 /* FP32 FMA and MUFU (ex2) throughput of the device from dependency-free microbenchmarks:
  * TFLOP/s (2 per FMA) and Tops/s.  No reference counterpart: the integrand's roofline

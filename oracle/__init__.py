@@ -55,6 +55,9 @@ _SIG = {
     "cpo_had_weight_grad": (None, [C.c_void_p, _PD, _PD]),
     "cpo_had_adjoint_sums": (None, [C.c_void_p, _PD, C.c_int, _U64, _U32, _U32, _U64, _U64, _PD, C.c_int]),
     "cpo_accept": (C.c_int, [_D, _D, _U32]),
+    "cpo_flow_forward": (None, [C.c_void_p, _PD, _PD, _PD]),
+    "cpo_flow_set_rounding": (None, [C.c_int]),
+    "cpo_flow_backward_batch": (None, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
 }
 
 _lib = None

@@ -629,3 +629,204 @@ void cpo_had_weight_x_batch(const cpo_had_cfg* c, const float* x, int64_t n, dou
   free(jobs);
   free(th);
 }
+
+/* ======================= the learned proposal (flow), FP64 ======================= */
+/* Same architecture and parameter layout as the CUDA flow: 4 affine couplings on logit space,
+ * MLP in -> 64 -> 64 -> out (ReLU), s = 4 tanh(s_raw / 4).  The forward reproduces the kernels'
+ * BF16 rounding points (weights, MLP inputs, post-ReLU activations); arithmetic is FP64.
+ * The backward is plain reverse-mode differentiation of that forward (rounding treated as the
+ * identity), the reference for the GPU's tensor-core training gradients. */
+#define FL_NC 4
+#define FL_PER 5768
+#define FL_W1 0
+#define FL_B1 1024
+#define FL_W2 1088
+#define FL_B2 5184
+#define FL_W3 5248
+#define FL_B3 5760
+#define FL_S 4.0
+
+static int fl_round = 1;
+void cpo_flow_set_rounding(int on) { fl_round = on; }
+
+static double bf16r(double x)
+{
+  if (!fl_round) return x;
+  float f = (float)x;
+  uint32_t b;
+  memcpy(&b, &f, 4);
+  b = (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;
+  memcpy(&f, &b, 4);
+  return (double)f;
+}
+
+static void fl_coupling(int c, int* nin, int cin[2], int* nt, int tr[2])
+{
+  static const int NIN[4] = {1, 2, 1, 2}, NT[4] = {2, 1, 2, 1};
+  static const int CIN[4][2] = {{0, 0}, {1, 2}, {1, 1}, {0, 2}}, TR[4][2] = {{1, 2}, {0, 0}, {0, 2}, {1, 1}};
+  *nin = NIN[c]; *nt = NT[c];
+  cin[0] = CIN[c][0]; cin[1] = CIN[c][1]; tr[0] = TR[c][0]; tr[1] = TR[c][1];
+}
+
+typedef struct {
+  double x[2], h1[64], h2[64], o[4], zin[3];
+} fl_tape;
+
+static void fl_mlp(const float* P, int c, int nin, const double in[2], fl_tape* t)
+{
+  const float* W1 = P + c * FL_PER + FL_W1;
+  const float* W2 = P + c * FL_PER + FL_W2;
+  const float* W3 = P + c * FL_PER + FL_W3;
+  const float* B = P + c * FL_PER;
+  for (int k = 0; k < 2; ++k) t->x[k] = k < nin ? bf16r(in[k]) : 0.0;
+  for (int j = 0; j < 64; ++j) {
+    double a = B[FL_B1 + j];
+    for (int k = 0; k < nin; ++k) a += t->x[k] * bf16r(W1[k * 64 + j]);
+    t->h1[j] = bf16r(a > 0 ? a : 0.0);
+  }
+  for (int j = 0; j < 64; ++j) {
+    double a = B[FL_B2 + j];
+    for (int k = 0; k < 64; ++k) a += t->h1[k] * bf16r(W2[k * 64 + j]);
+    t->h2[j] = bf16r(a > 0 ? a : 0.0);
+  }
+  for (int j = 0; j < 4; ++j) {
+    double a = B[FL_B3 + j];
+    for (int k = 0; k < 64; ++k) a += t->h2[k] * bf16r(W3[k * 8 + j]);
+    t->o[j] = a;
+  }
+}
+
+void cpo_flow_forward(const float* P, const double u[3], double v[3], double* logJ)
+{
+  double z[3], ld = 0.0;
+  for (int d = 0; d < 3; ++d) {
+    z[d] = log(u[d]) - log1p(-u[d]);
+    ld -= log(u[d]) + log1p(-u[d]);
+  }
+  for (int c = 0; c < FL_NC; ++c) {
+    int nin, nt, cin[2], tr[2];
+    fl_coupling(c, &nin, cin, &nt, tr);
+    fl_tape t;
+    double in[2] = {z[cin[0]], z[cin[1]]};
+    fl_mlp(P, c, nin, in, &t);
+    for (int j = 0; j < nt; ++j) {
+      double s = FL_S * tanh(t.o[j] / FL_S);
+      z[tr[j]] = z[tr[j]] * exp(s) + t.o[nt + j];
+      ld += s;
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    v[d] = 1.0 / (1.0 + exp(-z[d]));
+    ld += log(v[d]) + log1p(-v[d]);
+  }
+  *logJ = ld;
+}
+
+/* gradient of sum_p (cv_p . v_p + cJ_p lnJ_p) with respect to the parameters, accumulated */
+static void fl_backward_point(const float* P, const double u[3], const double cv[3], double cJ, double* G)
+{
+  double z[3];
+  fl_tape tape[FL_NC];
+  for (int d = 0; d < 3; ++d) z[d] = log(u[d]) - log1p(-u[d]);
+  for (int c = 0; c < FL_NC; ++c) {
+    int nin, nt, cin[2], tr[2];
+    fl_coupling(c, &nin, cin, &nt, tr);
+    for (int d = 0; d < 3; ++d) tape[c].zin[d] = z[d];
+    double in[2] = {z[cin[0]], z[cin[1]]};
+    fl_mlp(P, c, nin, in, &tape[c]);
+    for (int j = 0; j < nt; ++j) {
+      double s = FL_S * tanh(tape[c].o[j] / FL_S);
+      z[tr[j]] = z[tr[j]] * exp(s) + tape[c].o[nt + j];
+    }
+  }
+  double dz[3];
+  for (int d = 0; d < 3; ++d) {
+    double v = 1.0 / (1.0 + exp(-z[d]));
+    dz[d] = cv[d] * v * (1.0 - v) + cJ * (1.0 - 2.0 * v);
+  }
+  for (int c = FL_NC - 1; c >= 0; --c) {
+    int nin, nt, cin[2], tr[2];
+    fl_coupling(c, &nin, cin, &nt, tr);
+    const fl_tape* t = &tape[c];
+    const float* W1 = P + c * FL_PER + FL_W1;
+    const float* W2 = P + c * FL_PER + FL_W2;
+    const float* W3 = P + c * FL_PER + FL_W3;
+    double* g = G + c * FL_PER;
+    double dO[4] = {0, 0, 0, 0}, dzT[2] = {0, 0};
+    for (int j = 0; j < nt; ++j) {
+      double th = tanh(t->o[j] / FL_S), s = FL_S * th, e = exp(s);
+      int d = tr[j];
+      double ds = dz[d] * t->zin[d] * e + cJ;
+      dO[j] = ds * (1.0 - th * th);
+      dO[nt + j] = dz[d];
+      dzT[j] = dz[d] * e;
+    }
+    double dh2[64], dh1[64], dx[2] = {0, 0};
+    for (int j = 0; j < 4; ++j) {
+      g[FL_B3 + j] += dO[j];
+      for (int k = 0; k < 64; ++k) g[FL_W3 + k * 8 + j] += t->h2[k] * dO[j];
+    }
+    for (int k = 0; k < 64; ++k) {
+      double a = 0.0;
+      for (int j = 0; j < 4; ++j) a += dO[j] * bf16r(W3[k * 8 + j]);
+      dh2[k] = t->h2[k] > 0 ? a : 0.0;
+    }
+    for (int j = 0; j < 64; ++j) {
+      g[FL_B2 + j] += dh2[j];
+      for (int k = 0; k < 64; ++k) g[FL_W2 + k * 64 + j] += t->h1[k] * dh2[j];
+    }
+    for (int k = 0; k < 64; ++k) {
+      double a = 0.0;
+      for (int j = 0; j < 64; ++j) a += dh2[j] * bf16r(W2[k * 64 + j]);
+      dh1[k] = t->h1[k] > 0 ? a : 0.0;
+    }
+    for (int j = 0; j < 64; ++j) {
+      g[FL_B1 + j] += dh1[j];
+      for (int k = 0; k < nin; ++k) g[FL_W1 + k * 64 + j] += t->x[k] * dh1[j];
+    }
+    for (int k = 0; k < nin; ++k)
+      for (int j = 0; j < 64; ++j) dx[k] += dh1[j] * bf16r(W1[k * 64 + j]);
+    for (int j = 0; j < nt; ++j) dz[tr[j]] = dzT[j];
+    dz[cin[0]] += dx[0];
+    if (nin > 1) dz[cin[1]] += dx[1];
+  }
+}
+
+typedef struct {
+  const float* P;
+  const double *u, *cv, *cJ;
+  int64_t i0, i1;
+  double* G;
+} fl_job;
+
+static void* fl_thread(void* a)
+{
+  fl_job* j = (fl_job*)a;
+  for (int64_t i = j->i0; i < j->i1; ++i) fl_backward_point(j->P, j->u + 3 * i, j->cv + 3 * i, j->cJ[i], j->G);
+  return NULL;
+}
+
+/* G[FL_NC*FL_PER] = sum over points of the parameter gradient of cv . v + cJ lnJ */
+void cpo_flow_backward_batch(const float* P, int64_t n, const double* u, const double* cv, const double* cJ,
+                             double* G, int nthreads)
+{
+  const int NP = FL_NC * FL_PER;
+  nthreads = clamp_threads(nthreads, (uint64_t)n);
+  fl_job* jobs = (fl_job*)calloc((size_t)nthreads, sizeof(fl_job));
+  pthread_t* th = (pthread_t*)calloc((size_t)nthreads, sizeof(pthread_t));
+  int64_t per = n / nthreads, rem = n % nthreads, off = 0;
+  for (int t = 0; t < nthreads; ++t) {
+    jobs[t].P = P; jobs[t].u = u; jobs[t].cv = cv; jobs[t].cJ = cJ;
+    jobs[t].i0 = off; off += per + (t < rem ? 1 : 0); jobs[t].i1 = off;
+    jobs[t].G = (double*)calloc((size_t)NP, sizeof(double));
+    pthread_create(&th[t], NULL, fl_thread, &jobs[t]);
+  }
+  memset(G, 0, sizeof(double) * (size_t)NP);
+  for (int t = 0; t < nthreads; ++t) {
+    pthread_join(th[t], NULL);
+    for (int k = 0; k < NP; ++k) G[k] += jobs[t].G[k];
+    free(jobs[t].G);
+  }
+  free(jobs);
+  free(th);
+}

@@ -139,6 +139,15 @@ void cpo_had_adjoint_sums(const cpo_had_cfg* c, const double* edges, int nb, uin
 /* f * J_base at n points x (3n floats, as doubles), multi-threaded */
 void cpo_had_weight_x_batch(const cpo_had_cfg* c, const float* x, int64_t n, double* out, int nthreads);
 
+/* ---------------- learned proposal (flow) ---------------- */
+/* FP64 flow forward with the CUDA kernels' BF16 rounding points; P is the FP32 master layout. */
+void cpo_flow_forward(const float* P, const double u[3], double v[3], double* logJ);
+/* BF16 rounding emulation on (1, default) or off (0: plain FP64, for finite-difference checks) */
+void cpo_flow_set_rounding(int on);
+/* G = sum_p d(cv_p . v_p + cJ_p lnJ_p)/d params (reverse mode, FP64). */
+void cpo_flow_backward_batch(const float* P, int64_t n, const double* u, const double* cv, const double* cJ,
+                             double* G, int nthreads);
+
 /* ---------------- unweighting ---------------- */
 /* Accept draw of a point: word 3 of its Philox block, as u24. */
 int cpo_accept(double w, double wmax, uint32_t w3);

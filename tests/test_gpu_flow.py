@@ -1,0 +1,159 @@
+"""The learned proposal: BF16 tensor-core flow kernels against the FP64 CPU oracle.
+
+Tolerances: the forward runs in BF16 (weights, MLP inputs, activations) with FP32 accumulation,
+the oracle in FP64 with the same rounding points, so single BF16 rounding flips near ties move a
+few points: forward |dv| <= 2e-3 and |d ln J| <= 2e-2 for 99.9% of points.  The training
+gradient (tensor-core backward, BF16 operands) must agree with the FP64 backprop of the same
+cotangents to cosine similarity 0.999 and 5% in L2 norm."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NPAR = 4 * 5768
+PER = 5768
+
+
+def _used_mask():
+    m = np.zeros(NPAR, bool)
+    nin = [1, 2, 1, 2]
+    nout = [4, 2, 4, 2]
+    for c in range(4):
+        b = c * PER
+        for r in range(nin[c]):
+            m[b + r * 64:b + r * 64 + 64] = True
+        m[b + 1024:b + 5248] = True
+        for k in range(64):
+            m[b + 5248 + k * 8:b + 5248 + k * 8 + nout[c]] = True
+        m[b + 5760:b + 5760 + nout[c]] = True
+    return m
+
+
+def _random_flow(it, seed=3, scale=0.08):
+    it.flow_init(7)
+    P = it.flow_params.copy()
+    rng = np.random.default_rng(seed)
+    m = _used_mask()
+    for c in range(4):
+        b = c * PER
+        sl = slice(b + 5248, b + 5768)
+        P[sl] = np.where(m[sl], rng.normal(0, scale, 520), 0).astype(np.float32)
+        P[b + 1024:b + 1088] = rng.normal(0, 0.05, 64)
+        P[b + 5184:b + 5248] = rng.normal(0, 0.05, 64)
+    it.flow_params = P
+    return P
+
+
+def _xv(it, words):
+    """The flow's input: the VEGAS map of the words with a half-step offset (x_v strictly inside
+    (0, 1)), in FP32 as the kernel forms it, and ln of the VEGAS Jacobian."""
+    nb = it.nb
+    grid = it.grid
+    m = (words[:, :3] >> 8).astype(np.uint64) * nb
+    b = (m >> 24).astype(np.int64)
+    frac = (((m & 0xFFFFFF).astype(np.float64) + 0.5) / 2 ** 24).astype(np.float32)
+    lo = np.stack([grid[d][b[:, d]] for d in range(3)], 1).astype(np.float32)
+    wd = np.stack([grid[d][b[:, d] + 1] - grid[d][b[:, d]] for d in range(3)], 1).astype(np.float32)
+    x = (lo.astype(np.float64) + frac.astype(np.float64) * wd.astype(np.float64)).astype(np.float32)
+    x = np.clip(x, np.float32(5.9604645e-8), np.float32(0.99999994)).astype(np.float64)
+    lnjv = np.log(np.prod(nb * wd.astype(np.float64), 1))
+    return x, lnjv
+
+
+def test_untrained_flow_is_identity(integ):
+    integ.reset_grid()
+    integ.integrate(3, 1 << 20, alpha=1.5)
+    integ.flow_init(7)
+    out = integ.flow_sample(0, 4096, 3, 0).cpu().numpy()
+    xv, lnjv = _xv(integ, integ.philox_words(integ.cfg.seed, 0, 4096, 3, 0))
+    assert np.max(np.abs(out[:, :3] - xv)) < 2e-6
+    assert np.max(np.abs(out[:, 3] - lnjv)) < 2e-4 * np.maximum(1, np.abs(lnjv)).max()
+    integ.reset_grid()
+
+
+def test_flow_forward_matches_fp64_oracle(integ, orc):
+    P = _random_flow(integ)
+    n = 4096
+    out = integ.flow_sample(0, n, 3, 0).cpu().numpy().astype(np.float64)
+    u, lnjv = _xv(integ, integ.philox_words(integ.cfg.seed, 0, n, 3, 0))
+    out[:, 3] -= lnjv
+    L = orc.lib()
+    ref = np.zeros((n, 4))
+    v = np.zeros(3)
+    lj = C.c_double()
+    for i in range(n):
+        L.cpo_flow_forward(P.ctypes.data, orc.dptr(u[i].copy()), orc.dptr(v), C.byref(lj))
+        ref[i, :3] = v
+        ref[i, 3] = lj.value
+    dv = np.abs(out[:, :3] - ref[:, :3]).max(1)
+    dj = np.abs(out[:, 3] - ref[:, 3])
+    assert np.percentile(dv, 99.9) < 2e-3 and np.median(dv) < 1e-4, (np.median(dv), np.percentile(dv, 99.9))
+    assert np.percentile(dj, 99.9) < 2e-2 and np.median(dj) < 1e-3, (np.median(dj), np.percentile(dj, 99.9))
+    # the map is non-trivial: it moved the points
+    assert np.median(np.abs(ref[:, :3] - u)) > 1e-3
+
+
+def _cpu_cotangents(it, orc, flow_out, n):
+    """(w, d ln f/dx) at the flow's points from the FP64 oracle (complex step), as the GPU forms them."""
+    L = orc.lib()
+    cfg = orc.had_cfg()
+    x = flow_out[:, :3].astype(np.float64)
+    g = np.zeros((n, 7))
+    out = (C.c_double * 7)()
+    for i in range(n):
+        L.cpo_had_weight_grad(C.byref(cfg), orc.dptr(x[i].copy()), out)
+        g[i] = out[:]
+    f = g[:, 0]
+    w = f * np.exp(flow_out[:, 3].astype(np.float64))
+    dlnf = np.where(f[:, None] > 0, g[:, 1:4] / np.where(f > 0, f, 1)[:, None], 0)
+    return w, dlnf
+
+
+def test_training_gradient_matches_fp64_backprop(integ, orc):
+    integ.reset_grid()
+    integ.integrate(4, 1 << 20, alpha=1.5)
+    P = _random_flow(integ, seed=5, scale=0.05)
+    B = 8192
+    it_idx = 11
+    g_gpu, loss_gpu = integ.flow_loss_grad(B, it_idx)
+    flow_out = integ.flow_sample(0, B, it_idx, 2).cpu().numpy()
+    w, dlnF = _cpu_cotangents(integ, orc, flow_out, B)
+    sig = w.mean()
+    loss_cpu = (w * w).mean() / sig ** 2
+    assert abs(loss_gpu / loss_cpu - 1) < 2e-3, (loss_gpu, loss_cpu)
+    cJ = 2 * w * w / (B * sig ** 2)
+    cv = cJ[:, None] * dlnF
+    u, _ = _xv(integ, integ.philox_words(integ.cfg.seed, 0, B, it_idx, 2))
+    G = np.zeros(NPAR)
+    orc.lib().cpo_flow_backward_batch(P.ctypes.data, B, np.ascontiguousarray(u).ctypes.data,
+                                      np.ascontiguousarray(cv).ctypes.data, np.ascontiguousarray(cJ).ctypes.data,
+                                      G.ctypes.data, 8)
+    m = _used_mask()
+    a, b = g_gpu[m].astype(np.float64), G[m]
+    cos = a @ b / np.linalg.norm(a) / np.linalg.norm(b)
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert cos > 0.999 and rel < 5e-2, (cos, rel)
+    assert np.all(g_gpu[~m] == 0)
+    integ.reset_grid()
+
+
+def test_training_lowers_the_weight_variance():
+    import cupythia_b200 as cp
+    n = 1 << 22
+    with cp.Integrator() as it:
+        it.integrate(8, 1 << 22, alpha=1.5)
+        base = it.iteration(n, 500, alpha=0.0)
+        it.flow_init(7)
+        loss = it.flow_train(120, 65536, lr=1e-3)
+        it.flow_enable(True)
+        flow = it.iteration(n, 500, alpha=0.0)
+        it.flow_enable(False)
+    assert np.all(np.isfinite(loss))
+    assert loss[-10:].mean() < loss[:5].mean()
+    rv_base = (base["sigma_err"] / base["sigma"]) ** 2
+    rv_flow = (flow["sigma_err"] / flow["sigma"]) ** 2
+    print("relative variance VEGAS %.3e  flow+VEGAS %.3e  loss %.4f -> %.4f" % (rv_base, rv_flow, loss[0], loss[-1]))
+    assert rv_flow < rv_base
+    assert abs(flow["sigma"] - base["sigma"]) < 5 * np.hypot(flow["sigma_err"], base["sigma_err"])

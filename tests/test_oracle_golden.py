@@ -141,3 +141,41 @@ def test_complex_step_gradient_matches_finite_differences(orc):
             fd = (L.cpo_had_weight_x(C.byref(cp_), orc.dptr(x), None) -
                   L.cpo_had_weight_x(C.byref(cm_), orc.dptr(x), None)) / (2 * h)
             assert g[4 + k] == pytest.approx(fd, rel=1e-5, abs=1e-9 * abs(g[0]))
+
+
+def test_flow_oracle_backprop_matches_finite_differences(orc):
+    """The FP64 reference backprop of the flow against central differences of its forward."""
+    L = orc.lib()
+    L.cpo_flow_set_rounding(0)
+    try:
+        rng = np.random.default_rng(4)
+        npar = 4 * 5768
+        P = (rng.normal(0, 0.2, npar)).astype(np.float32)
+        n = 6
+        u = rng.uniform(0.05, 0.95, (n, 3))
+        cv = rng.normal(0, 1, (n, 3))
+        cJ = rng.normal(0, 1, n)
+        G = np.zeros(npar)
+        L.cpo_flow_backward_batch(P.ctypes.data, n, u.ctypes.data, cv.ctypes.data, cJ.ctypes.data, G.ctypes.data, 2)
+
+        def objective(Pp):
+            tot = 0.0
+            for i in range(n):
+                v = np.zeros(3)
+                lj = C.c_double()
+                L.cpo_flow_forward(Pp.ctypes.data, orc.dptr(u[i].copy()), orc.dptr(v), C.byref(lj))
+                tot += float(cv[i] @ v) + cJ[i] * lj.value
+            return tot
+        # parameters that the architecture uses: W1 row 0, b1, W2, b2, W3 cols < 2 nt, b3
+        idx = [0 * 5768 + 5, 0 * 5768 + 1024 + 7, 1 * 5768 + 1088 + 300, 2 * 5768 + 5184 + 9,
+               3 * 5768 + 5248 + 8 * 10 + 1, 0 * 5768 + 5760 + 3, 1 * 5768 + 64 + 2, 2 * 5768 + 1088 + 4000]
+        for k in idx:
+            h = 1e-4
+            Pp, Pm = P.astype(np.float64).copy(), P.astype(np.float64).copy()
+            Pp[k] += h
+            Pm[k] -= h
+            fd = (objective(Pp.astype(np.float32)) - objective(Pm.astype(np.float32))) / (
+                float(np.float32(Pp[k])) - float(np.float32(Pm[k])))
+            assert G[k] == pytest.approx(fd, rel=2e-3, abs=1e-6), (k, G[k], fd)
+    finally:
+        L.cpo_flow_set_rounding(1)
