@@ -1,18 +1,25 @@
 """Benchmark: unweighted events/s of pp -> 2 jets (13 TeV, pT_hat > 20 GeV, CTEQ5L, first-order
 alpha_s(mZ) = 0.13, the five HardQCD 2 -> 2 processes) on B200, at a relative sigma error
-<= 1% per step.
+<= 1% per step, for two forms of the integrator on the same workload:
+
+  plain VEGAS    classic Lepage refinement (10 x 2^24 points, alpha 1.5), w_max = q99.9
+  flow+adjoint   variance-gradient grid refinement (adjoint kernel, 12 x 2^22 points), then a
+                 BF16 coupling flow after the VEGAS map trained on 200 x 65536 points by the
+                 pathwise gradient of <w^2>/<w>^2, w_max = q99.9 through the flow
 
 One step = one production pass over a batch of counter-RNG points: draw -> (flow) -> VEGAS map
 -> (tau, y, cos theta) -> matrix elements x PDFs x alpha_s -> weights -> unweighting against
-w_max (99.9th percentile) -> on-device compaction into 64-byte event records.  Grid adaptation
-(and flow training) run before the timed region and are reported separately.
+w_max -> on-device compaction into 64-byte event records.  Grid adaptation and flow training
+run before the timed region and are reported separately (adapt_seconds).
 
-  value   steady-state events/s, inputs resident, CUDA events on the library's stream, max over
-          ranks; every rank produces a disjoint range of counter points (weak scaling, no
-          data-path collective)
-  e2e     the same through the host-buffer C-ABI call cp_generate_host: the step's inputs
-          (VEGAS grid) copied host -> device and every event record copied device -> pinned
-          host memory inside the timed region
+  value        flow+adjoint events/s, inputs resident, CUDA events on the library's stream,
+               max over ranks; every rank produces a disjoint range of counter points (weak
+               scaling, no data-path collective); plain_vegas holds the same for the plain form
+  e2e          the flow+adjoint form through the host-buffer C-ABI call cp_generate_host: the
+               step's inputs (VEGAS grid) copied host -> device and every event record copied
+               device -> pinned host memory inside the timed region
+  roofline     the dominant kernel of the timed step from live per-kernel CUDA-event durations
+               (cp_set_kernel_timing); roofline_secondary the other one
   --impl reference   stock Pythia 8.317 (ProcessLevel, the same settings) on all host cores
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
@@ -145,6 +152,45 @@ def measured_peaks():
 
 
 # --------------------------------------------------------------------------- our arm
+# algorithmic work per point of the two dominant kernels
+FP32_FLOP_PER_POINT = 3278.0      # k_unw_accept: FADD + FMUL + 2 FFMA per point (ncu SASS counters, profiles/)
+FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
+
+
+def production(it, n, records, k0, warmup, steps, pg, dev, stream, clocks=None):
+    """warmup + steps production passes (unweighting + compaction), device-timed per step."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")   # > 126 MB L2
+    for k in range(warmup):
+        it.unweight(n, iteration=k0 + k, records=records)
+    barrier(pg, dev)
+    it.set_kernel_timing(True)
+    it.kernel_times(reset=True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    stats = []
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        for k in range(steps):
+            flush.zero_()
+            evs[k][0].record(stream)
+            stats.append(it.unweight(n, iteration=k0 + warmup + k, records=records)[1])
+            evs[k][1].record(stream)
+        stream.synchronize()
+    barrier(pg, dev)
+    it.set_kernel_timing(False)
+    ktimes = it.kernel_times(reset=True)
+    ms = sum(s_.elapsed_time(e_) for s_, e_ in evs)
+    return stats, ms, ktimes
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -157,98 +203,112 @@ def run_ours(a):
     stream = torch.cuda.Stream(device=dev)
     it.set_stream(stream.cuda_stream)
     n = a.points
-
-    # ---- adaptation (untimed in `value`, reported): classic VEGAS refinement, then w_max
-    t0 = time.perf_counter()
-    per, comb = it.integrate(ADAPT_ITERS, ADAPT_POINTS, alpha=1.5, skip=3)
-    wmax = it.weight_quantile(0.999)
-    torch.cuda.synchronize()
-    adapt_s = time.perf_counter() - t0
-
-    cap = n
-    records = torch.empty((cap, RECORD_BYTES), dtype=torch.uint8, device=f"cuda:{dev}")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")   # > 126 MB L2
-    r0 = rank * (a.steps + a.warmup + 1)     # disjoint counter iterations per rank
-
-    def step(k):
-        return it.unweight(n, iteration=1000 + r0 + k, records=records)[1]
+    r0 = 1000 + rank * 100000            # disjoint counter iterations per rank
+    records = torch.empty((n, RECORD_BYTES), dtype=torch.uint8, device=f"cuda:{dev}")
 
     with torch.cuda.stream(stream):
-        for k in range(a.warmup):
-            step(k)
-        barrier(pg, dev)
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-               for _ in range(a.steps)]
-        stats = []
-        with Clocks(dev) as clk:
-            for k in range(a.steps):
-                flush.zero_()
-                evs[k][0].record(stream)
-                stats.append(step(a.warmup + k))
-                evs[k][1].record(stream)
-            stream.synchronize()
-        barrier(pg, dev)
-    ms = sum(s.elapsed_time(e) for s, e in evs)
-    events = sum(s["n_accepted"] for s in stats)
-    sec = allmax(pg, ms / 1e3, dev)
-    events_all = allsum(pg, events, dev)
-    rel_err = max(s["sigma_err"] / s["sigma"] for s in stats)
+        # ---- plain VEGAS form: classic refinement (config 2), w_max = q99.9, production
+        t0 = time.perf_counter()
+        per, comb = it.integrate(ADAPT_ITERS, ADAPT_POINTS, alpha=1.5, skip=3)
+        wmax_plain = it.weight_quantile(0.999)
+        torch.cuda.synchronize()
+        adapt_plain = time.perf_counter() - t0
+        st_p, ms_p, kt_p = production(it, n, records, r0, a.warmup, a.steps, pg, dev, stream)
+
+        # ---- flow + adjoint form: variance-gradient grid refinement (adjoint), flow trained on
+        # the integrator's weights (200 x 65536 points), w_max = q99.9 through the flow
+        t0 = time.perf_counter()
+        ghist = it.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
+        it.flow_init(7)
+        losses = it.flow_train(200, 65536, lr=1e-3)
+        it.flow_enable(True)
+        it.iteration(ADAPT_POINTS, 300, alpha=0.0)
+        wmax_flow = it.weight_quantile(0.999)
+        torch.cuda.synchronize()
+        adapt_flow = time.perf_counter() - t0
+        clk = Clocks(dev)
+        st_f, ms_f, kt_f = production(it, n, records, r0 + 50000, a.warmup, a.steps, pg, dev, stream, clk)
+
+    ev_f = sum(s_["n_accepted"] for s_ in st_f)
+    ev_p = sum(s_["n_accepted"] for s_ in st_p)
+    sec_f = allmax(pg, ms_f / 1e3, dev)
+    sec_p = allmax(pg, ms_p / 1e3, dev)
+    value = allsum(pg, ev_f, dev) / sec_f
+    value_plain = allsum(pg, ev_p, dev) / sec_p
+    rel_err = max(s_["sigma_err"] / s_["sigma"] for s_ in st_f)
 
     # ---- e2e through the host-buffer C-ABI call (grid H2D + records D2H inside the region)
-    eta_max = max(s_["eta"] for s_ in stats)
+    eta_max = max(s_["eta"] for s_ in st_f)
     host = torch.empty((int(n * min(1.0, 1.2 * eta_max)) + 4096, RECORD_BYTES), dtype=torch.uint8,
                        pin_memory=True)
     grid = it.grid
-    e2e_events = 0
-    for k in range(2):   # warm-up of the host path
+    for k in range(2):
         it.grid = grid
-        it.generate_host(n, host, iteration=5000 + r0 + k, chunk=1 << 24)
+        it.generate_host(n, host, iteration=r0 + 90000 + k, chunk=1 << 24)
     barrier(pg, dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e2e_steps = max(1, a.steps // 2)
     e0.record(stream)
     w0 = time.perf_counter()
-    d2h = 0
+    d2h, e2e_events = 0, 0
     for k in range(e2e_steps):
         it.grid = grid
-        s = it.generate_host(n, host, iteration=6000 + r0 + k, chunk=1 << 24)
-        e2e_events += s["n_accepted"]
-        d2h += s["n_accepted"] * RECORD_BYTES
+        s_ = it.generate_host(n, host, iteration=r0 + 91000 + k, chunk=1 << 24)
+        e2e_events += s_["n_accepted"]
+        d2h += s_["n_accepted"] * RECORD_BYTES
     e1.record(stream)
     stream.synchronize()
     wall = time.perf_counter() - w0
     e2e_sec = allmax(pg, max(e0.elapsed_time(e1) / 1e3, wall), dev)
     e2e_all = allsum(pg, e2e_events, dev)
 
-    # ---- roofline of the dominant kernel (k_unw_accept): FP32-pipe work per point
+    # ---- rooflines of the two dominant kernels from their live CUDA-event durations
     peaks, src = measured_peaks()
-    fp32_peak = fp32_peak_tflops(it, stream)
-    ops = FP32_FLOP_PER_POINT
-    achieved = ops * n * a.steps / (ms / 1e3) / 1e12
-    unit_ms = ms / a.steps
+    fp32_peak, mufu_peak = it.measure_peaks()
+    acc_ms, acc_n = kt_f["accept"]
+    flow_ms, flow_n = kt_f["flow_forward"]
+    roof_acc = FP32_FLOP_PER_POINT * n / (acc_ms / acc_n / 1e3) / 1e12
+    roof_flow = FLOW_FLOP_PER_POINT * n / (flow_ms / flow_n / 1e3) / 1e12
+    bf16_peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
+    r_acc = {"bound": "fp32", "kernel": "k_unw_accept", "achieved": roof_acc, "peak": fp32_peak,
+             "unit": "TFLOP/s", "frac": roof_acc / fp32_peak,
+             "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks)",
+             "flop_per_point": FP32_FLOP_PER_POINT, "traffic": None, "ms_per_launch": acc_ms / acc_n}
+    r_flow = {"bound": "tensor", "kernel": "k_flow_fwd", "achieved": roof_flow, "peak": bf16_peak,
+              "unit": "TFLOP/s", "frac": roof_flow / bf16_peak,
+              "peak_source": "MEASURED_PEAKS.json bf16 sustained (%s)" % src,
+              "flop_per_point": FLOW_FLOP_PER_POINT, "traffic": None, "ms_per_launch": flow_ms / flow_n}
+    roof, roof2 = (r_acc, r_flow) if acc_ms >= flow_ms else (r_flow, r_acc)
 
     line = {
-        "metric": METRIC, "value": events_all / sec, "unit": UNIT, "n_gpus": world,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec / a.steps,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec_f / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (counter-based Philox draws, seed 42)",
-        "config": {"workload": WORKLOAD, "form": "plain VEGAS (classic refinement)",
+        "config": {"workload": WORKLOAD, "form": "flow+adjoint: classic VEGAS, variance-gradient (adjoint) grid "
+                   "refinement, BF16 coupling flow trained 200 x 65536 points, unweighting at q99.9",
                    "points_per_step_per_gpu": n, "adapt_points": ADAPT_ITERS * ADAPT_POINTS,
                    "l2": "256 MB buffer written between timed steps; records written per step exceed L2",
                    "parallelism": f"dp{world} (disjoint counter ranges)"},
         "sigma_mb": comb["sigma"], "sigma_err_mb": comb["sigma_err"], "step_sigma_rel_err_max": rel_err,
-        "eta": float(np.mean([s["eta"] for s in stats])), "w_max": wmax,
-        "weighted_points_per_s": n * a.steps * world / sec,
-        "adapt_seconds": adapt_s,
+        "eta": float(np.mean([s_["eta"] for s_ in st_f])), "w_max": wmax_flow,
+        "weighted_points_per_s": n * a.steps * world / sec_f,
+        "plain_vegas": {"value": value_plain, "unit": UNIT, "ms_per_step": 1e3 * sec_p / a.steps,
+                        "eta": float(np.mean([s_["eta"] for s_ in st_p])), "w_max": wmax_plain,
+                        "weighted_points_per_s": n * a.steps * world / sec_p,
+                        "step_sigma_rel_err_max": max(s_["sigma_err"] / s_["sigma"] for s_ in st_p),
+                        "adapt_seconds": adapt_plain},
+        "flow_vs_plain": value / value_plain,
+        "adapt_seconds": adapt_plain + adapt_flow,
+        "flow_training": {"steps": 200, "batch": 65536, "loss_first": float(losses[0]),
+                          "loss_last20": float(np.mean(losses[-20:])), "adjoint_rel_var": ghist[-1]["rel_var"]},
+        "kernel_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in kt_f.items()},
         "e2e": {"value": e2e_all / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": GRID_BYTES,
                 "d2h_bytes_per_step": int(d2h / e2e_steps)},
-        "gpu_launches": 3 * a.steps,
-        "roofline": {"bound": "fp32", "kernel": "k_unw_accept", "achieved": achieved,
-                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks)",
-                     "flop_per_point": ops, "traffic": None, "ms_per_launch": unit_ms,
-                     "hbm_peak_gbs": peaks.get("hbm_gbs"), "hbm_peak_source": src},
+        "gpu_launches": 4 * a.steps,
+        "roofline": roof, "roofline_secondary": roof2,
+        "mufu_peak_tops": mufu_peak,
         "clocks": clk.summary(),
     }
     if rank == 0:
@@ -257,15 +317,6 @@ def run_ours(a):
     it.close()
     if pg is not None:
         pg.destroy_process_group()
-
-
-# FP32 FLOP per point of the fused integrand (FADD + FMUL + 2 FFMA, thread level), from the ncu
-# SASS counters of k_unw_accept on a 2^22-point pass; see profiles/.
-FP32_FLOP_PER_POINT = 3278.0
-
-
-def fp32_peak_tflops(it, stream):
-    return it.measure_peaks()[0]
 
 
 # --------------------------------------------------------------------------- CPU baselines

@@ -86,6 +86,17 @@ class Integrator:
         self._check(self.lib.cp_measure_peaks(self.h, C.byref(f), C.byref(m)))
         return f.value, m.value
 
+    def set_kernel_timing(self, on=True):
+        self._check(self.lib.cp_set_kernel_timing(self.h, 1 if on else 0))
+
+    def kernel_times(self, reset=True):
+        """{kernel: (total ms, launches)} of the production pass since the last reset."""
+        ms = np.zeros(3)
+        n = np.zeros(3, np.uint64)
+        self._check(self.lib.cp_kernel_times(self.h, ms.ctypes.data_as(C.c_void_p), n.ctypes.data_as(C.c_void_p),
+                                             1 if reset else 0))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(["flow_forward", "accept", "build"])}
+
     def sm_count(self):
         n = C.c_int()
         self._check(self.lib.cp_device_sm_count(self.h, C.byref(n)))

@@ -120,6 +120,8 @@ SIGNATURES = {
     "cp_flow_enable": [_P, _i],
     "cp_flow_train": [_P, _i, _u64, _d, _P],
     "cp_flow_loss_grad": [_P, _u64, _u32, _P, _P],
+    "cp_set_kernel_timing": [_P, _i],
+    "cp_kernel_times": [_P, _P, _P, _i],
     "cp_measure_peaks": [_P, C.POINTER(_d), C.POINTER(_d)],
     "cp_vegas_pass_noalloc": [C.POINTER(cp_config), _u64, _u32, _P, _P, _P],
     "cp_partonic_integrate": [_P, _d, _d, _d, _d, _u64, _u64, C.POINTER(cp_result)],

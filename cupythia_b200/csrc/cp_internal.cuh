@@ -78,6 +78,12 @@ struct cp_handle {
   uint64_t flow_buf_cap = 0;
   int flow_on = 0;
   long flow_t = 0;
+  // optional per-kernel timing of the production pass (CUDA events on the handle's stream):
+  // 0 = flow forward, 1 = accept (K1), 2 = record build (K2)
+  int timing = 0;
+  cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double t_ms[3] = {0, 0, 0};
+  uint64_t t_launches[3] = {0, 0, 0};
   std::string err;
 };
 

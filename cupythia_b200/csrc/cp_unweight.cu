@@ -206,6 +206,7 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
   L.flow = nullptr;
+  if (h->timing) cudaEventRecord(h->tev[0], h->stream);
   if (h->flow_on) {
     rc = cp_flow_buffer(h, n);
     if (rc) return rc;
@@ -213,13 +214,26 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
     if (rc) return rc;
     L.flow = h->d_flow_buf;
   }
+  if (h->timing) cudaEventRecord(h->tev[1], h->stream);
   k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
   CP_LAUNCH_CHECK(h, "k_unw_accept");
+  if (h->timing) cudaEventRecord(h->tev[2], h->stream);
   k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
   if (capacity) {
     k_unw_build<<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
     CP_LAUNCH_CHECK(h, "k_unw_build");
+  }
+  if (h->timing) {
+    cudaEventRecord(h->tev[3], h->stream);
+    if (cudaEventSynchronize(h->tev[3]) == cudaSuccess) {
+      float a = 0.f, b = 0.f, c = 0.f;
+      cudaEventElapsedTime(&a, h->tev[0], h->tev[1]);
+      cudaEventElapsedTime(&b, h->tev[1], h->tev[2]);
+      cudaEventElapsedTime(&c, h->tev[2], h->tev[3]);
+      h->t_ms[0] += a; h->t_ms[1] += b; h->t_ms[2] += c;
+      h->t_launches[0] += h->flow_on ? 1 : 0; h->t_launches[1] += 1; h->t_launches[2] += capacity ? 1 : 0;
+    }
   }
   return CP_OK;
 }
@@ -362,5 +376,28 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   if (out) fill_unw(tot, (double)n_points, wm[0], out);
   if (total_acc > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_generate_host: record buffer too small");
   if (tot[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}
+
+// Per-kernel timing of the production pass: on != 0 records CUDA events around the flow forward,
+// the accept kernel and the record builder (plus the tiny slot reduction) on the handle's stream
+// and accumulates their durations; cp_kernel_times reads and optionally resets them.
+extern "C" int cp_set_kernel_timing(cp_handle* h, int on)
+{
+  CP_CHECK_HANDLE(h);
+  if (on && !h->tev[0])
+    for (int k = 0; k < 4; ++k) CP_CUDA(h, cudaEventCreate(&h->tev[k]));
+  h->timing = on ? 1 : 0;
+  return CP_OK;
+}
+
+extern "C" int cp_kernel_times(cp_handle* h, double* ms3, uint64_t* launches3, int reset)
+{
+  CP_CHECK_HANDLE(h);
+  for (int k = 0; k < 3; ++k) {
+    if (ms3) ms3[k] = h->t_ms[k];
+    if (launches3) launches3[k] = h->t_launches[k];
+    if (reset) { h->t_ms[k] = 0.0; h->t_launches[k] = 0; }
+  }
   return CP_OK;
 }

@@ -259,6 +259,12 @@ int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* 
 int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, float* grad_host, double* loss_host);
 
 /* ---------------------------------------------------------------- measurement ------ */
+/* Per-kernel CUDA-event timing of the production pass (cp_unweight / cp_generate_host): slot 0
+ * the flow forward, 1 the accept kernel, 2 the record builder (with the slot reduction).
+ * No reference counterpart (the reference times whole stages with a host clock,
+ * cuPythia/03_fused_resident_me/fused_gg2gg.cu:93-100). */
+int cp_set_kernel_timing(cp_handle* h, int on);
+int cp_kernel_times(cp_handle* h, double* ms3_host, uint64_t* launches3_host, int reset);
 /* FP32 FMA and MUFU (ex2) throughput of the device from dependency-free microbenchmarks:
  * TFLOP/s (2 per FMA) and Tops/s.  No reference counterpart: the integrand's roofline
  * denominators (it is SIMT FP32 / SFU work). */
