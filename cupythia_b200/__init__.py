@@ -236,6 +236,10 @@ class Integrator:
     def flow_enable(self, on=True):
         self._check(self.lib.cp_flow_enable(self.h, 1 if on else 0))
 
+    def flow_kernel(self, which):
+        """Forward kernel: "tcgen05" (TMEM accumulators, default) or "mma" (warp-level mma.sync)."""
+        self._check(self.lib.cp_flow_select_kernel(self.h, {"tcgen05": 0, "mma": 1}[which]))
+
     def flow_train(self, steps, batch=65536, lr=1e-3):
         loss = np.zeros(steps)
         self._check(self.lib.cp_flow_train(self.h, steps, batch, lr, loss.ctypes.data_as(C.c_void_p)))

@@ -118,6 +118,7 @@ SIGNATURES = {
     "cp_flow_set_params": [_P, _P, _i],
     "cp_flow_sample": [_P, _u64, _u64, _u32, _u32, _P],
     "cp_flow_enable": [_P, _i],
+    "cp_flow_select_kernel": [_P, _i],
     "cp_flow_train": [_P, _i, _u64, _d, _P],
     "cp_flow_loss_grad": [_P, _u64, _u32, _P, _P],
     "cp_set_kernel_timing": [_P, _i],

@@ -125,14 +125,14 @@ int cp_flow_ensure(cp_handle* h)
   CP_CUDA(h, cudaMalloc(&h->d_flow_pk, sizeof(uint2) * CP_FLOW_NC * CP_FLOW_P_PER));
   CP_CUDA(h, cudaMalloc(&h->d_flow_bias, sizeof(float) * CP_FLOW_NC * CP_FLOW_NB));
   CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flow_fwd_smem()));
-  return CP_OK;
+  return cp_flow_tc_alloc(h);
 }
 
 int cp_flow_repack(cp_handle* h)
 {
   k_flow_pack<<<CP_FLOW_NC, 256, 0, h->stream>>>(h->d_flow, h->d_flow_pk, h->d_flow_bias);
   CP_LAUNCH_CHECK(h, "k_flow_pack");
-  return CP_OK;
+  return cp_flow_tc_repack(h);
 }
 
 int cp_flow_buffer(cp_handle* h, uint64_t n)
@@ -151,6 +151,7 @@ int cp_flow_buffer(cp_handle* h, uint64_t n)
 // Enqueues the flow forward for points [point0, point0 + n) into out (no synchronisation).
 int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out)
 {
+  if (h->flow_kernel == 0) return cp_flow_tc_enqueue(h, point0, n, iter, stream, out);
   static int per_sm = -1;
   if (per_sm < 0) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_fwd, CP_THREADS, flow_fwd_smem()) != cudaSuccess ||
@@ -212,6 +213,16 @@ extern "C" int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_
   int rc = cp_flow_forward_enqueue(h, point0, n, iter, stream, reinterpret_cast<float4*>(out_dev));
   if (rc) return rc;
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return cp_flow_tc_status(h);
+}
+
+// Selects the flow forward kernel: 0 = tcgen05 (TMEM accumulators, default), 1 = warp-level
+// mma.sync tiles (the kernel the training pass shares).
+extern "C" int cp_flow_select_kernel(cp_handle* h, int which)
+{
+  CP_CHECK_HANDLE(h);
+  if (which != 0 && which != 1) return cp_fail(h, CP_ERR_INVALID, "cp_flow_select_kernel: 0 (tcgen05) or 1 (mma.sync)");
+  h->flow_kernel = which;
   return CP_OK;
 }
 

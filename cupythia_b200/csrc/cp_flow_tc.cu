@@ -1,0 +1,411 @@
+// cp_flow_tc.cu -- the flow forward (sampling) pass on the 5th-generation tensor cores.
+//
+// Same map as k_flow_fwd (Philox words -> VEGAS map -> logit -> 4 affine couplings -> sigmoid),
+// with every dense layer as tcgen05.mma over 128-point tiles: A (activations) and B (weights) in
+// shared memory, the FP32 accumulator in TMEM, one elected thread per warpgroup issuing.
+//
+// Launch: one persistent CTA per SM (the shared-memory footprint admits one), 4 warpgroups of
+// 128 threads.  Each warpgroup owns two 128-point tiles in flight ("slots") with 64 TMEM
+// columns and a 16 KB activation buffer each; thread r of the warpgroup is row r (one point) of
+// both tiles and TMEM lane r.  Per coupling and slot there are three steps
+//   ep1: wait for layer 1, TMEM -> bias-free ReLU -> BF16 -> activation buffer, issue layer 2
+//   ep2: the same for layer 2, issue layer 3
+//   ep3: wait for layer 3, read the 4 output columns, update the point, write the next
+//        coupling's layer-1 input, issue its layer 1
+// and the steps of the two slots alternate, so one slot's MMAs run while the other slot's
+// epilogue runs.  The biases are part of the MMAs: layer 1 has them as input columns 14 and 15
+// (constant 1) times weight rows holding the BF16 high and low parts of the FP32 bias; layers 2
+// and 3 add one K = 16 MMA of a constant block (columns 0 and 1 equal to 1) against the hi/lo
+// bias rows.  hi + lo reproduces the FP32 bias to about 2^-17 relative.
+//
+// Every mbarrier wait is bounded (about 1 s of clock); on expiry the warpgroup stops issuing,
+// finishes its loop without waiting, the kernel sets *status and releases its TMEM.
+#include "cp_flow.cuh"
+#include "cp_internal.cuh"
+#include "cp_tc.cuh"
+
+// weight image of one coupling, bytes (K-major, no swizzle; see cp_tc.cuh)
+#define CP_TC_B1 0        // [N 64][K 16]: W1 rows 0..n_in-1, bias hi/lo in K 14/15
+#define CP_TC_B2 2048     // [N 64][K 64]: W2
+#define CP_TC_B2B 10240   // [N 64][K 16]: b2 hi/lo in K 0/1
+#define CP_TC_B3 12288    // [N 16][K 64]: W3 (outputs 0..7, rest zero)
+#define CP_TC_B3B 14336   // [N 16][K 16]: b3 hi/lo in K 0/1
+#define CP_TC_PER 14848
+#define CP_TC_IMG (CP_FLOW_NC * CP_TC_PER)
+#define CP_TC_WG 4
+#define CP_TC_THREADS (CP_TC_WG * 128)
+#define CP_TC_HBYTES 16384                      // activation buffer of one slot: [128][64] bf16
+#define CP_TC_S_ONES CP_TC_IMG                  // [128][16] bf16 constant block
+#define CP_TC_S_H (CP_TC_S_ONES + 4096)
+#define CP_TC_S_EDGE (CP_TC_S_H + CP_TC_WG * 2 * CP_TC_HBYTES)
+#define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
+#define CP_TC_SMEM (CP_TC_S_MISC + 128 + 1024)  // + slack for 1024-byte alignment of the base
+#define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
+#define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
+
+static_assert(CP_TC_S_H % 1024 == 0, "activation buffers must stay aligned");
+static_assert(CP_TC_SMEM <= 227 * 1024, "shared memory budget");
+
+constexpr uint32_t CP_TC_IDESC64 = cp_tc_idesc_bf16(64);
+constexpr uint32_t CP_TC_IDESC16 = cp_tc_idesc_bf16(16);
+
+// byte offset of element (row r, column k) in a K-major no-swizzle tile of R rows
+__host__ __device__ __forceinline__ int cp_tc_off(int r, int k, int R) { return (k >> 3) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2; }
+
+__device__ __forceinline__ uint16_t cp_bf16_bits(float v)
+{
+  __nv_bfloat16 b = __float2bfloat16_rn(v);
+  return *reinterpret_cast<uint16_t*>(&b);
+}
+__device__ __forceinline__ void cp_bf16_split(float v, uint16_t& hi, uint16_t& lo)
+{
+  hi = cp_bf16_bits(v);
+  lo = cp_bf16_bits(v - __uint_as_float((uint32_t)hi << 16));
+}
+
+// FP32 master parameters -> the shared-memory weight image of every coupling
+__global__ void k_flow_pack_tc(const float* __restrict__ P, uint8_t* __restrict__ img)
+{
+  const int c = blockIdx.x;
+  const CpCoupling kc = cp_coupling(c);
+  const float* W1 = P + c * CP_FLOW_PER + CP_FLOW_W1;
+  const float* b1 = P + c * CP_FLOW_PER + CP_FLOW_B1;
+  const float* W2 = P + c * CP_FLOW_PER + CP_FLOW_W2;
+  const float* b2 = P + c * CP_FLOW_PER + CP_FLOW_B2;
+  const float* W3 = P + c * CP_FLOW_PER + CP_FLOW_W3;
+  const float* b3 = P + c * CP_FLOW_PER + CP_FLOW_B3;
+  uint8_t* q = img + c * CP_TC_PER;
+  for (int e = threadIdx.x; e < CP_TC_PER / 2; e += blockDim.x) {
+    uint16_t v = 0, hi, lo;
+    int off;
+    if (e < 1024) {                       // B1 [64][16]
+      const int nn = e >> 4, k = e & 15;
+      off = CP_TC_B1 + cp_tc_off(nn, k, 64);
+      cp_bf16_split(b1[nn], hi, lo);
+      if (k < kc.nin) v = cp_bf16_bits(W1[k * 64 + nn]);
+      else if (k == 14) v = hi;
+      else if (k == 15) v = lo;
+    } else if (e < 5120) {                // B2 [64][64]
+      const int i = e - 1024, nn = i >> 6, k = i & 63;
+      off = CP_TC_B2 + cp_tc_off(nn, k, 64);
+      v = cp_bf16_bits(W2[k * 64 + nn]);
+    } else if (e < 6144) {                // B2B [64][16]
+      const int i = e - 5120, nn = i >> 4, k = i & 15;
+      off = CP_TC_B2B + cp_tc_off(nn, k, 64);
+      cp_bf16_split(b2[nn], hi, lo);
+      v = k == 0 ? hi : (k == 1 ? lo : (uint16_t)0);
+    } else if (e < 7168) {                // B3 [16][64]
+      const int i = e - 6144, nn = i >> 6, k = i & 63;
+      off = CP_TC_B3 + cp_tc_off(nn, k, 16);
+      if (nn < 8) v = cp_bf16_bits(W3[k * 8 + nn]);
+    } else {                              // B3B [16][16]
+      const int i = e - 7168, nn = i >> 4, k = i & 15;
+      off = CP_TC_B3B + cp_tc_off(nn, k, 16);
+      if (nn < 8) {
+        cp_bf16_split(b3[nn], hi, lo);
+        v = k == 0 ? hi : (k == 1 ? lo : (uint16_t)0);
+      }
+    }
+    *reinterpret_cast<uint16_t*>(q + off) = v;
+  }
+}
+
+// Elementwise transforms of the tensor-core path with the hardware approximations (lg2/ex2 and
+// fast reciprocal; absolute errors of a few 1e-7 in z and ln J).  The log-Jacobian uses the same
+// computed quantities as the map (z' = z e^s + t with ln J += s), so the weights stay consistent.
+__device__ __forceinline__ float cp_tc_logit(float u, float& z)
+{
+  const float lu = __logf(u), l1u = __logf(1.f - u);
+  z = lu - l1u;
+  return -(lu + l1u);
+}
+__device__ __forceinline__ float cp_tc_sigmoid(float z, float& v)
+{
+  const float e = __expf(-fabsf(z));
+  const float inv = __fdividef(1.f, 1.f + e);
+  v = z >= 0.f ? inv : e * inv;
+  return -fabsf(z) - 2.f * __logf(1.f + e);
+}
+// CP_FLOW_S tanh(x / CP_FLOW_S) from one exponential
+__device__ __forceinline__ float cp_tc_softclamp(float x)
+{
+  const float a = fabsf(x) * (2.f / CP_FLOW_S);
+  const float t = __expf(-a);
+  return copysignf(CP_FLOW_S * __fdividef(1.f - t, 1.f + t), x);
+}
+
+struct CpTcPoint {
+  float z0, z1, z2, ld;
+};
+
+__device__ __forceinline__ float cp_sel3(const CpTcPoint& t, int i) { return i == 0 ? t.z0 : (i == 1 ? t.z1 : t.z2); }
+
+// this thread's row of the layer-1 input of coupling c: (in0, in1, 0 ... 0, 1, 1)
+__device__ __forceinline__ void cp_tc_write_in(uint32_t hbuf, int row, int c, const CpTcPoint& t)
+{
+  const CpCoupling k = cp_coupling(c);
+  const float in0 = cp_sel3(t, k.cin[0]);
+  const float in1 = k.nin > 1 ? cp_sel3(t, k.cin[1]) : 0.f;
+  cp_sts128(hbuf + row * 16, cp_bf2(in0, in1), 0u, 0u, 0u);
+  cp_sts128(hbuf + 2048 + row * 16, 0u, 0u, 0u, CP_TC_ONE2);
+}
+
+__device__ __forceinline__ void cp_tc_issue_l1(uint32_t d, uint32_t hbuf, uint32_t w)
+{
+  cp_tc_mma(d, cp_tc_desc(hbuf, 2048, 128), cp_tc_desc(w + CP_TC_B1, 1024, 128), CP_TC_IDESC64, 0u);
+}
+__device__ __forceinline__ void cp_tc_issue_l2(uint32_t d, uint32_t hbuf, uint32_t ones, uint32_t w)
+{
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    cp_tc_mma(d, cp_tc_desc(hbuf + j * 4096, 2048, 128), cp_tc_desc(w + CP_TC_B2 + j * 2048, 1024, 128), CP_TC_IDESC64,
+              j > 0 ? 1u : 0u);
+  cp_tc_mma(d, cp_tc_desc(ones, 2048, 128), cp_tc_desc(w + CP_TC_B2B, 1024, 128), CP_TC_IDESC64, 1u);
+}
+__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint32_t hbuf, uint32_t ones, uint32_t w)
+{
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    cp_tc_mma(d, cp_tc_desc(hbuf + j * 4096, 2048, 128), cp_tc_desc(w + CP_TC_B3 + j * 512, 256, 128), CP_TC_IDESC16,
+              j > 0 ? 1u : 0u);
+  cp_tc_mma(d, cp_tc_desc(ones, 2048, 128), cp_tc_desc(w + CP_TC_B3B, 256, 128), CP_TC_IDESC16, 1u);
+}
+
+// makes this warpgroup's shared-memory writes visible to the tensor core and meets at the
+// warpgroup barrier; afterwards the issuing thread may start MMAs that read them
+__device__ __forceinline__ void cp_tc_publish(uint32_t bar_id)
+{
+  cp_fence_proxy_async();
+  cp_tc_fence_before();
+  cp_bar_wg(bar_id);
+}
+
+// waits for the slot's MMAs (warp-uniform result)
+__device__ __forceinline__ bool cp_tc_wait(uint32_t mbar, uint32_t& phase, volatile int* abort)
+{
+  const bool ok = cp_mbar_wait_bounded(mbar, phase, abort);
+  phase ^= 1u;
+  cp_tc_fence_after();
+  return __all_sync(0xffffffffu, ok);
+}
+
+// TMEM [row][0:64] -> ReLU -> BF16 -> activation buffer row
+__device__ __forceinline__ void cp_tc_hidden_out(uint32_t taddr, uint32_t hbuf, int row, bool ok)
+{
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    float v[32];
+    if (ok) {
+      cp_tc_ld32(taddr + half * 32, v);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = 0.f;
+    }
+#pragma unroll
+    for (int kb = 0; kb < 4; ++kb)
+      cp_sts128(hbuf + (half * 4 + kb) * 2048 + row * 16, cp_relu_bf2(v[8 * kb], v[8 * kb + 1]),
+                cp_relu_bf2(v[8 * kb + 2], v[8 * kb + 3]), cp_relu_bf2(v[8 * kb + 4], v[8 * kb + 5]),
+                cp_relu_bf2(v[8 * kb + 6], v[8 * kb + 7]));
+  }
+}
+
+__global__ void __launch_bounds__(CP_TC_THREADS, 1)
+    k_flow_fwd_tc(const uint4* __restrict__ img_g, const double* __restrict__ edges, int nb, uint64_t seed,
+                  uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* __restrict__ out,
+                  int* __restrict__ status)
+{
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  const uint32_t raw = cp_smem_u32(smem_raw);
+  const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
+  uint8_t* sm = smem_raw + pad;
+  const uint32_t sbase = raw + pad;
+  float2* sEdge = reinterpret_cast<float2*>(sm + CP_TC_S_EDGE);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + CP_TC_S_MISC + 64);
+  int* abort_flags = reinterpret_cast<int*>(sm + CP_TC_S_MISC + 80);
+
+  const int tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, row = tid & 127;
+
+  for (int e = tid; e < CP_TC_IMG / 16; e += CP_TC_THREADS) reinterpret_cast<uint4*>(sm)[e] = img_g[e];
+  for (int e = tid; e < 256; e += CP_TC_THREADS)
+    reinterpret_cast<uint4*>(sm + CP_TC_S_ONES)[e] = e < 128 ? make_uint4(CP_TC_ONE2, 0u, 0u, 0u) : make_uint4(0u, 0u, 0u, 0u);
+  for (int k = tid; k < 3 * nb; k += CP_TC_THREADS) {
+    const int d = k / nb, b = k - d * nb;
+    const double lo = edges[d * (nb + 1) + b], hi = edges[d * (nb + 1) + b + 1];
+    sEdge[d * CP_MAX_BINS + b] = make_float2((float)lo, (float)(hi - lo));
+  }
+  if (tid < CP_TC_WG) abort_flags[tid] = 0;
+  if (tid == 0) {
+    for (int i = 0; i < 2 * CP_TC_WG; ++i) cp_mbar_init(cp_smem_u32(&mbar[i]), 1);
+    cp_mbar_init_fence();
+  }
+  if (warp == 0) {
+    cp_tc_alloc(cp_smem_u32(tmem_slot), CP_TC_TMEM_COLS);
+    cp_tc_relinquish();
+  }
+  cp_fence_proxy_async();
+  cp_tc_fence_before();
+  __syncthreads();
+  cp_tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const uint32_t bar_id = 1 + wg;
+  volatile int* abort = abort_flags + wg;
+  const bool issuer = row == 0;
+  const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+  const uint32_t ones = sbase + CP_TC_S_ONES;
+  uint32_t hb[2], tc[2], mb[2], ph[2] = {0u, 0u};
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    hb[s] = sbase + CP_TC_S_H + (wg * 2 + s) * CP_TC_HBYTES;
+    tc[s] = tmem + (uint32_t)((wg * 2 + s) * 64);
+    mb[s] = cp_smem_u32(&mbar[wg * 2 + s]);
+  }
+
+  const uint64_t npairs = (n + 255) / 256;
+  for (uint64_t q = (uint64_t)blockIdx.x * CP_TC_WG + wg; q < npairs; q += (uint64_t)gridDim.x * CP_TC_WG) {
+    CpTcPoint t[2];
+    uint64_t p[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      p[s] = q * 256 + s * 128 + row;
+      uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
+      if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
+      float jv = 1.f, ld = 0.f, z[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int bin;
+        const float xv = cp_flow_vegas_in(sEdge + d * CP_MAX_BINS, nb, w[d], jv, bin);
+        ld += cp_tc_logit(xv, z[d]);
+      }
+      t[s].z0 = z[0]; t[s].z1 = z[1]; t[s].z2 = z[2];
+      t[s].ld = ld + __logf(jv);
+      cp_tc_write_in(hb[s], row, 0, t[s]);
+    }
+    cp_tc_publish(bar_id);
+    if (issuer && !*abort) {
+      cp_tc_fence_after();
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        cp_tc_issue_l1(tc[s], hb[s], sbase);
+        cp_tc_commit(mb[s]);
+      }
+    }
+#pragma unroll 1
+    for (int c = 0; c < CP_FLOW_NC; ++c) {
+      const uint32_t w = sbase + c * CP_TC_PER;
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {           // ep1: layer-1 output -> layer 2
+        const bool ok = cp_tc_wait(mb[s], ph[s], abort);
+        cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
+        cp_tc_publish(bar_id);
+        if (issuer && !*abort) {
+          cp_tc_fence_after();
+          cp_tc_issue_l2(tc[s], hb[s], ones, w);
+          cp_tc_commit(mb[s]);
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {           // ep2: layer-2 output -> layer 3
+        const bool ok = cp_tc_wait(mb[s], ph[s], abort);
+        cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
+        cp_tc_publish(bar_id);
+        if (issuer && !*abort) {
+          cp_tc_fence_after();
+          cp_tc_issue_l3(tc[s], hb[s], ones, w);
+          cp_tc_commit(mb[s]);
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {           // ep3: coupling update, next coupling's layer 1
+        const bool ok = cp_tc_wait(mb[s], ph[s], abort);
+        float o[4] = {0.f, 0.f, 0.f, 0.f};
+        if (ok) cp_tc_ld4(tc[s] + lane_base, o);
+        const CpCoupling k = cp_coupling(c);
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          if (j >= k.nt) break;
+          const float sc = cp_tc_softclamp(o[j]), sh = o[k.nt + j];
+          const int d = k.tr[j];
+          const float zn = fmaf(cp_sel3(t[s], d), __expf(sc), sh);
+          if (d == 0) t[s].z0 = zn;
+          else if (d == 1) t[s].z1 = zn;
+          else t[s].z2 = zn;
+          t[s].ld += sc;
+        }
+        if (c + 1 < CP_FLOW_NC) {
+          cp_tc_write_in(hb[s], row, c + 1, t[s]);
+          cp_tc_publish(bar_id);
+          if (issuer && !*abort) {
+            cp_tc_fence_after();
+            cp_tc_issue_l1(tc[s], hb[s], w + CP_TC_PER);
+            cp_tc_commit(mb[s]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      float v0, v1, v2;
+      float ld = t[s].ld;
+      ld += cp_tc_sigmoid(t[s].z0, v0);
+      ld += cp_tc_sigmoid(t[s].z1, v1);
+      ld += cp_tc_sigmoid(t[s].z2, v2);
+      if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+    }
+    if (cp_bar_wg_or(bar_id, *abort != 0)) break;
+  }
+  if (issuer && *abort) atomicOr(status, 1);
+  cp_tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    cp_tc_fence_after();
+    cp_tc_dealloc(tmem, CP_TC_TMEM_COLS);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------
+int cp_flow_tc_repack(cp_handle* h)
+{
+  k_flow_pack_tc<<<CP_FLOW_NC, 256, 0, h->stream>>>(h->d_flow, h->d_flow_tc);
+  CP_LAUNCH_CHECK(h, "k_flow_pack_tc");
+  return CP_OK;
+}
+
+int cp_flow_tc_alloc(cp_handle* h)
+{
+  if (!h->d_flow_tc) CP_CUDA(h, cudaMalloc(&h->d_flow_tc, CP_TC_IMG));
+  if (!h->d_flow_status) {
+    CP_CUDA(h, cudaMalloc(&h->d_flow_status, sizeof(int)));
+    CP_CUDA(h, cudaMemsetAsync(h->d_flow_status, 0, sizeof(int), h->stream));
+  }
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CP_TC_SMEM));
+  return CP_OK;
+}
+
+int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out)
+{
+  const uint64_t pairs = (n + 255) / 256;
+  const uint64_t want = (pairs + CP_TC_WG - 1) / CP_TC_WG;
+  const int grid = (int)(want < (uint64_t)h->num_sms ? want : (uint64_t)h->num_sms);
+  if (grid < 1) return CP_OK;
+  k_flow_fwd_tc<<<grid, CP_TC_THREADS, CP_TC_SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_edges,
+                                                                 h->nb, h->cfg.seed, point0, n, iter, stream, out,
+                                                                 h->d_flow_status);
+  CP_LAUNCH_CHECK(h, "k_flow_fwd_tc");
+  return CP_OK;
+}
+
+// Reads and clears the device status of the tensor-core flow kernel (after the stream has
+// been synchronised): CP_ERR_TIMEOUT if a bounded wait expired since the last check.
+int cp_flow_tc_status(cp_handle* h)
+{
+  if (!h->d_flow_status) return CP_OK;
+  int s = 0;
+  CP_CUDA(h, cudaMemcpy(&s, h->d_flow_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!s) return CP_OK;
+  CP_CUDA(h, cudaMemset(h->d_flow_status, 0, sizeof(int)));
+  return cp_fail(h, CP_ERR_TIMEOUT, "k_flow_fwd_tc: a tensor-core wait expired (results of this pass are invalid)");
+}

@@ -337,8 +337,10 @@ __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g
 }
 
 // ------------------------------------------------------------------------------------------
-// 4. weight gradients G[M][N] += sum_p A[p][0:M]^T B[p][0:N] on the tensor cores
-//    (A, B bf16 row-major with leading dims lda = M, ldb = N; M in {16, 64}, N in {16, 64})
+// 4. weight and bias gradients of one layer shape for all couplings (blockIdx.y = coupling):
+//    G[M][N] += sum_p A[p][0:M]^T B[p][0:N] on the tensor cores, and the bias gradient
+//    Gb[N] += sum_p B[p][0:N] from the same staged tiles
+//    (A, B bf16 row-major with leading dims M and N; M in {16, 64}, N in {16, 64})
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void cp_ldsm_x4_t(uint32_t r[4], const void* p)
 {
@@ -347,49 +349,64 @@ __device__ __forceinline__ void cp_ldsm_x4_t(uint32_t r[4], const void* p)
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
 }
 
+#define CP_WG_ROWS 64   // points staged per iteration
+
 template <int M, int N>
-__global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
-                                                    uint64_t n, float* __restrict__ G, int ldg, int nvalid, int chunk)
+__global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__ A0, const uint16_t* __restrict__ B0,
+                                                    uint64_t n, float* __restrict__ G0, int ldg, int nvalid, int chunk,
+                                                    int bias_rel)
 {
   constexpr int MT = M / 16, NT = N / 8, TPW = (MT * NT + 3) / 4;
-  __shared__ __align__(16) uint16_t sA[16 * M];
-  __shared__ __align__(16) uint16_t sB[16 * N];
+  __shared__ __align__(16) uint16_t sA[CP_WG_ROWS * M];
+  __shared__ __align__(16) uint16_t sB[CP_WG_ROWS * N];
+  const int c = blockIdx.y;
+  const uint16_t* A = A0 + (uint64_t)c * n * M;
+  const uint16_t* B = B0 + (uint64_t)c * n * N;
+  float* G = G0 + c * CP_FLOW_PER;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
   const int mi = lane >> 3, rw = lane & 7;
   float acc[TPW][4];
 #pragma unroll
   for (int j = 0; j < TPW; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  const int bcol = threadIdx.x % N, brow0 = threadIdx.x / N;
+  float bsum = 0.f;
   const uint64_t p_begin = (uint64_t)blockIdx.x * chunk;
   const uint64_t p_end = p_begin + chunk < n ? p_begin + chunk : n;
-  for (uint64_t p0 = p_begin; p0 < p_end; p0 += 16) {
-    for (int e = threadIdx.x; e < 16 * M / 8; e += blockDim.x) {
+  for (uint64_t p0 = p_begin; p0 < p_end; p0 += CP_WG_ROWS) {
+    for (int e = threadIdx.x; e < CP_WG_ROWS * M / 8; e += blockDim.x) {
       const int row = e / (M / 8), col = (e % (M / 8)) * 8;
       uint4 v = make_uint4(0, 0, 0, 0);
       if (p0 + row < p_end) v = *reinterpret_cast<const uint4*>(A + (p0 + row) * M + col);
       *reinterpret_cast<uint4*>(&sA[row * M + col]) = v;
     }
-    for (int e = threadIdx.x; e < 16 * N / 8; e += blockDim.x) {
+    for (int e = threadIdx.x; e < CP_WG_ROWS * N / 8; e += blockDim.x) {
       const int row = e / (N / 8), col = (e % (N / 8)) * 8;
       uint4 v = make_uint4(0, 0, 0, 0);
       if (p0 + row < p_end) v = *reinterpret_cast<const uint4*>(B + (p0 + row) * N + col);
       *reinterpret_cast<uint4*>(&sB[row * N + col]) = v;
     }
     __syncthreads();
+    for (int r = brow0; r < CP_WG_ROWS; r += 128 / N) bsum += __uint_as_float(((uint32_t)sB[r * N + bcol]) << 16);
 #pragma unroll
-    for (int j = 0; j < TPW; ++j) {
-      const int t = warp + 4 * j;
-      if (t < MT * NT) {
-        const int mt = t / NT, nt = t % NT;
-        uint32_t a[4], bq[2];
-        // A^T of m-tile mt: 8x8 blocks (points 0-7 | 8-15) x (m +0 | +8), delivered transposed
-        cp_ldsm_x4_t(a, &sA[((mi >> 1) * 8 + rw) * M + mt * 16 + (mi & 1) * 8]);
-        // B of n-tile nt: blocks (points 0-7 | 8-15) x (n tile), delivered transposed
-        {
-          const uint32_t ad = (uint32_t)__cvta_generic_to_shared(&sB[((mi & 1) * 8 + rw) * N + nt * 8]);
-          asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
-                       : "=r"(bq[0]), "=r"(bq[1]) : "r"(ad));
+    for (int ks = 0; ks < CP_WG_ROWS / 16; ++ks) {
+      const uint16_t* tA = sA + ks * 16 * M;
+      const uint16_t* tB = sB + ks * 16 * N;
+#pragma unroll
+      for (int j = 0; j < TPW; ++j) {
+        const int t = warp + 4 * j;
+        if (t < MT * NT) {
+          const int mt = t / NT, nt = t % NT;
+          uint32_t a[4], bq[2];
+          // A^T of m-tile mt: 8x8 blocks (points 0-7 | 8-15) x (m +0 | +8), delivered transposed
+          cp_ldsm_x4_t(a, &tA[((mi >> 1) * 8 + rw) * M + mt * 16 + (mi & 1) * 8]);
+          // B of n-tile nt: blocks (points 0-7 | 8-15) x (n tile), delivered transposed
+          {
+            const uint32_t ad = (uint32_t)__cvta_generic_to_shared(&tB[((mi & 1) * 8 + rw) * N + nt * 8]);
+            asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];\n"
+                         : "=r"(bq[0]), "=r"(bq[1]) : "r"(ad));
+          }
+          cp_mma_bf16(acc[j], a, make_uint2(bq[0], bq[1]));
         }
-        cp_mma_bf16(acc[j], a, make_uint2(bq[0], bq[1]));
       }
     }
     __syncthreads();
@@ -403,17 +420,7 @@ __global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__
     if (n0 < nvalid) { atomicAdd(&G[m0 * ldg + n0], acc[j][0]); atomicAdd(&G[(m0 + 8) * ldg + n0], acc[j][2]); }
     if (n0 + 1 < nvalid) { atomicAdd(&G[m0 * ldg + n0 + 1], acc[j][1]); atomicAdd(&G[(m0 + 8) * ldg + n0 + 1], acc[j][3]); }
   }
-}
-
-// column sums of a bf16 [n][ld] array (bias gradients)
-__global__ void k_flow_colsum(const uint16_t* __restrict__ D, uint64_t n, int ld, int ncols, float* __restrict__ out)
-{
-  const int col = threadIdx.x % ncols;
-  const int lanes = blockDim.x / ncols;
-  float s = 0.f;
-  for (uint64_t p = (uint64_t)blockIdx.x * lanes + threadIdx.x / ncols; p < n; p += (uint64_t)gridDim.x * lanes)
-    s += __uint_as_float(((uint32_t)D[p * ld + col]) << 16);
-  if ((int)threadIdx.x < lanes * ncols) atomicAdd(&out[col], s);
+  if (bcol < nvalid) atomicAdd(&G[bias_rel + bcol], bsum);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -508,23 +515,17 @@ static int flow_train_step(cp_handle* h, const FlowTrainBufs& t, uint64_t B, uin
   k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, B, t.zs, t.vj, t.wg, t.sums, t);
   CP_LAUNCH_CHECK(h, "k_flow_bwd");
   float* G = h->d_flow + CP_FLOW_NPARAM;
-  const int chunk = 4096;
-  const int cblk = (int)((B + chunk - 1) / chunk);
-  for (int c = 0; c < CP_FLOW_NC; ++c) {
-    float* g = G + c * CP_FLOW_PER;
-    k_flow_wgrad<16, 64><<<cblk, 128, 0, h->stream>>>(t.X + (uint64_t)c * B * 16, t.D1 + (uint64_t)c * B * 64, B,
-                                                      g + CP_FLOW_W1, 64, 64, chunk);
-    k_flow_wgrad<64, 64><<<cblk, 128, 0, h->stream>>>(t.H1 + (uint64_t)c * B * 64, t.D2 + (uint64_t)c * B * 64, B,
-                                                      g + CP_FLOW_W2, 64, 64, chunk);
-    // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
-    k_flow_wgrad<64, 16><<<cblk, 128, 0, h->stream>>>(t.H2 + (uint64_t)c * B * 64, t.DO + (uint64_t)c * B * 16, B,
-                                                      g + CP_FLOW_W3, 8, 8, chunk);
-    CP_LAUNCH_CHECK(h, "k_flow_wgrad");
-    k_flow_colsum<<<64, 256, 0, h->stream>>>(t.D1 + (uint64_t)c * B * 64, B, 64, 64, g + CP_FLOW_B1);
-    k_flow_colsum<<<64, 256, 0, h->stream>>>(t.D2 + (uint64_t)c * B * 64, B, 64, 64, g + CP_FLOW_B2);
-    k_flow_colsum<<<64, 256, 0, h->stream>>>(t.DO + (uint64_t)c * B * 16, B, 16, 8, g + CP_FLOW_B3);
-    CP_LAUNCH_CHECK(h, "k_flow_colsum");
-  }
+  // about 64 blocks per coupling and layer; chunks are whole multiples of the staged rows
+  const uint64_t chunk = ((B + 63) / 64 + CP_WG_ROWS - 1) / CP_WG_ROWS * CP_WG_ROWS;
+  const dim3 grid((unsigned)((B + chunk - 1) / chunk), CP_FLOW_NC);
+  k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, B, G + CP_FLOW_W1, 64, 64, (int)chunk,
+                                                    CP_FLOW_B1 - CP_FLOW_W1);
+  k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, B, G + CP_FLOW_W2, 64, 64, (int)chunk,
+                                                    CP_FLOW_B2 - CP_FLOW_W2);
+  // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
+  k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, B, G + CP_FLOW_W3, 8, 8, (int)chunk,
+                                                    CP_FLOW_B3 - CP_FLOW_W3);
+  CP_LAUNCH_CHECK(h, "k_flow_wgrad");
   return CP_OK;
 }
 

@@ -78,6 +78,11 @@ struct cp_handle {
   uint64_t flow_buf_cap = 0;
   int flow_on = 0;
   long flow_t = 0;
+  // tensor-core (tcgen05) forward: shared-memory weight image, bounded-wait status flag;
+  // flow_kernel 0 = tcgen05 kernel, 1 = the warp-level mma.sync kernel
+  uint8_t* d_flow_tc = nullptr;
+  int* d_flow_status = nullptr;
+  int flow_kernel = 0;
   // optional per-kernel timing of the production pass (CUDA events on the handle's stream):
   // 0 = flow forward, 1 = accept (K1), 2 = record build (K2)
   int timing = 0;
@@ -93,6 +98,10 @@ int cp_ensure_slots(cp_handle* h, size_t doubles);
 int cp_ensure_iters(cp_handle* h, int n);
 int cp_flow_buffer(cp_handle* h, uint64_t n);
 int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out);
+int cp_flow_tc_alloc(cp_handle* h);
+int cp_flow_tc_repack(cp_handle* h);
+int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out);
+int cp_flow_tc_status(cp_handle* h);
 
 #define CP_CHECK_HANDLE(h) \
   do { if (!(h)) return CP_ERR_INVALID; } while (0)

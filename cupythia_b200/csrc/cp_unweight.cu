@@ -282,6 +282,7 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   CP_CUDA(h, cudaMemcpyAsync(red, h->d_red, sizeof red, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaMemcpyAsync(&cnt, h->d_counter, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   if (out) fill_unw(red, (double)n_points, wm[0], out);
   if (cnt > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_unweight: record buffer too small (n_accepted reported)");
   if (red[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
@@ -367,6 +368,7 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   if (cnt) cudaFree(cnt);
   if (e != cudaSuccess) return cp_fail_cuda(h, e, "cp_generate_host");
   if (rc) return rc;
+  if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   uint64_t total_acc = 0;
   for (uint64_t c = 0; c < nchunks; ++c) {

@@ -290,6 +290,7 @@ extern "C" int cp_vegas_iteration(cp_handle* h, uint64_t n_points, uint32_t iter
   CpIterDev r;
   CP_CUDA(h, cudaMemcpyAsync(&r, h->d_iters, sizeof r, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   if (out) fill_result(r, out);
   if (r.nbad > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
   return CP_OK;
@@ -314,6 +315,7 @@ extern "C" int cp_integrate(cp_handle* h, int n_iter, uint64_t n_points, double 
                                   cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) { delete[] recs; return cp_fail_cuda(h, e, "cp_integrate readback"); }
+  if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) { delete[] recs; return rc; }
   double wsum = 0, w2 = 0, sw = 0, sw2 = 0, wmax = 0, nbad = 0, npts = 0;
   for (int it = 0; it < n_iter; ++it) {
     if (per_iter) fill_result(recs[it], per_iter + it);

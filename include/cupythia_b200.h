@@ -235,9 +235,9 @@ int cp_adjoint(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream, 
 int cp_vegas_gradient_step(cp_handle* h, uint64_t n_points, uint32_t iter, double lr, cp_grad* out_host);
 
 /* ---------------------------------------------------------------- learned proposal -- */
-/* A RealNVP-style flow on [0,1]^3 in front of the VEGAS map: logit, 4 affine couplings (MLP
- * in -> 64 -> 64 -> out, ReLU, BF16 weights and activations on the tensor cores, FP32
- * accumulation), sigmoid.  No reference counterpart (the reference has no learned proposal).
+/* A RealNVP-style flow on [0,1]^3 after the VEGAS map (between it and the base phase-space map):
+ * logit, 4 affine couplings (MLP in -> 64 -> 64 -> out, ReLU, BF16 weights and activations on
+ * the tensor cores, FP32 accumulation), sigmoid.  No reference counterpart (the reference has no learned proposal).
  * FP32 master parameters: cp_flow_num_params() floats in the layout of cupythia_b200/csrc/cp_flow.cuh. */
 int cp_flow_num_params(void);
 /* Xavier-uniform weights from the counter RNG with key `seed` (7 in the production recipe),
@@ -248,6 +248,10 @@ int cp_flow_set_params(cp_handle* h, const float* params_host, int n);
 /* Flow samples of points [point0, point0+n), counter (iter, stream): out (dev, 16-byte aligned)
  * holds (v0, v1, v2, ln|dv/du|) per point. */
 int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float* out_dev);
+/* Forward kernel used by cp_flow_sample and the flow-routed passes: 0 = tcgen05 MMAs with TMEM
+ * accumulators over 128-point tiles (default), 1 = warp-level mma.sync tiles.  Both compute the
+ * same map; CP_ERR_TIMEOUT from a flow-routed call means a bounded tensor-core wait expired. */
+int cp_flow_select_kernel(cp_handle* h, int which);
 /* Routes cp_vegas_iteration / cp_integrate / cp_point_weights / cp_unweight / cp_generate_host
  * through the flow (on = 1) or the Philox words directly (on = 0). */
 int cp_flow_enable(cp_handle* h, int on);

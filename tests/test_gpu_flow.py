@@ -95,6 +95,26 @@ def test_flow_forward_matches_fp64_oracle(integ, orc):
     assert np.median(np.abs(ref[:, :3] - u)) > 1e-3
 
 
+def test_tcgen05_forward_matches_mma_forward(integ):
+    """The tcgen05 kernel (TMEM accumulators, biases inside the MMAs as BF16 hi/lo pairs) and the
+    warp-level mma.sync kernel compute the same map; they differ by FP32 accumulation order and
+    the ~2^-17 bias split, which moves a BF16 rounding of a hidden unit now and then."""
+    integ.reset_grid()
+    integ.integrate(3, 1 << 20, alpha=1.5)
+    _random_flow(integ, seed=11)
+    n = 100_003                                    # ragged: not a multiple of the 256-point tile pair
+    integ.flow_kernel("mma")
+    ref = integ.flow_sample(17, n, 5, 0).cpu().numpy().astype(np.float64)
+    integ.flow_kernel("tcgen05")
+    out = integ.flow_sample(17, n, 5, 0).cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(out))
+    dv = np.abs(out[:, :3] - ref[:, :3]).max(1)
+    dj = np.abs(out[:, 3] - ref[:, 3])
+    assert np.percentile(dv, 99.9) < 2e-3 and np.median(dv) < 1e-5, (np.median(dv), np.percentile(dv, 99.9))
+    assert np.percentile(dj, 99.9) < 2e-2 and np.median(dj) < 1e-4, (np.median(dj), np.percentile(dj, 99.9))
+    integ.reset_grid()
+
+
 def _cpu_cotangents(it, orc, flow_out, n):
     """(w, d ln f/dx) at the flow's points from the FP64 oracle (complex step), as the GPU forms them."""
     L = orc.lib()
