@@ -220,7 +220,7 @@ def run_ours(a):
         t0 = time.perf_counter()
         ghist = it.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
         it.flow_init(7)
-        losses = it.flow_train(200, 65536, lr=1e-3)
+        losses = it.flow_train(200, 65536, lr=8e-3)
         it.flow_enable(True)
         it.iteration(ADAPT_POINTS, 300, alpha=0.0)
         wmax_flow = it.weight_quantile(0.999)

@@ -9,6 +9,7 @@ Device buffers are torch CUDA tensors; torch is only the allocator here, every n
 computed by the library's own kernels.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -17,7 +18,7 @@ from ._lib import (CP_PROC_ALL, CP_PROC_GG2GG, CP_PROC_GG2QQBAR, CP_PROC_QG2QG, 
                    CP_PROC_QQ2QQ, CP_PROC_QQBAR2GG, CpError, cp_config, cp_event, cp_grad,
                    cp_result, cp_unweight_result)
 
-__all__ = ["Integrator", "CpError", "default_config", "CP_PROC_ALL"]
+__all__ = ["Integrator", "CpError", "default_config", "CP_PROC_ALL", "events_view", "colour_tags", "write_lhef"]
 
 
 def _torch():
@@ -306,10 +307,49 @@ class Integrator:
 
 
 EVENT_DTYPE = np.dtype([("id", "<i2", 4), ("pz_in", "<f4", 2), ("p3", "<f4", 4), ("p4", "<f4", 4),
-                        ("weight", "<f4"), ("pt_hat", "<f4"), ("process", "<u4"), ("point", "<u4")])
+                        ("weight", "<f4"), ("pt_hat", "<f4"), ("process", "<u2"), ("colour", "<u2"),
+                        ("point", "<u4")])
 
 
 def events_view(records):
     """Structured numpy view (cp_event layout) of a [n, 64] uint8 record array or tensor."""
     a = records.cpu().numpy() if hasattr(records, "cpu") else np.asarray(records)
     return np.ascontiguousarray(a).view(EVENT_DTYPE).reshape(-1)
+
+
+def colour_tags(events):
+    """(col, acol) int arrays [n, 4] of structured records (EVENT_DTYPE): colour indices 1..4 of
+    the flow each record's process chose (cp_colour_tags), 0 = no colour."""
+    lib = _lib.load()
+    ev = np.asarray(events)
+    col = np.zeros((len(ev), 4), np.int32)
+    acol = np.zeros((len(ev), 4), np.int32)
+    cache = {}
+    for i, (p, c) in enumerate(zip(ev["process"].tolist(), ev["colour"].tolist())):
+        key = (p, c)
+        if key not in cache:
+            a = (C.c_int * 4)()
+            b = (C.c_int * 4)()
+            rc = lib.cp_colour_tags(p, c, a, b)
+            if rc:
+                raise CpError(rc, f"invalid colour flow {c} for process {p}")
+            cache[key] = (list(a), list(b))
+        col[i], acol[i] = cache[key]
+    return col, acol
+
+
+def write_lhef(path, records, sigma_mb, sigma_err_mb, cfg=None):
+    """Les Houches Event File 3.0 of host or device records (cp_write_lhef); cfg defaults to the
+    library's default configuration."""
+    lib = _lib.load()
+    if cfg is None:
+        cfg = cp_config()
+        lib.cp_config_default(C.byref(cfg))
+    a = records.cpu().numpy() if hasattr(records, "cpu") else np.asarray(records)
+    a = np.ascontiguousarray(a)
+    n = a.nbytes // 64
+    rc = lib.cp_write_lhef(C.byref(cfg), a.ctypes.data_as(C.c_void_p), n, sigma_mb, sigma_err_mb,
+                           os.fsencode(str(path)))
+    if rc:
+        raise CpError(rc, "cp_write_lhef failed")
+

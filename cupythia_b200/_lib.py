@@ -50,7 +50,7 @@ class cp_event(C.Structure):
     _fields_ = [
         ("id", C.c_int16 * 4), ("pz_in", C.c_float * 2), ("p3", C.c_float * 4),
         ("p4", C.c_float * 4), ("weight", C.c_float), ("pt_hat", C.c_float),
-        ("process", C.c_uint32), ("point", C.c_uint32),
+        ("process", C.c_uint16), ("colour", C.c_uint16), ("point", C.c_uint32),
     ]
 
 
@@ -119,6 +119,8 @@ SIGNATURES = {
     "cp_flow_sample": [_P, _u64, _u64, _u32, _u32, _P],
     "cp_flow_enable": [_P, _i],
     "cp_flow_select_kernel": [_P, _i],
+    "cp_colour_tags": [C.c_uint16, C.c_uint16, _P, _P],
+    "cp_write_lhef": [C.POINTER(cp_config), _P, _u64, _d, _d, C.c_char_p],
     "cp_flow_train": [_P, _i, _u64, _d, _P],
     "cp_flow_loss_grad": [_P, _u64, _u32, _P, _P],
     "cp_set_kernel_timing": [_P, _i],

@@ -398,7 +398,8 @@ struct CpEventRec {
   float p4[4];
   float weight;
   float pt_hat;
-  uint32_t process;
+  uint16_t process;
+  uint16_t colour;
   uint32_t point;
 };
 
@@ -512,15 +513,59 @@ CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, f
   } else { id[2] = a; id[3] = bb; }
 }
 
+// Colour flow of the process's setIdColAcol (pythia8317/src/SigmaQCD.cc: Sigma2gg2gg :135-148,
+// Sigma2gg2qqbar :195-205, Sigma2qg2qg :232-244, Sigma2qq2qq :292-304, Sigma2qqbar2gg
+// :331-342): the topology is drawn with rc in proportion to its kinematic term, the gg -> gg
+// orientation with rs.  Encoded as: bits 0-1 topology index (order of the setColAcol calls in
+// the source), bit 2 swapColAcol applied, bit 3 swapCol1234 applied.  tp = tHat/sHat,
+// up = uHat/sHat; common factors of the terms are dropped.
+CP_HD uint32_t cp_colour_flow(int code, const int id[4], float tp, float up, float rc, float rs)
+{
+  uint32_t topo = 0, swapCA = 0, swap12 = 0;
+  if (code == 111) {
+    const float rt = 1.f / tp, ru = 1.f / up, tu = tp * ru, ut = up * rt;
+    const float a = (tp + 1.f) * (tp + 1.f) + (rt + 1.f) * (rt + 1.f) + 1.f;
+    const float b = (up + 1.f) * (up + 1.f) + (ru + 1.f) * (ru + 1.f) + 1.f;
+    const float c = (tu + 1.f) * (tu + 1.f) + (ut + 1.f) * (ut + 1.f) + 1.f;
+    const float r = (a + b + c) * rc;
+    topo = r < a ? 0u : (r < a + b ? 1u : 2u);
+    swapCA = rs > 0.5f ? 1u : 0u;
+  } else if (code == 112) {
+    const float a = (1.f / 6.f) * (up / tp) - 0.375f * up * up;
+    const float b = (1.f / 6.f) * (tp / up) - 0.375f * tp * tp;
+    topo = (a + b) * rc < a ? 0u : 1u;
+  } else if (code == 113) {
+    const float a = (up / tp) * (up / tp) - (4.f / 9.f) * up;
+    const float b = 1.f / (tp * tp) - (4.f / 9.f) / up;
+    topo = (a + b) * rc < a ? 0u : 1u;
+    swap12 = id[0] == 21 ? 1u : 0u;
+    swapCA = (id[0] < 0 || id[1] < 0) ? 1u : 0u;
+  } else if (code == 114) {
+    topo = id[0] * id[1] > 0 ? 0u : 1u;
+    if (id[1] == id[0]) {
+      const float T = (1.f + up * up) / (tp * tp), U = (1.f + tp * tp) / (up * up);
+      if ((T + U) * rc > T) topo = 2u;
+    }
+    swapCA = id[0] < 0 ? 1u : 0u;
+  } else {
+    const float a = (32.f / 27.f) * (up / tp) - (8.f / 3.f) * up * up;
+    const float b = (32.f / 27.f) * (tp / up) - (8.f / 3.f) * tp * tp;
+    topo = (a + b) * rc < a ? 0u : 1u;
+    swapCA = id[0] < 0 ? 1u : 0u;
+  }
+  return topo | (swapCA << 2) | (swap12 << 3);
+}
+
 // Lab-frame four-momenta: parton 3 at cos(theta*) = z from beam A, azimuth phi; boost by the
 // rapidity y = (ln x1 - ln x2)/2 of the parton system (massless, PhaseSpace.cc 2 -> 2 kinematics).
 CP_HD void cp_make_event(const CpHadParams& P, const CpPoint& pt, float r0, float r1, float r2,
-                         float r3, float weight, uint32_t point, CpEventRec& ev)
+                         float r3, float rc, float rs, float weight, uint32_t point, CpEventRec& ev)
 {
   int code, id[4];
   cp_pick_flavours(P, pt, r0, r1, r3, code, id);
   for (int k = 0; k < 4; ++k) ev.id[k] = (int16_t)id[k];
   const CpKin& k = pt.k;
+  ev.colour = (uint16_t)cp_colour_flow(code, id, -0.5f * k.omz, -0.5f * k.opz, rc, rs);
   float eBeam = 0.5f * cp_sqrtf(P.s);
   float x1 = cp_expf(k.lnx1), x2 = cp_expf(k.lnx2);
   ev.pz_in[0] = eBeam * x1;
@@ -546,6 +591,6 @@ CP_HD void cp_make_event(const CpHadParams& P, const CpPoint& pt, float r0, floa
   ev.p4[2] = -pzs * ch + pstar * sh; ev.p4[3] = pstar * ch - pzs * sh;
   ev.weight = weight;
   ev.pt_hat = cp_sqrtf(k.pT2);
-  ev.process = (uint32_t)code;
+  ev.process = (uint16_t)code;
   ev.point = point;
 }

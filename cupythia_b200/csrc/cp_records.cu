@@ -1,0 +1,114 @@
+// cp_records.cu -- host-side consumers of the 64-byte event records: colour tags of the encoded
+// colour flow, and a Les Houches Event File (LHEF 3.0) writer.  Host code only: these entry
+// points need no GPU.
+//
+// The LHEF layout follows the Les Houches accord as the reference writes it
+// (cuPythia/pipeline/lhe_writer.cu:46-70, cuPythia/07_unweighting_lhe/unweight_lhe.cu:74-102):
+// <init> with the beam line (IDBMUP EBMUP PDFGUP PDFSUP IDWTUP NPRUP) and one line per process
+// (XSECUP XERRUP XMAXUP LPRUP), then one <event> per record with NUP IDPRUP XWGTUP SCALUP AQEDUP
+// AQCDUP and one line per parton (IDUP ISTUP MOTHUP1 MOTHUP2 ICOLUP1 ICOLUP2 PUP1..5 VTIMUP
+// SPINUP).  Unlike the reference (one process, a fixed gg -> gg colour ring) every record
+// carries its own process code and the colour flow its setIdColAcol chose.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include "cp_internal.cuh"
+
+// colour topologies in the order of the setColAcol calls of each process's setIdColAcol
+// (pythia8317/src/SigmaQCD.cc), (col1, acol1, col2, acol2, col3, acol3, col4, acol4)
+static const int8_t kTopo[5][3][8] = {
+    {{1, 2, 2, 3, 1, 4, 4, 3}, {1, 2, 3, 1, 3, 4, 4, 2}, {1, 2, 3, 4, 1, 4, 3, 2}},   // 111 g g -> g g
+    {{1, 2, 2, 3, 1, 0, 0, 3}, {1, 2, 3, 1, 3, 0, 0, 2}, {0, 0, 0, 0, 0, 0, 0, 0}},   // 112 g g -> q qbar
+    {{1, 0, 2, 1, 3, 0, 2, 3}, {1, 0, 2, 3, 2, 0, 1, 3}, {0, 0, 0, 0, 0, 0, 0, 0}},   // 113 q g -> q g
+    {{1, 0, 2, 0, 2, 0, 1, 0}, {1, 0, 0, 1, 2, 0, 0, 2}, {1, 0, 2, 0, 1, 0, 2, 0}},   // 114 q q -> q q
+    {{1, 0, 0, 2, 1, 3, 3, 2}, {1, 0, 0, 2, 3, 2, 1, 3}, {0, 0, 0, 0, 0, 0, 0, 0}}};  // 115 q qbar -> g g
+
+extern "C" int cp_colour_tags(uint16_t process, uint16_t colour, int col[4], int acol[4])
+{
+  if (process < 111 || process > 115 || !col || !acol) return CP_ERR_INVALID;
+  const int topo = colour & 3;
+  if (topo > 2 || (topo == 2 && process != 111 && process != 114)) return CP_ERR_INVALID;
+  const int8_t* t = kTopo[process - 111][topo];
+  int c[4], a[4];
+  for (int k = 0; k < 4; ++k) { c[k] = t[2 * k]; a[k] = t[2 * k + 1]; }
+  if (colour & 8) {   // swapCol1234: partons 1 <-> 2 and 3 <-> 4
+    int x;
+    x = c[0]; c[0] = c[1]; c[1] = x;  x = a[0]; a[0] = a[1]; a[1] = x;
+    x = c[2]; c[2] = c[3]; c[3] = x;  x = a[2]; a[2] = a[3]; a[3] = x;
+  }
+  if (colour & 4)     // swapColAcol
+    for (int k = 0; k < 4; ++k) { const int x = c[k]; c[k] = a[k]; a[k] = x; }
+  for (int k = 0; k < 4; ++k) { col[k] = c[k]; acol[k] = a[k]; }
+  return CP_OK;
+}
+
+// LHEF tag of a colour index (0 = none)
+static inline int lhef_tag(int c) { return c ? 500 + c : 0; }
+
+extern "C" int cp_write_lhef(const cp_config* cfg, const cp_event* events, uint64_t n, double sigma_mb,
+                             double sigma_err_mb, const char* path)
+{
+  if (!cfg || (n && !events) || !path) return CP_ERR_INVALID;
+  CpHadParams P{};
+  const CpHadConfig hc{cfg->sqrt_s, cfg->pt_hat_min, cfg->alphas_mz, cfg->k_ren, cfg->k_fac, cfg->convert2mb,
+                       cfg->n_quark_in, cfg->n_quark_new, cfg->proc_mask};
+  if (cp_build_had_params(hc, P)) return CP_ERR_INVALID;
+  FILE* f = fopen(path, "w");
+  if (!f) return CP_ERR_INVALID;
+  const double eBeam = 0.5 * cfg->sqrt_s;
+  const double mb2pb = 1e9;
+  // per-process counts and summed weights: XSECUP_k = sigma * (sum of weights of k) / (sum of weights)
+  double wsum[5] = {0, 0, 0, 0, 0}, wtot = 0.0, wmax = 0.0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const int code = events[i].process;
+    if (code < 111 || code > 115) { fclose(f); return CP_ERR_INVALID; }
+    wsum[code - 111] += events[i].weight;
+    wtot += events[i].weight;
+    wmax = events[i].weight > wmax ? events[i].weight : wmax;
+  }
+  int nproc = 0;
+  for (int k = 0; k < 5; ++k) nproc += wsum[k] > 0 ? 1 : 0;
+  fprintf(f, "<LesHouchesEvents version=\"3.0\">\n<header>\n");
+  fprintf(f, "  cupythia_b200 unweighted pp -> 2 jets, sqrt(s) = %.1f GeV, pT_hat > %.2f GeV, CTEQ5L,\n",
+          cfg->sqrt_s, cfg->pt_hat_min);
+  fprintf(f, "  alpha_s(mZ) = %.4f first order, mu_R^2 = %.3g pT^2, mu_F^2 = %.3g pT^2; %llu events\n",
+          cfg->alphas_mz, cfg->k_ren, cfg->k_fac, (unsigned long long)n);
+  fprintf(f, "</header>\n<init>\n");
+  // IDBMUP1 IDBMUP2 EBMUP1 EBMUP2 PDFGUP1 PDFGUP2 PDFSUP1 PDFSUP2 IDWTUP NPRUP
+  // (PDFSUP 19051 = CTEQ5L in the LHAPDF numbering; IDWTUP 3: unit-weight events)
+  fprintf(f, "2212 2212 %.10E %.10E 0 0 19051 19051 3 %d\n", eBeam, eBeam, nproc);
+  for (int k = 0; k < 5; ++k) {
+    if (wsum[k] <= 0) continue;
+    const double frac = wsum[k] / wtot;
+    const double xs = sigma_mb * mb2pb * frac;
+    const double xe = mb2pb * sqrt(sigma_err_mb * sigma_err_mb * frac * frac +
+                                   sigma_mb * sigma_mb * frac * (1.0 - frac) / (n > 0 ? (double)n : 1.0));
+    fprintf(f, "%.10E %.10E %.10E %d\n", xs, xe, wmax, 111 + k);
+  }
+  fprintf(f, "</init>\n");
+  for (uint64_t i = 0; i < n; ++i) {
+    const cp_event& e = events[i];
+    int col[4], acol[4];
+    if (cp_colour_tags(e.process, e.colour, col, acol) != CP_OK) { fclose(f); return CP_ERR_INVALID; }
+    const double pT2 = (double)e.pt_hat * e.pt_hat;
+    const double scale = sqrt(pT2 * cfg->k_fac);
+    const double aS = cp_alphas(P, (float)(pT2 * cfg->k_ren));
+    fprintf(f, "<event>\n");
+    // NUP IDPRUP XWGTUP SCALUP AQEDUP AQCDUP
+    fprintf(f, "4 %d %.8E %.8E 7.8175100E-03 %.8E\n", (int)e.process, (double)e.weight, scale, aS);
+    // IDUP ISTUP MOTHUP1 MOTHUP2 ICOLUP1 ICOLUP2 PX PY PZ E M VTIMUP SPINUP
+    for (int k = 0; k < 2; ++k)
+      fprintf(f, "%d -1 0 0 %d %d 0.0000000000E+00 0.0000000000E+00 %.10E %.10E 0.0000000000E+00 0. 9.\n",
+              (int)e.id[k], lhef_tag(col[k]), lhef_tag(acol[k]), (double)e.pz_in[k], fabs((double)e.pz_in[k]));
+    const float* p[2] = {e.p3, e.p4};
+    for (int k = 0; k < 2; ++k)
+      fprintf(f, "%d 1 1 2 %d %d %.10E %.10E %.10E %.10E 0.0000000000E+00 0. 9.\n", (int)e.id[2 + k],
+              lhef_tag(col[2 + k]), lhef_tag(acol[2 + k]), (double)p[k][0], (double)p[k][1], (double)p[k][2],
+              (double)p[k][3]);
+    fprintf(f, "</event>\n");
+  }
+  fprintf(f, "</LesHouchesEvents>\n");
+  const int bad = ferror(f);
+  fclose(f);
+  return bad ? CP_ERR_INVALID : CP_OK;
+}

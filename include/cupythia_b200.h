@@ -79,7 +79,10 @@ typedef struct cp_event {
   float p4[4];         /* px, py, pz, E of outgoing 4                               */
   float weight;        /* 1, or w / w_max for overweight events (> 1)               */
   float pt_hat;        /* GeV                                                       */
-  uint32_t process;    /* Pythia process code 111..115                              */
+  uint16_t process;    /* Pythia process code 111..115                              */
+  uint16_t colour;     /* colour flow of the process's setIdColAcol: bits 0-1 topology
+                          (order of its setColAcol calls), bit 2 swapColAcol, bit 3
+                          swapCol1234; cp_colour_tags() expands it to col/acol tags   */
   uint32_t point;      /* low 32 bits of the point index that produced the event    */
 } cp_event;
 
@@ -261,6 +264,20 @@ int cp_flow_enable(cp_handle* h, int on);
 int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host);
 /* The training gradient of one batch (counter iteration iter, stream 2) without an update. */
 int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, float* grad_host, double* loss_host);
+
+/* ---------------------------------------------------------------- record consumers -- */
+/* Host-only (no GPU needed).  Colour tags (1..4, 0 = none) of the four partons of a record from
+ * its process code and encoded colour flow, as the process's setIdColAcol sets them
+ * (pythia8317/src/SigmaQCD.cc:135-342, setColAcol + swapColAcol / swapCol1234). */
+int cp_colour_tags(uint16_t process, uint16_t colour, int col[4], int acol[4]);
+/* Writes n host records as a Les Houches Event File 3.0 (the reference's LHE writers:
+ * cuPythia/pipeline/lhe_writer.cu:46-70, cuPythia/07_unweighting_lhe/unweight_lhe.cu:74-102):
+ * beams and PDF set from cfg, one <init> line per process present with XSECUP = sigma x its
+ * share of the event weights (pb), IDWTUP 3; per event IDPRUP = process code, XWGTUP = the
+ * record weight (1, or w / w_max for overweight events), SCALUP = sqrt(k_fac) pT_hat,
+ * AQCDUP = alpha_s(k_ren pT_hat^2) at first order, colour tags 501.. from cp_colour_tags. */
+int cp_write_lhef(const cp_config* cfg, const cp_event* events_host, uint64_t n, double sigma_mb,
+                  double sigma_err_mb, const char* path);
 
 /* ---------------------------------------------------------------- measurement ------ */
 /* Per-kernel CUDA-event timing of the production pass (cp_unweight / cp_generate_host): slot 0

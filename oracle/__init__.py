@@ -55,6 +55,7 @@ _SIG = {
     "cpo_had_weight_grad": (None, [C.c_void_p, _PD, _PD]),
     "cpo_had_adjoint_sums": (None, [C.c_void_p, _PD, C.c_int, _U64, _U32, _U32, _U64, _U64, _PD, C.c_int]),
     "cpo_accept": (C.c_int, [_D, _D, _U32]),
+    "cpo_pick_record": (C.c_int, [C.c_void_p, _PD, _D, _D, _D, _D, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "cpo_flow_forward": (None, [C.c_void_p, _PD, _PD, _PD]),
     "cpo_flow_set_rounding": (None, [C.c_int]),
     "cpo_flow_backward_batch": (None, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
@@ -127,3 +128,13 @@ def cupythia_ref():
     L.ref_cpuMC.restype = _D
     L.ref_cpuMC.argtypes = [_U64, _U64, _D, _D, _D]
     return L
+
+
+def pick_record(cfg, x, r0, r1, r3, rc, rs):
+    """(code, ids[4], colour) of the oracle's record picks at the point x (cpo_pick_record)."""
+    ids = (C.c_int * 4)()
+    col = C.c_int()
+    xx = np.ascontiguousarray(np.asarray(x, np.float64))
+    code = lib().cpo_pick_record(C.byref(cfg), dptr(xx), r0, r1, r3, rc, rs, ids, C.byref(col))
+    return code, list(ids), col.value
+

@@ -251,6 +251,116 @@ double cpo_had_weight_x(const cpo_had_cfg* c, const double x[3], double tyz[3])
   return weight_x_r(c, c->aSmZ, c->kR, c->pTmin, x, tyz);
 }
 
+/* ---------------------------------------------------------------------------------------
+ * Record picks of one accepted point at x (FP64), the rules of the device record builder:
+ *  process      k in proportion to the sum of its pair terms at the point (r0; the device's own
+ *               rule: Pythia instead picks a process container by its sigmaMax first),
+ *  pair         SigmaProcess::pickInState (pythia8317/src/SigmaProcess.cc:486-508): the first
+ *               pair of the initFlux list (:124-193) at which the running sum of pair terms
+ *               reaches r1 x the process total (the last pair if rounding leaves none),
+ *  new flavour  Sigma2gg2qqbar::sigmaKin (pythia8317/src/SigmaQCD.cc:173): 1 + int(nQuarkNew r3),
+ *  colour       the process's setIdColAcol (SigmaQCD.cc: gg2gg :135-148, gg2qqbar :195-205,
+ *               qg2qg :232-244, qq2qq :292-304, qqbar2gg :331-342): topology with rc in
+ *               proportion to its kinematic term, gg -> gg orientation swapped when rs > 0.5.
+ * Returns the process code (0 if the point has no weight); id[4] and the colour code in the
+ * record's encoding (bits 0-1 topology, bit 2 swapColAcol, bit 3 swapCol1234).
+ * ------------------------------------------------------------------------------------- */
+int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3, double rc,
+                    double rs, int id[4], int* colour)
+{
+  double tyz[3];
+  if (!(weight_x_r(c, c->aSmZ, c->kR, c->pTmin, x, tyz) > 0.0)) return 0;
+  const double s = c->sqrtS * c->sqrtS;
+  const double tau = tyz[0], y = tyz[1], z = tyz[2];
+  const double sH = tau * s, tH = -0.5 * sH * (1.0 - z), uH = -0.5 * sH * (1.0 + z);
+  const double x1 = sqrt(tau) * exp(y), x2 = sqrt(tau) * exp(-y);
+  const double pT2 = tH * uH / sH;
+  const double alpS = alphas_r(c->aSmZ, pT2 * c->kR);
+  double A[8], B[8];
+  cteq5l_r(x1, pT2 * c->kF, A);
+  cteq5l_r(x2, pT2 * c->kF, B);
+  const int nQ = c->nQuarkIn;
+  /* pair lists in initFlux order */
+  int pa[5][128], pb[5][128], np[5] = {0, 0, 0, 0, 0};
+  double ps[5][128], tot[5] = {0, 0, 0, 0, 0};
+  const int bit[5] = {CPO_GG2GG, CPO_GG2QQBAR, CPO_QG2QG, CPO_QQ2QQ, CPO_QQBAR2GG};
+#define CPO_ADD(k, a, b, me)                                                       \
+  do {                                                                             \
+    const double v_ = (me) * xf_of_r(A, a) * xf_of_r(B, b);                        \
+    pa[k][np[k]] = a; pb[k][np[k]] = b; ps[k][np[k]] = v_; ++np[k]; tot[k] += v_;  \
+  } while (0)
+  if (c->procMask & bit[0]) CPO_ADD(0, 21, 21, me_gg2gg_r(sH, tH, uH, alpS));
+  if (c->procMask & bit[1]) CPO_ADD(1, 21, 21, me_gg2qqbar_r(sH, tH, uH, alpS, c->nQuarkNew));
+  if (c->procMask & bit[2]) {
+    const double me = me_qg2qg_r(sH, tH, uH, alpS);
+    for (int q = -nQ; q <= nQ; ++q)
+      if (q) { CPO_ADD(2, q, 21, me); CPO_ADD(2, 21, q, me); }
+  }
+  if (c->procMask & bit[3])
+    for (int q1 = -nQ; q1 <= nQ; ++q1)
+      for (int q2 = -nQ; q2 <= nQ; ++q2)
+        if (q1 && q2) CPO_ADD(3, q1, q2, me_qq2qq_r(sH, tH, uH, alpS, q1, q2));
+  if (c->procMask & bit[4]) {
+    const double me = me_qqbar2gg_r(sH, tH, uH, alpS);
+    for (int q = -nQ; q <= nQ; ++q)
+      if (q) CPO_ADD(4, q, -q, me);
+  }
+#undef CPO_ADD
+  double all = 0.0;
+  for (int k = 0; k < 5; ++k) all += tot[k];
+  double t = r0 * all;
+  int k = 0;
+  while (k < 4 && (t >= tot[k] || tot[k] <= 0.0)) { t -= tot[k]; ++k; }
+  if (tot[k] <= 0.0) { k = 0; while (k < 4 && !(tot[k] > 0.0)) ++k; }
+  double u = r1 * tot[k];
+  int i = 0;
+  for (; i < np[k] - 1; ++i) {
+    u -= ps[k][i];
+    if (u <= 0.0) break;
+  }
+  const int a = pa[k][i], b = pb[k][i];
+  id[0] = a; id[1] = b;
+  if (k == 0 || k == 4) { id[2] = 21; id[3] = 21; }
+  else if (k == 1) {
+    int qn = 1 + (int)(c->nQuarkNew * r3);
+    if (qn > c->nQuarkNew) qn = c->nQuarkNew;
+    id[2] = qn; id[3] = -qn;
+  } else { id[2] = a; id[3] = b; }
+  /* colour flow */
+  const double sH2 = sH * sH, tH2 = tH * tH, uH2 = uH * uH;
+  int topo = 0, swapCA = 0, swap12 = 0;
+  if (k == 0) {
+    const double sTS = (9. / 4.) * (tH2 / sH2 + 2. * tH / sH + 3. + 2. * sH / tH + sH2 / tH2);
+    const double sUS = (9. / 4.) * (uH2 / sH2 + 2. * uH / sH + 3. + 2. * sH / uH + sH2 / uH2);
+    const double sTU = (9. / 4.) * (tH2 / uH2 + 2. * tH / uH + 3. + 2. * uH / tH + uH2 / tH2);
+    const double r = (sTS + sUS + sTU) * rc;
+    topo = r < sTS ? 0 : (r < sTS + sUS ? 1 : 2);
+    swapCA = rs > 0.5;
+  } else if (k == 1) {
+    const double sTS = (1. / 6.) * uH / tH - (3. / 8.) * uH2 / sH2;
+    const double sUS = (1. / 6.) * tH / uH - (3. / 8.) * tH2 / sH2;
+    topo = (sTS + sUS) * rc < sTS ? 0 : 1;
+  } else if (k == 2) {
+    const double sTS = uH2 / tH2 - (4. / 9.) * uH / sH;
+    const double sTU = sH2 / tH2 - (4. / 9.) * sH / uH;
+    topo = (sTS + sTU) * rc < sTS ? 0 : 1;
+    swap12 = id[0] == 21;
+    swapCA = id[0] < 0 || id[1] < 0;
+  } else if (k == 3) {
+    const double sT = (4. / 9.) * (sH2 + uH2) / tH2, sU = (4. / 9.) * (sH2 + tH2) / uH2;
+    topo = id[0] * id[1] > 0 ? 0 : 1;
+    if (id[1] == id[0] && (sT + sU) * rc > sT) topo = 2;
+    swapCA = id[0] < 0;
+  } else {
+    const double sTS = (32. / 27.) * uH / tH - (8. / 3.) * uH2 / sH2;
+    const double sUS = (32. / 27.) * tH / uH - (8. / 3.) * tH2 / sH2;
+    topo = (sTS + sUS) * rc < sTS ? 0 : 1;
+    swapCA = id[0] < 0;
+  }
+  *colour = topo | (swapCA << 2) | (swap12 << 3);
+  return 111 + k;
+}
+
 double cpo_vegas_map(const double* edges, int nb, const uint32_t w[3], double x[3], int bins[3])
 {
   double jac = 1.0;

@@ -9,6 +9,10 @@
 //   gen    <nAccepted> <seed> <threads> [pTmin] [aSmZ]
 //                                       ProcessLevel-only HardQCD generation, one Pythia per thread,
 //                                       prints tried/accepted/s and sigmaGen +- sigmaErr
+//   lhef   <file> [shower]              reads a Les Houches Event File back (Beams:frameType = 4);
+//                                       with shower = 1 also showers (MPI off) and hadronizes every
+//                                       event, which needs a valid colour flow; prints counts and
+//                                       the largest total four-momentum imbalance
 // Settings follow the hadronic dijet configuration: pp at 13 TeV, HardQCD gg2gg, qg2qg,
 // qqbar2gg, gg2qqbar, qq2qq on, PhaseSpace:pTHatMin = 20, PDF:pSet = 2 (CTEQ5L),
 // SigmaProcess:alphaSvalue = 0.13 at first order, parton and hadron levels off.
@@ -144,12 +148,56 @@ static int cmd_gen(long nAcc, int seed, int threads, double pTmin, double aSmZ)
   return 0;
 }
 
+static int cmd_lhef(const char* path, int shower)
+{
+  Pythia p(xmlDir(), false);
+  p.readString("Beams:frameType = 4");
+  p.settings.word("Beams:LHEF", path);
+  p.readString("PDF:pSet = 2");
+  if (shower) {
+    p.readString("PartonLevel:MPI = off");
+  } else {
+    p.readString("PartonLevel:all = off");
+    p.readString("HadronLevel:all = off");
+  }
+  p.readString("Next:numberCount = 0");
+  if (!getenv("CP_PYTHIA_VERBOSE")) p.readString("Print:quiet = on");
+  if (!p.init()) {
+    printf("{\"init\": false}\n");
+    return 2;
+  }
+  const double eTot = p.info.eA() + p.info.eB();
+  long nOk = 0, nAbort = 0, nCode[5] = {0, 0, 0, 0, 0};
+  double maxImb = 0.0;
+  for (;;) {
+    if (!p.next()) {
+      if (p.info.atEndOfFile()) break;
+      if (++nAbort > 1000) break;
+      continue;
+    }
+    ++nOk;
+    const int code = p.info.codeSub();
+    if (code >= 111 && code <= 115) ++nCode[code - 111];
+    double px = 0, py = 0, pz = 0, e = 0;
+    const Event& ev = shower ? p.event : p.process;
+    for (int i = 0; i < ev.size(); ++i)
+      if (ev[i].isFinal()) { px += ev[i].px(); py += ev[i].py(); pz += ev[i].pz(); e += ev[i].e(); }
+    double imb = fabs(px) + fabs(py) + (shower ? fabs(pz) + fabs(e - eTot) : 0.0);
+    if (imb > maxImb) maxImb = imb;
+  }
+  printf("{\"init\": true, \"read\": %ld, \"aborted\": %ld, \"max_imbalance_gev\": %.6g, "
+         "\"by_code\": [%ld, %ld, %ld, %ld, %ld], \"sigma_gen_mb\": %.8g, \"e_cm\": %.8g}\n",
+         nOk, nAbort, maxImb, nCode[0], nCode[1], nCode[2], nCode[3], nCode[4], p.info.sigmaGen(), eTot);
+  return 0;
+}
+
 int main(int argc, char** argv)
 {
   if (argc < 2) { fprintf(stderr, "usage: pythia_ref pdf|alphas|sigma|gen ...\n"); return 1; }
   if (!strcmp(argv[1], "pdf")) return cmd_pdf(argc - 2, argv + 2);
   if (!strcmp(argv[1], "alphas")) return cmd_alphas(argc - 2, argv + 2);
   if (!strcmp(argv[1], "sigma") && argc > 2) return cmd_sigma(argv[2]);
+  if (!strcmp(argv[1], "lhef") && argc > 2) return cmd_lhef(argv[2], argc > 3 ? atoi(argv[3]) : 0);
   if (!strcmp(argv[1], "gen") && argc > 4)
     return cmd_gen(atol(argv[2]), atoi(argv[3]), atoi(argv[4]), argc > 5 ? atof(argv[5]) : 20.0,
                    argc > 6 ? atof(argv[6]) : 0.13);

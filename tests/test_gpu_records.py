@@ -1,0 +1,80 @@
+"""Event records on the GPU against the oracle: the record builder's process, incoming pair,
+new flavour and colour flow (pickInState + setIdColAcol restated in cpo_pick_record) at the
+kernel's own points and random numbers, and the LHE file of device records read back by Pythia.
+The kernel evaluates the pair sums in FP32 and the oracle in FP64, so a pick can differ when a
+random number falls within rounding of a boundary: at most 1 in 1000 records may differ."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+N = 1 << 20
+
+
+@pytest.fixture(scope="module")
+def production():
+    import cupythia_b200 as cp
+    it = cp.Integrator()
+    it.integrate(6, 1 << 21, alpha=1.5)
+    it.iteration(N, 60, alpha=0.0)
+    it.weight_quantile(0.999)
+    rec, st = it.unweight(N, iteration=61)
+    yield it, cp.events_view(rec), st
+    it.close()
+
+
+def _u24(w):
+    return (w >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
+
+
+def test_record_picks_match_oracle(production):
+    it, ev, st = production
+    sub = ev[:20000]
+    pts = sub["point"].astype(np.int64)
+    _, x = it.point_weights(0, N, 61, with_x=True)
+    x = x.cpu().numpy()[pts].astype(np.float64)
+    w1 = it.philox_words(it.cfg.seed, 0, N, 61, 1)[pts]
+    w3 = it.philox_words(it.cfg.seed, 0, N, 61, 3)[pts]
+    cfg = oracle.had_cfg()
+    bad = 0
+    codes = np.zeros(len(sub), int)
+    for i in range(len(sub)):
+        r = [float(_u24(w1[i, 0])), float(_u24(w1[i, 1])), float(_u24(w1[i, 3])), float(_u24(w3[i, 0])),
+             float(_u24(w3[i, 1]))]
+        code, ids, colour = oracle.pick_record(cfg, x[i], *r)
+        codes[i] = code
+        if (code, ids, colour) != (int(sub["process"][i]), sub["id"][i].tolist(), int(sub["colour"][i])):
+            bad += 1
+    assert bad <= len(sub) // 1000, bad
+    assert set(np.unique(codes)) == {111, 112, 113, 114, 115}
+
+
+def test_device_colour_flows_are_valid(production):
+    import cupythia_b200 as cp
+    from test_records import _valid_flow
+    _, ev, _ = production
+    sub = ev[:50000]
+    col, acol = cp.colour_tags(sub)
+    ok = [_valid_flow(e.tolist(), c.tolist(), a.tolist()) for e, c, a in zip(sub["id"], col, acol)]
+    assert all(ok)
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.PYTHIA_REF), reason="oracle/_ref not built")
+def test_lhef_of_device_records_reads_back_in_pythia(production, tmp_path):
+    import cupythia_b200 as cp
+    it, ev, st = production
+    n = 2000
+    path = tmp_path / "gpu.lhe"
+    cp.write_lhef(path, ev[:n], st["sigma"], st["sigma_err"], cfg=it.cfg)
+    r = subprocess.run([oracle.PYTHIA_REF, "lhef", str(path), "1"], capture_output=True, text=True, timeout=600)
+    out = json.loads(r.stdout.strip().split("\n")[-1])
+    assert out["init"] and out["read"] == n and out["aborted"] == 0, out
+    assert out["max_imbalance_gev"] < 0.05, out
+    assert out["by_code"] == [int((ev[:n]["process"] == c).sum()) for c in range(111, 116)]
+    assert abs(out["sigma_gen_mb"] / st["sigma"] - 1) < 1e-6
