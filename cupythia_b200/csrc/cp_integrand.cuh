@@ -475,21 +475,41 @@ CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, f
       a = 21; bb = q;   // rounding fall-through keeps the last pair
     }
   } else if (k == 3) {
-    float tot2 = 0.f;
-    for (int q1 = -5; q1 <= 5; ++q1)
-      for (int q2 = -5; q2 <= 5; ++q2)
-        if (q1 && q2) tot2 += cp_xf_id(A, q1) * cp_xf_id(B, q2) * cp_qq_pair_bracket(pt.b, q1, q2);
+    // pickInState over the 100 (q1, q2) pairs in initFlux order, walked row by row: the row
+    // total A(q1) sum_q2 B(q2) br(q1, q2) from the three bracket classes first, then the pair
+    // inside the chosen row
+    const float brS = 0.5f * (pt.b.qqU + pt.b.qqTU + pt.b.qqT), brO = pt.b.qqT + pt.b.qqST, brT = pt.b.qqT;
+    const float SB = B[0] + B[1] + B[3] + B[4] + 2.f * (B[5] + B[6] + B[7]);
+    float row[10], tot2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      const int q = i < 5 ? i - 5 : i - 4;
+      row[i] = cp_xf_id(A, q) * (brT * SB + (brS - brT) * cp_xf_id(B, q) + (brO - brT) * cp_xf_id(B, -q));
+      tot2 += row[i];
+    }
     float u = r1 * tot2;
-    a = 5; bb = 5;
-    bool done = false;
-    for (int q1 = -5; q1 <= 5 && !done; ++q1)
-      for (int q2 = -5; q2 <= 5; ++q2) {
-        if (!q1 || !q2) continue;
-        float s = cp_xf_id(A, q1) * cp_xf_id(B, q2) * cp_qq_pair_bracket(pt.b, q1, q2);
-        a = q1; bb = q2;
-        if (u < s) { done = true; break; }
-        u -= s;
+    int ir = 9;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      if (ir == 9 && i < 9) {
+        if (u < row[i]) ir = i;
+        else u -= row[i];
       }
+    }
+    const int q1 = ir < 5 ? ir - 5 : ir - 4;
+    const float a1 = cp_xf_id(A, q1);
+    a = q1; bb = 5;
+    bool done = false;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+      const int q2 = i < 5 ? i - 5 : i - 4;
+      if (!done) {
+        const float s = a1 * cp_xf_id(B, q2) * (q2 == q1 ? brS : (q2 == -q1 ? brO : brT));
+        bb = q2;
+        if (u < s) done = true;
+        else u -= s;
+      }
+    }
   } else if (k == 4) {
     float tot2 = 0.f;
     for (int q = -5; q <= 5; ++q)
@@ -521,9 +541,14 @@ CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, f
 // up = uHat/sHat; common factors of the terms are dropped.
 CP_HD uint32_t cp_colour_flow(int code, const int id[4], float tp, float up, float rc, float rs)
 {
+#if defined(__CUDA_ARCH__)
+  const float rt = __frcp_rn(tp), ru = __frcp_rn(up);
+#else
+  const float rt = 1.f / tp, ru = 1.f / up;
+#endif
   uint32_t topo = 0, swapCA = 0, swap12 = 0;
   if (code == 111) {
-    const float rt = 1.f / tp, ru = 1.f / up, tu = tp * ru, ut = up * rt;
+    const float tu = tp * ru, ut = up * rt;
     const float a = (tp + 1.f) * (tp + 1.f) + (rt + 1.f) * (rt + 1.f) + 1.f;
     const float b = (up + 1.f) * (up + 1.f) + (ru + 1.f) * (ru + 1.f) + 1.f;
     const float c = (tu + 1.f) * (tu + 1.f) + (ut + 1.f) * (ut + 1.f) + 1.f;
@@ -531,30 +556,38 @@ CP_HD uint32_t cp_colour_flow(int code, const int id[4], float tp, float up, flo
     topo = r < a ? 0u : (r < a + b ? 1u : 2u);
     swapCA = rs > 0.5f ? 1u : 0u;
   } else if (code == 112) {
-    const float a = (1.f / 6.f) * (up / tp) - 0.375f * up * up;
-    const float b = (1.f / 6.f) * (tp / up) - 0.375f * tp * tp;
+    const float a = (1.f / 6.f) * up * rt - 0.375f * up * up;
+    const float b = (1.f / 6.f) * tp * ru - 0.375f * tp * tp;
     topo = (a + b) * rc < a ? 0u : 1u;
   } else if (code == 113) {
-    const float a = (up / tp) * (up / tp) - (4.f / 9.f) * up;
-    const float b = 1.f / (tp * tp) - (4.f / 9.f) / up;
+    const float a = (up * rt) * (up * rt) - (4.f / 9.f) * up;
+    const float b = rt * rt - (4.f / 9.f) * ru;
     topo = (a + b) * rc < a ? 0u : 1u;
     swap12 = id[0] == 21 ? 1u : 0u;
     swapCA = (id[0] < 0 || id[1] < 0) ? 1u : 0u;
   } else if (code == 114) {
     topo = id[0] * id[1] > 0 ? 0u : 1u;
     if (id[1] == id[0]) {
-      const float T = (1.f + up * up) / (tp * tp), U = (1.f + tp * tp) / (up * up);
+      const float T = (1.f + up * up) * rt * rt, U = (1.f + tp * tp) * ru * ru;
       if ((T + U) * rc > T) topo = 2u;
     }
     swapCA = id[0] < 0 ? 1u : 0u;
   } else {
-    const float a = (32.f / 27.f) * (up / tp) - (8.f / 3.f) * up * up;
-    const float b = (32.f / 27.f) * (tp / up) - (8.f / 3.f) * tp * tp;
+    const float a = (32.f / 27.f) * up * rt - (8.f / 3.f) * up * up;
+    const float b = (32.f / 27.f) * tp * ru - (8.f / 3.f) * tp * tp;
     topo = (a + b) * rc < a ? 0u : 1u;
     swapCA = id[0] < 0 ? 1u : 0u;
   }
   return topo | (swapCA << 2) | (swap12 << 3);
 }
+
+// Colour draws from the low bytes of the record block (the picks use the high 24 bits of each
+// word): rc, 24 bits from bytes 0 of words 0..2; rs, 8 bits from byte 0 of word 3.
+CP_HD float cp_colour_rc(const uint32_t w[4])
+{
+  return (float)((w[0] & 0xFFu) | ((w[1] & 0xFFu) << 8) | ((w[2] & 0xFFu) << 16)) * (1.f / 16777216.f);
+}
+CP_HD float cp_colour_rs(const uint32_t w[4]) { return (float)(w[3] & 0xFFu) * (1.f / 256.f); }
 
 // Lab-frame four-momenta: parton 3 at cos(theta*) = z from beam A, azimuth phi; boost by the
 // rapidity y = (ln x1 - ln x2)/2 of the parton system (massless, PhaseSpace.cc 2 -> 2 kinematics).

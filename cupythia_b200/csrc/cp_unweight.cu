@@ -13,7 +13,7 @@
 //
 // Random numbers: the accept draw is word 3 of the point's Philox block (stream 0); accepted
 // points draw a second block from stream 1 for the process / pair / azimuth / new-flavour picks
-// and a third from stream 3 (word 0: colour topology, word 1: gg -> gg colour orientation).
+// (high 24 bits of words 0..3) and the colour topology / orientation (their low bytes).
 #include <vector>
 #include "cp_internal.cuh"
 
@@ -164,16 +164,15 @@ __global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, c
        k += (uint64_t)gridDim.x * CP_THREADS) {
     const uint4 tail = reinterpret_cast<const uint4*>(L.out + k)[3];
     const uint64_t point = L.point0 + tail.w;
-    uint32_t wd[4], w2[4], w3[4];
+    uint32_t wd[4], w2[4];
     cp_point_words(L.seed, point, L.iter, 0, wd);
     cp_point_words(L.seed, point, L.iter, 1, w2);
-    cp_point_words(L.seed, point, L.iter, 3, w3);
     CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, tail.w);
     CpPoint pt;
     cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt);
     CpEventRec ev;
-    cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_u24(w3[0]),
-                  cp_u24(w3[1]), __uint_as_float(tail.x), (uint32_t)point, ev);
+    cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
+                  cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
     const uint4* src = reinterpret_cast<const uint4*>(&ev);
     uint4* dst = reinterpret_cast<uint4*>(L.out + k);
 #pragma unroll

@@ -40,13 +40,14 @@ def test_record_picks_match_oracle(production):
     _, x = it.point_weights(0, N, 61, with_x=True)
     x = x.cpu().numpy()[pts].astype(np.float64)
     w1 = it.philox_words(it.cfg.seed, 0, N, 61, 1)[pts]
-    w3 = it.philox_words(it.cfg.seed, 0, N, 61, 3)[pts]
     cfg = oracle.had_cfg()
     bad = 0
     codes = np.zeros(len(sub), int)
     for i in range(len(sub)):
-        r = [float(_u24(w1[i, 0])), float(_u24(w1[i, 1])), float(_u24(w1[i, 3])), float(_u24(w3[i, 0])),
-             float(_u24(w3[i, 1]))]
+        w = [int(v) for v in w1[i]]
+        rc = ((w[0] & 0xFF) | ((w[1] & 0xFF) << 8) | ((w[2] & 0xFF) << 16)) / 16777216.0
+        rs = (w[3] & 0xFF) / 256.0
+        r = [float(_u24(w1[i, 0])), float(_u24(w1[i, 1])), float(_u24(w1[i, 3])), rc, rs]
         code, ids, colour = oracle.pick_record(cfg, x[i], *r)
         codes[i] = code
         if (code, ids, colour) != (int(sub["process"][i]), sub["id"][i].tolist(), int(sub["colour"][i])):
