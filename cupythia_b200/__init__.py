@@ -78,6 +78,10 @@ class Integrator:
     def _check(self, rc):
         return _lib.check(self.lib, self.h, rc)
 
+    def set_point_offset(self, offset):
+        """Shard offset added to every pass's point indices (cp_set_point_offset)."""
+        self._check(self.lib.cp_set_point_offset(self.h, int(offset)))
+
     def set_stream(self, stream):
         self._check(self.lib.cp_set_stream(self.h, C.c_void_p(stream)))
 

@@ -87,6 +87,7 @@ SIGNATURES = {
     "cp_create": [C.POINTER(cp_config), C.POINTER(_P)],
     "cp_destroy": [_P],
     "cp_set_stream": [_P, _P],
+    "cp_set_point_offset": [_P, _u64],
     "cp_synchronize": [_P],
     "cp_device_sm_count": [_P, C.POINTER(_i)],
     "cp_philox_words": [_P, _u64, _u64, _u64, _u32, _u32, _P],

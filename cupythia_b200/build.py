@@ -20,6 +20,11 @@ def sources():
     return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
 
 
+BIN = os.path.join(HERE, "bin")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+DRIVERS = ["fused_gg2gg", "vegas", "pdf_xsec", "cub_compaction", "unweight_lhe", "generate"]
+
+
 def deps():
     return sources() + glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + glob.glob(
         os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
@@ -48,5 +53,31 @@ def build(force=False, verbose=False, ptxas_v=False):
     return LIB
 
 
+def build_drivers(force=False, verbose=False):
+    """Stage drivers (drivers/*.cc, C++ over the C ABI) -> bin/<name>, linked to the library."""
+    build(force=False)
+    os.makedirs(BIN, exist_ok=True)
+    hdr = [os.path.join(HERE, "drivers", "drv.h"), os.path.join(ROOT, "include", "cupythia_b200.h")]
+    out = []
+    for name in DRIVERS:
+        src = os.path.join(HERE, "drivers", name + ".cc")
+        exe = os.path.join(BIN, name)
+        out.append(exe)
+        if not force and os.path.exists(exe) and all(
+                os.path.getmtime(f) <= os.path.getmtime(exe) for f in [src, LIB] + hdr):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-Wall", src, "-I" + os.path.join(CUDA_HOME, "include"),
+               "-L" + HERE, "-lcupythia_b200", "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+               "-Wl,-rpath,$ORIGIN/..", "-o", exe]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"g++ failed building the stage driver {name}")
+    return out
+
+
 if __name__ == "__main__":
     build(force=True, verbose=True, ptxas_v="-v" in sys.argv)
+    build_drivers(force=True, verbose=True)

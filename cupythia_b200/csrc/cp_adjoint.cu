@@ -215,7 +215,7 @@ static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream,
   double* red = h->d_slots + (size_t)blocks * width;
   double* out = red + width;
   AdjLaunch L;
-  L.seed = h->cfg.seed; L.point0 = 0; L.n = n; L.iter = iter; L.stream = stream; L.nb = nb;
+  L.seed = h->cfg.seed; L.point0 = h->point_offset; L.n = n; L.iter = iter; L.stream = stream; L.nb = nb;
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.slots = h->d_slots;
   const double pt = h->cfg.pt_hat_min, s = h->cfg.sqrt_s * h->cfg.sqrt_s, a = h->cfg.alphas_mz;
   L.lnTauMin = (float)log(4.0 * pt * pt / s);

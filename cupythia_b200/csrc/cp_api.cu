@@ -154,6 +154,16 @@ extern "C" int cp_destroy(cp_handle* h)
 
 extern "C" const char* cp_last_error(const cp_handle* h) { return h ? h->err.c_str() : "null handle"; }
 
+// Offset of this handle's point indices (cuPythia/common/rng.cuh:5-19: shard i of M points per
+// shard works on the global points [i M, i M + count)); every pass then draws the Philox block of
+// global point offset + p, so shards are disjoint and their union is the single-device run.
+extern "C" int cp_set_point_offset(cp_handle* h, uint64_t offset)
+{
+  CP_CHECK_HANDLE(h);
+  h->point_offset = offset;
+  return CP_OK;
+}
+
 extern "C" int cp_set_stream(cp_handle* h, void* s)
 {
   CP_CHECK_HANDLE(h);

@@ -69,6 +69,8 @@ struct cp_handle {
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
   unsigned long long* d_counter = nullptr; // accepted-event counter
   uint64_t last_n = 0;
+  // added to every point index of the integration, production and adjoint passes (sharding)
+  uint64_t point_offset = 0;
   // learned proposal: FP32 master/grad/Adam moments (4 x n_param), packed BF16 fragments,
   // staged biases, per-point (v, ln J) buffer; flow_on routes the passes through the flow
   float* d_flow = nullptr;

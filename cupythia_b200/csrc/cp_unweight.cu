@@ -201,6 +201,7 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   int rc = cp_ensure_slots(h, (size_t)blocks * CP_UNW_SLOT);
   if (rc) return rc;
   if (n > (1ull << 32)) return cp_fail(h, CP_ERR_INVALID, "at most 2^32 points per production call");
+  point0 += h->point_offset;
   UnwLaunch L;
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.nb = h->nb;
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;

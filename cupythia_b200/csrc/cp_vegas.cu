@@ -230,6 +230,7 @@ static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, 
   const int width = CP_SLOT_HEAD + 3 * h->nb;
   int rc = cp_ensure_slots(h, (size_t)h->had_blocks * width);
   if (rc) return rc;
+  point0 += h->point_offset;
   HadLaunch L;
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.stream = stream;
   L.nb = h->nb; L.edges = h->d_edges; L.slots = h->d_slots; L.w_out = w_out; L.x_out = x_out;

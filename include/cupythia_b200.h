@@ -106,6 +106,11 @@ typedef struct cp_grad {
 /* ---------------------------------------------------------------- handles ---------- */
 int cp_abi_version(void);
 int cp_config_default(cp_config* cfg);
+/* Adds `offset` to the point index of every integration, production and adjoint pass of this
+ * handle (the counter of point p becomes offset + p): the reference's shard offset
+ * (cupythia_shard_offset, cuPythia/common/rng.cuh:5-19; the stage drivers read CUPYTHIA_SHARD
+ * and CUPYTHIA_SHARD_N into it).  Records carry the low 32 bits of the global index. */
+int cp_set_point_offset(cp_handle* h, uint64_t offset);
 /* replaces the per-stage cudaMalloc/setup of the cuPythia mains (e.g. 11_vegas_importance/vegas.cu:94-105) */
 int cp_create(const cp_config* cfg, cp_handle** out);
 int cp_destroy(cp_handle* h);
