@@ -191,11 +191,35 @@ class _Null:
         return False
 
 
+def oracle_sigma():
+    with open(os.path.join(ROOT, "tests", "golden", "sigma_oracle.json")) as f:
+        g = json.load(f)
+    return g["sigma_mb"], g["sigma_err_mb"]
+
+
+def quality(stats, n, sec_per_step, adapt_s):
+    """The 1%-error gate and the pull against the FP64 oracle (tests/golden/sigma_oracle.json):
+    inverse-variance combination of the timed steps, the points (and time) one step's throughput
+    needs for delta sigma / sigma = 1%, with and without the adaptation in front."""
+    import math
+    w = [1.0 / s_["sigma_err"] ** 2 for s_ in stats]
+    sig = sum(wi * s_["sigma"] for wi, s_ in zip(w, stats)) / sum(w)
+    err = 1.0 / math.sqrt(sum(w))
+    so, eo = oracle_sigma()
+    rel_point = max(s_["sigma_err"] / s_["sigma"] for s_ in stats) * math.sqrt(n)   # per-point relative std
+    n_1pct = math.ceil((rel_point / 0.01) ** 2)
+    t_1pct = sec_per_step * n_1pct / n
+    return {"sigma_mb": sig, "sigma_err_mb": err, "oracle_sigma_mb": so, "oracle_sigma_err_mb": eo,
+            "pull_vs_oracle": (sig - so) / math.sqrt(err ** 2 + eo ** 2),
+            "points_to_1pct": n_1pct, "time_to_1pct_s": {"steady": t_1pct, "with_adaptation": adapt_s + t_1pct}}
+
+
 def run_ours(a):
     import numpy as np
     import torch
 
     import cupythia_b200 as cp
+    from cupythia_b200.distributed import ShardedIntegrator
     rank, world, pg = dist_init(a.gpus)
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
@@ -203,29 +227,33 @@ def run_ours(a):
     stream = torch.cuda.Stream(device=dev)
     it.set_stream(stream.cuda_stream)
     n = a.points
-    r0 = 1000 + rank * 100000            # disjoint counter iterations per rank
+    r0 = 1000
+    si = ShardedIntegrator(it)           # adaptation: shared points, one exchange per iteration
     records = torch.empty((n, RECORD_BYTES), dtype=torch.uint8, device=f"cuda:{dev}")
 
     with torch.cuda.stream(stream):
         # ---- plain VEGAS form: classic refinement (config 2), w_max = q99.9, production
         t0 = time.perf_counter()
-        per, comb = it.integrate(ADAPT_ITERS, ADAPT_POINTS, alpha=1.5, skip=3)
-        wmax_plain = it.weight_quantile(0.999)
+        per, comb = si.integrate(ADAPT_ITERS, ADAPT_POINTS, alpha=1.5, skip=3)
+        wmax_plain = si.weight_quantile(0.999)
         torch.cuda.synchronize()
         adapt_plain = time.perf_counter() - t0
+        it.set_point_offset(rank * n)    # production: this rank's own points, no exchange
         st_p, ms_p, kt_p = production(it, n, records, r0, a.warmup, a.steps, pg, dev, stream)
 
         # ---- flow + adjoint form: variance-gradient grid refinement (adjoint), flow trained on
         # the integrator's weights (200 x 65536 points), w_max = q99.9 through the flow
         t0 = time.perf_counter()
+        it.set_point_offset(0)           # gradient steps and training: replicated on every rank
         ghist = it.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
         it.flow_init(7)
         losses = it.flow_train(200, 65536, lr=8e-3)
         it.flow_enable(True)
-        it.iteration(ADAPT_POINTS, 300, alpha=0.0)
-        wmax_flow = it.weight_quantile(0.999)
+        si.iteration(ADAPT_POINTS, 300, alpha=0.0)
+        wmax_flow = si.weight_quantile(0.999)
         torch.cuda.synchronize()
         adapt_flow = time.perf_counter() - t0
+        it.set_point_offset(rank * n)
         clk = Clocks(dev)
         st_f, ms_f, kt_f = production(it, n, records, r0 + 50000, a.warmup, a.steps, pg, dev, stream, clk)
 
@@ -236,6 +264,7 @@ def run_ours(a):
     value = allsum(pg, ev_f, dev) / sec_f
     value_plain = allsum(pg, ev_p, dev) / sec_p
     rel_err = max(s_["sigma_err"] / s_["sigma"] for s_ in st_f)
+    q_f, q_p = quality(st_f, n, sec_f / a.steps, adapt_plain + adapt_flow), quality(st_p, n, sec_p / a.steps, adapt_plain)
 
     # ---- e2e through the host-buffer C-ABI call (grid H2D + records D2H inside the region)
     eta_max = max(s_["eta"] for s_ in st_f)
@@ -290,7 +319,8 @@ def run_ours(a):
                    "refinement, BF16 coupling flow trained 200 x 65536 points, unweighting at q99.9",
                    "points_per_step_per_gpu": n, "adapt_points": ADAPT_ITERS * ADAPT_POINTS,
                    "l2": "256 MB buffer written between timed steps; records written per step exceed L2",
-                   "parallelism": f"dp{world} (disjoint counter ranges)"},
+                   "parallelism": f"dp{world}: contiguous point shards per rank; adaptation sums "
+                                  "all-reduced once per iteration, production without exchange"},
         "sigma_mb": comb["sigma"], "sigma_err_mb": comb["sigma_err"], "step_sigma_rel_err_max": rel_err,
         "eta": float(np.mean([s_["eta"] for s_ in st_f])), "w_max": wmax_flow,
         "weighted_points_per_s": n * a.steps * world / sec_f,
@@ -298,8 +328,9 @@ def run_ours(a):
                         "eta": float(np.mean([s_["eta"] for s_ in st_p])), "w_max": wmax_plain,
                         "weighted_points_per_s": n * a.steps * world / sec_p,
                         "step_sigma_rel_err_max": max(s_["sigma_err"] / s_["sigma"] for s_ in st_p),
-                        "adapt_seconds": adapt_plain},
+                        "adapt_seconds": adapt_plain, "quality": q_p},
         "flow_vs_plain": value / value_plain,
+        "quality": q_f,
         "adapt_seconds": adapt_plain + adapt_flow,
         "flow_training": {"steps": 200, "batch": 65536, "loss_first": float(losses[0]),
                           "loss_last20": float(np.mean(losses[-20:])), "adjoint_rel_var": ghist[-1]["rel_var"]},

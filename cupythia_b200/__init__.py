@@ -162,6 +162,32 @@ class Integrator:
         self._check(self.lib.cp_integrate(self.h, n_iter, n_points, alpha, skip, per, C.byref(comb)))
         return [p.as_dict() for p in per], comb.as_dict()
 
+    # ------------------------------------------------------------------ multi-GPU pieces
+    def accumulate(self, n_points, iteration=0):
+        """One pass over this handle's points; returns its sums as a device float64 tensor of
+        CP_SLOT_HEAD + 3 n_bins entries (sum w, sum w^2, max w, n_bad, per-bin sums of w^2)."""
+        torch = _torch()
+        out = torch.empty(_lib.CP_SLOT_HEAD + 3 * self.nb, dtype=torch.float64, device=self.device)
+        self._check(self.lib.cp_vegas_accumulate(self.h, n_points, iteration, _ptr(out)))
+        return out
+
+    def refine(self, sums, n_total, alpha=1.5):
+        """Iteration result and grid refinement from (rank-reduced) sums."""
+        r = cp_result()
+        self._check(self.lib.cp_vegas_refine_sums(self.h, _ptr(sums), float(n_total), alpha, C.byref(r)))
+        return r.as_dict()
+
+    def weight_histogram(self):
+        torch = _torch()
+        out = torch.empty(_lib.CP_QBINS, dtype=torch.int64, device=self.device)
+        self._check(self.lib.cp_weight_histogram(self.h, _ptr(out)))
+        return out
+
+    def quantile_from_histogram(self, hist, q=0.999):
+        v = C.c_double()
+        self._check(self.lib.cp_weight_quantile_hist(self.h, _ptr(hist), q, C.byref(v)))
+        return v.value
+
     def point_weights(self, point0, n, iteration=0, with_x=False):
         torch = _torch()
         w = torch.empty(n, dtype=torch.float32, device=self.device)

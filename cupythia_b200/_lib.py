@@ -88,6 +88,10 @@ SIGNATURES = {
     "cp_destroy": [_P],
     "cp_set_stream": [_P, _P],
     "cp_set_point_offset": [_P, _u64],
+    "cp_vegas_accumulate": [_P, _u64, _u32, _P],
+    "cp_vegas_refine_sums": [_P, _P, _d, _d, C.POINTER(cp_result)],
+    "cp_weight_histogram": [_P, _P],
+    "cp_weight_quantile_hist": [_P, _P, _d, C.POINTER(_d)],
     "cp_synchronize": [_P],
     "cp_device_sm_count": [_P, C.POINTER(_i)],
     "cp_philox_words": [_P, _u64, _u64, _u64, _u32, _u32, _P],
@@ -134,6 +138,9 @@ SIGNATURES = {
 }
 OPTIONAL = {}
 EXTRA_RESTYPES = {"cp_last_error": C.c_char_p}
+
+CP_SLOT_HEAD = 4
+CP_QBINS = 4096
 
 _lib = None
 

@@ -391,6 +391,66 @@ extern "C" int cp_weight_quantile(cp_handle* h, double q, double* w_q)
 }
 
 // ------------------------------------------------------------------------------------------
+// Distributed iteration: a pass over this handle's points into a caller buffer, and the
+// refinement from sums the caller has reduced over ranks (sum over every entry except the
+// maximum weight at index 2, which is reduced by max).
+// ------------------------------------------------------------------------------------------
+extern "C" int cp_vegas_accumulate(cp_handle* h, uint64_t n_points, uint32_t iter, double* sums_dev)
+{
+  CP_CHECK_HANDLE(h);
+  if (n_points < 1 || !sums_dev) return cp_fail(h, CP_ERR_INVALID, "cp_vegas_accumulate: bad arguments");
+  int rc = had_launch(h, 0, n_points, iter, 0, nullptr, nullptr);
+  if (rc) return rc;
+  CP_CUDA(h, cudaMemcpyAsync(sums_dev, h->d_red, sizeof(double) * (CP_SLOT_HEAD + 3 * h->nb), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
+  return CP_OK;
+}
+
+extern "C" int cp_vegas_refine_sums(cp_handle* h, const double* sums_dev, double n_total, double alpha, cp_result* out)
+{
+  CP_CHECK_HANDLE(h);
+  if (!sums_dev || !(n_total >= 2)) return cp_fail(h, CP_ERR_INVALID, "cp_vegas_refine_sums: bad arguments");
+  int rc = cp_ensure_iters(h, 1);
+  if (rc) return rc;
+  CP_CUDA(h, cudaMemcpyAsync(h->d_red, sums_dev, sizeof(double) * (CP_SLOT_HEAD + 3 * h->nb), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  k_refine<<<1, 32, 0, h->stream>>>(h->d_edges, h->d_red, h->nb, n_total, alpha, h->d_iters);
+  CP_LAUNCH_CHECK(h, "k_refine");
+  CpIterDev r;
+  CP_CUDA(h, cudaMemcpyAsync(&r, h->d_iters, sizeof r, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (out) fill_result(r, out);
+  if (r.nbad > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}
+
+extern "C" int cp_weight_histogram(cp_handle* h, unsigned long long* hist_dev)
+{
+  CP_CHECK_HANDLE(h);
+  if (!hist_dev) return cp_fail(h, CP_ERR_INVALID, "cp_weight_histogram: null buffer");
+  if (h->last_n == 0) return cp_fail(h, CP_ERR_INVALID, "cp_weight_histogram: run a pass first");
+  CP_CUDA(h, cudaMemcpyAsync(hist_dev, h->d_qhist, sizeof(unsigned long long) * CP_QBINS, cudaMemcpyDeviceToDevice,
+                             h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}
+
+extern "C" int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* hist_dev, double q, double* w_q)
+{
+  CP_CHECK_HANDLE(h);
+  if (!hist_dev || !(q > 0.0 && q < 1.0)) return cp_fail(h, CP_ERR_INVALID, "cp_weight_quantile_hist: bad arguments");
+  k_quantile<<<1, 256, 0, h->stream>>>(hist_dev, q, h->d_wmax);
+  CP_LAUNCH_CHECK(h, "k_quantile");
+  double v[2];
+  CP_CUDA(h, cudaMemcpyAsync(v, h->d_wmax, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (w_q) *w_q = v[0];
+  return CP_OK;
+}
+
+// ------------------------------------------------------------------------------------------
 // Allocation-free VEGAS pass.
 //
 // For callers that must not allocate device memory: code running inside a CUDA graph that is

@@ -169,6 +169,21 @@ int cp_vegas_iteration(cp_handle* h, uint64_t n_points, uint32_t iter, double al
  * index >= skip. */
 int cp_integrate(cp_handle* h, int n_iter, uint64_t n_points, double alpha, int skip,
                  cp_result* per_iter_host, cp_result* combined_host);
+/* Multi-GPU iteration (one process per GPU, contiguous point shards via cp_set_point_offset;
+ * the exchange of the survey's multi-GPU plan): cp_vegas_accumulate runs this handle's pass over
+ * n_points points and writes its CP_SLOT_HEAD + 3 n_bins sums (dev) -- sum w, sum w^2, max w,
+ * n_bad, then the per-bin sums of w^2 of each dimension; the caller reduces them over ranks
+ * (sum, max for entry 2) and every rank refines identically with cp_vegas_refine_sums
+ * (n_total = the points of all ranks).  The reference shards events the same way
+ * (cuPythia/common/rng.cuh:5-19) but never exchanges a grid. */
+#define CP_SLOT_HEAD 4
+int cp_vegas_accumulate(cp_handle* h, uint64_t n_points, uint32_t iter, double* sums_dev);
+int cp_vegas_refine_sums(cp_handle* h, const double* sums_dev, double n_total, double alpha, cp_result* out_host);
+/* Weight histogram of the last pass (CP_QBINS u64 counts, dev) and the quantile of a histogram
+ * reduced (summed) over ranks: every rank then unweights against the same w_max. */
+#define CP_QBINS 4096
+int cp_weight_histogram(cp_handle* h, unsigned long long* hist_dev);
+int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* hist_dev, double q, double* w_q_host);
 /* Per-point weights (dev) of points [point0, point0+n) of iteration iter on the current grid,
  * and optionally the mapped x (dev, 3n floats) the integrand was evaluated at. */
 int cp_point_weights(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, float* w_dev,
