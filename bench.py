@@ -248,8 +248,18 @@ def run_ours(a):
         ghist = it.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
         it.flow_init(7)
         losses = it.flow_train(200, 65536, lr=8e-3)
+        # proposal choice (config 5): the flow only where its weight variance beats VEGAS alone
+        # on the same grid at equal points, else VEGAS is the fallback
+        it.flow_enable(False)
+        r_vegas = si.iteration(ADAPT_POINTS, 300, alpha=0.0)
         it.flow_enable(True)
-        si.iteration(ADAPT_POINTS, 300, alpha=0.0)
+        r_flowp = si.iteration(ADAPT_POINTS, 300, alpha=0.0)
+        relvar = {k: (r["sigma_err"] / r["sigma"]) ** 2 * ADAPT_POINTS for k, r in
+                  (("vegas", r_vegas), ("flow", r_flowp))}
+        use_flow = relvar["flow"] < relvar["vegas"]
+        if not use_flow:
+            it.flow_enable(False)
+            si.iteration(ADAPT_POINTS, 300, alpha=0.0)
         wmax_flow = si.weight_quantile(0.999)
         torch.cuda.synchronize()
         adapt_flow = time.perf_counter() - t0
@@ -332,6 +342,8 @@ def run_ours(a):
         "flow_vs_plain": value / value_plain,
         "quality": q_f,
         "adapt_seconds": adapt_plain + adapt_flow,
+        "proposal": {"used": "flow" if use_flow else "vegas (fallback)",
+                     "relative_variance_per_point": relvar},
         "flow_training": {"steps": 200, "batch": 65536, "loss_first": float(losses[0]),
                           "loss_last20": float(np.mean(losses[-20:])), "adjoint_rel_var": ghist[-1]["rel_var"]},
         "kernel_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in kt_f.items()},

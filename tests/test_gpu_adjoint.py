@@ -99,6 +99,32 @@ def test_parameter_gradients_match_central_differences(adapted):
         assert abs(g["dvar"][k] / fd_v - 1) < 2e-3, (name, g["dvar"][k], fd_v)
 
 
+@pytest.mark.parametrize("alphas_mz,k_ren,pt_hat_min", [(0.11, 0.5, 10.0), (0.14, 2.0, 50.0)])
+def test_parameter_gradients_across_the_ranges(alphas_mz, k_ren, pt_hat_min):
+    """The ends of the parameter ranges (alpha_s(mZ) in [0.11, 0.14], scale factor in [0.5, 2],
+    pT_hat cut in [10, 50] GeV): adjoint against central differences with 2^26 points."""
+    import cupythia_b200 as cp
+    base = {"alphas_mz": alphas_mz, "k_ren": k_ren, "pt_hat_min": pt_hat_min}
+    n = 1 << 26
+    with cp.Integrator(**base) as it:
+        it.integrate(5, 1 << 22, alpha=1.5)
+        g = it.adjoint(n, iteration=24)
+        grid = it.grid
+    assert g["n_bad"] == 0
+    for k, name in enumerate(PARAMS):
+        h = 1e-3 * base[name]
+        est = []
+        for sgn in (+1, -1):
+            with cp.Integrator(**dict(base, **{name: base[name] + sgn * h})) as jt:
+                jt.grid = grid
+                r = jt.iteration(n, 24, alpha=0.0)
+                est.append((r["sigma"], r["sum_w2"] / n - r["sigma"] ** 2))
+        fd_s = (est[0][0] - est[1][0]) / (2 * h)
+        fd_v = (est[0][1] - est[1][1]) / (2 * h)
+        assert abs(g["dsigma"][k] / fd_s - 1) < 2e-3, (name, g["dsigma"][k], fd_s)
+        assert abs(g["dvar"][k] / fd_v - 1) < 2e-3, (name, g["dvar"][k], fd_v)
+
+
 def test_edge_gradients_match_central_differences(adapted):
     """The edge gradient is the small residual of two large terms (Jacobian change and point shift),
     so the finite difference needs an exactly realised step: the grid is put on FP32-representable
