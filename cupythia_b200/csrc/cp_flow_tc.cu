@@ -4,10 +4,12 @@
 // with every dense layer as tcgen05.mma over 128-point tiles: A (activations) and B (weights) in
 // shared memory, the FP32 accumulator in TMEM, one elected thread per warpgroup issuing.
 //
-// Launch: one persistent CTA per SM (the shared-memory footprint admits one), 4 warpgroups of
-// 128 threads.  Each warpgroup owns two 128-point tiles in flight ("slots") with 64 TMEM
-// columns and a 16 KB activation buffer each; thread r of the warpgroup is row r (one point) of
-// both tiles and TMEM lane r.  Per coupling and slot there are three steps
+// Launch: one persistent CTA per SM (the shared-memory footprint admits one): 4 epilogue
+// warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two 128-point tiles in
+// flight ("slots") with 64 TMEM columns and a 16 KB activation buffer each; thread r of the
+// warpgroup is row r (one point) of both tiles and TMEM lane r.  An issuing warp does nothing
+// but poll its warpgroup's two publish barriers and issue each slot's next layer, so no
+// epilogue warp ever waits on MMA issue.  Per coupling and slot the epilogue has three steps
 //   ep1: wait for layer 1, TMEM -> bias-free ReLU -> BF16 -> activation buffer, issue layer 2
 //   ep2: the same for layer 2, issue layer 3
 //   ep3: wait for layer 3, read the 4 output columns, update the point, write the next
@@ -18,8 +20,12 @@
 // and 3 add one K = 16 MMA of a constant block (columns 0 and 1 equal to 1) against the hi/lo
 // bias rows.  hi + lo reproduces the FP32 bias to about 2^-17 relative.
 //
-// Every mbarrier wait is bounded (about 1 s of clock); on expiry the warpgroup stops issuing,
-// finishes its loop without waiting, the kernel sets *status and releases its TMEM.
+// Synchronisation is by mbarriers: each epilogue warp publishes its rows of a step (proxy fence,
+// one arrival per warp on the slot's publish barrier); the issuing warp, seeing four arrivals,
+// issues and commits to the slot's MMA barrier, which the epilogue warps wait on before reading
+// TMEM.  Every wait is bounded (about 1 s of clock without progress); on expiry the waiting side
+// raises its warpgroup's abort flag, no further MMAs are issued for it, its warps finish their loops without waiting, the kernel sets *status and
+// releases its TMEM.
 #include "cp_flow.cuh"
 #include "cp_internal.cuh"
 #include "cp_tc.cuh"
@@ -33,13 +39,13 @@
 #define CP_TC_PER 14848
 #define CP_TC_IMG (CP_FLOW_NC * CP_TC_PER)
 #define CP_TC_WG 4
-#define CP_TC_THREADS (CP_TC_WG * 128)
+#define CP_TC_THREADS (CP_TC_WG * 128 + CP_TC_WG * 32)   // 4 epilogue warpgroups + 4 issuing warps
 #define CP_TC_HBYTES 16384                      // activation buffer of one slot: [128][64] bf16
 #define CP_TC_S_ONES CP_TC_IMG                  // [128][16] bf16 constant block
 #define CP_TC_S_H (CP_TC_S_ONES + 4096)
 #define CP_TC_S_EDGE (CP_TC_S_H + CP_TC_WG * 2 * CP_TC_HBYTES)
 #define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
-#define CP_TC_SMEM (CP_TC_S_MISC + 128 + 1024)  // + slack for 1024-byte alignment of the base
+#define CP_TC_SMEM (CP_TC_S_MISC + 384 + 1024)  // + slack for 1024-byte alignment of the base
 #define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
 #define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
 
@@ -171,13 +177,14 @@ __device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint32_t hbuf, uint32
   cp_tc_mma(d, cp_tc_desc(ones, 2048, 128), cp_tc_desc(w + CP_TC_B3B, 256, 128), CP_TC_IDESC16, 1u);
 }
 
-// makes this warpgroup's shared-memory writes visible to the tensor core and meets at the
-// warpgroup barrier; afterwards the issuing thread may start MMAs that read them
-__device__ __forceinline__ void cp_tc_publish(uint32_t bar_id)
+// makes this warp's shared-memory writes (and its earlier TMEM reads) visible to the tensor core
+// and arrives once on the slot's publish barrier (four arrivals complete a step)
+__device__ __forceinline__ void cp_tc_publish(uint32_t pub)
 {
   cp_fence_proxy_async();
   cp_tc_fence_before();
-  cp_bar_wg(bar_id);
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) cp_mbar_arrive(pub);
 }
 
 // waits for the slot's MMAs (warp-uniform result)
@@ -220,9 +227,9 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   uint8_t* sm = smem_raw + pad;
   const uint32_t sbase = raw + pad;
   float2* sEdge = reinterpret_cast<float2*>(sm + CP_TC_S_EDGE);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + CP_TC_S_MISC + 64);
-  int* abort_flags = reinterpret_cast<int*>(sm + CP_TC_S_MISC + 80);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC);   // [0, 8) MMA done, [8, 16) publish
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + CP_TC_S_MISC + 128);
+  int* abort_flags = reinterpret_cast<int*>(sm + CP_TC_S_MISC + 144);
 
   const int tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, row = tid & 127;
 
@@ -236,7 +243,10 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   }
   if (tid < CP_TC_WG) abort_flags[tid] = 0;
   if (tid == 0) {
-    for (int i = 0; i < 2 * CP_TC_WG; ++i) cp_mbar_init(cp_smem_u32(&mbar[i]), 1);
+    for (int i = 0; i < 2 * CP_TC_WG; ++i) {
+      cp_mbar_init(cp_smem_u32(&mbar[i]), 1);
+      cp_mbar_init(cp_smem_u32(&mbar[2 * CP_TC_WG + i]), 4);
+    }
     cp_mbar_init_fence();
   }
   if (warp == 0) {
@@ -248,114 +258,136 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   __syncthreads();
   cp_tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-
-  const uint32_t bar_id = 1 + wg;
-  volatile int* abort = abort_flags + wg;
-  const bool issuer = row == 0;
-  const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
   const uint32_t ones = sbase + CP_TC_S_ONES;
-  uint32_t hb[2], tc[2], mb[2], ph[2] = {0u, 0u};
-#pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    hb[s] = sbase + CP_TC_S_H + (wg * 2 + s) * CP_TC_HBYTES;
-    tc[s] = tmem + (uint32_t)((wg * 2 + s) * 64);
-    mb[s] = cp_smem_u32(&mbar[wg * 2 + s]);
-  }
-
   const uint64_t npairs = (n + 255) / 256;
-  for (uint64_t q = (uint64_t)blockIdx.x * CP_TC_WG + wg; q < npairs; q += (uint64_t)gridDim.x * CP_TC_WG) {
-    CpTcPoint t[2];
-    uint64_t p[2];
+  const uint64_t stride = (uint64_t)gridDim.x * CP_TC_WG;
+
+  if (warp >= 4 * CP_TC_WG) {
+    // ---- issuing warps: warp 16 + g serves warpgroup g; one lane scans its two publish barriers
+    const int g = warp - 4 * CP_TC_WG;
+    if ((tid & 31) == 0) {
+      const uint64_t q0 = (uint64_t)blockIdx.x * CP_TC_WG + g;
+      const uint64_t cnt = q0 < npairs ? (npairs - q0 + stride - 1) / stride : 0;
+      uint32_t rem0 = (uint32_t)(3 * CP_FLOW_NC * cnt), rem1 = rem0, pos0 = 0, pos1 = 0, pph0 = 0, pph1 = 0;
+      const uint32_t pub0 = cp_smem_u32(&mbar[2 * CP_TC_WG + 2 * g]), pub1 = pub0 + 8;
+      const uint32_t hb0 = sbase + CP_TC_S_H + (2 * g) * CP_TC_HBYTES, hb1 = hb0 + CP_TC_HBYTES;
+      const uint32_t tc0 = tmem + (uint32_t)(2 * g * 64), tc1 = tc0 + 64;
+      const uint32_t done0 = cp_smem_u32(&mbar[2 * g]), done1 = done0 + 8;
+      volatile int* abort = abort_flags + g;
+      long long t0 = clock64();
+      while (rem0 | rem1) {
+        if (*abort) break;
+        bool progress = false;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          uint32_t& rem = s ? rem1 : rem0;
+          uint32_t& pos = s ? pos1 : pos0;
+          uint32_t& pph = s ? pph1 : pph0;
+          if (!rem || !cp_mbar_test(s ? pub1 : pub0, pph)) continue;
+          pph ^= 1u;
+          cp_tc_fence_after();
+          const uint32_t hb = s ? hb1 : hb0, tc = s ? tc1 : tc0;
+          const uint32_t w = sbase + (pos / 3) * CP_TC_PER, layer = pos % 3;
+          if (layer == 0) cp_tc_issue_l1(tc, hb, w);
+          else if (layer == 1) cp_tc_issue_l2(tc, hb, ones, w);
+          else cp_tc_issue_l3(tc, hb, ones, w);
+          cp_tc_commit(s ? done1 : done0);
+          pos = pos == 3 * CP_FLOW_NC - 1 ? 0u : pos + 1;
+          --rem;
+          progress = true;
+        }
+        if (progress) {
+          t0 = clock64();
+        } else if (clock64() - t0 > CP_TC_WAIT_CYCLES) {
+          *abort = 1;
+          break;
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue warpgroups
+    volatile int* abort = abort_flags + wg;
+    const uint32_t bar_id = 1 + wg;
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+    uint32_t hb[2], tc[2], mb[2], pb[2], ph[2] = {0u, 0u};
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-      p[s] = q * 256 + s * 128 + row;
-      uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
-      if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
-      float jv = 1.f, ld = 0.f, z[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        int bin;
-        const float xv = cp_flow_vegas_in(sEdge + d * CP_MAX_BINS, nb, w[d], jv, bin);
-        ld += cp_tc_logit(xv, z[d]);
-      }
-      t[s].z0 = z[0]; t[s].z1 = z[1]; t[s].z2 = z[2];
-      t[s].ld = ld + __logf(jv);
-      cp_tc_write_in(hb[s], row, 0, t[s]);
+      hb[s] = sbase + CP_TC_S_H + (wg * 2 + s) * CP_TC_HBYTES;
+      tc[s] = tmem + (uint32_t)((wg * 2 + s) * 64);
+      mb[s] = cp_smem_u32(&mbar[wg * 2 + s]);
+      pb[s] = cp_smem_u32(&mbar[2 * CP_TC_WG + wg * 2 + s]);
     }
-    cp_tc_publish(bar_id);
-    if (issuer && !*abort) {
-      cp_tc_fence_after();
+    for (uint64_t q = (uint64_t)blockIdx.x * CP_TC_WG + wg; q < npairs; q += stride) {
+      CpTcPoint t[2];
+      uint64_t p[2];
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
-        cp_tc_issue_l1(tc[s], hb[s], sbase);
-        cp_tc_commit(mb[s]);
+        p[s] = q * 256 + s * 128 + row;
+        uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
+        if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
+        float jv = 1.f, ld = 0.f, z[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          int bin;
+          const float xv = cp_flow_vegas_in(sEdge + d * CP_MAX_BINS, nb, w[d], jv, bin);
+          ld += cp_tc_logit(xv, z[d]);
+        }
+        t[s].z0 = z[0]; t[s].z1 = z[1]; t[s].z2 = z[2];
+        t[s].ld = ld + __logf(jv);
+        cp_tc_write_in(hb[s], row, 0, t[s]);
+        cp_tc_publish(pb[s]);
       }
-    }
 #pragma unroll 1
-    for (int c = 0; c < CP_FLOW_NC; ++c) {
-      const uint32_t w = sbase + c * CP_TC_PER;
+      for (int c = 0; c < CP_FLOW_NC; ++c) {
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {           // ep1: layer-1 output -> layer 2
-        const bool ok = cp_tc_wait(mb[s], ph[s], abort);
-        cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
-        cp_tc_publish(bar_id);
-        if (issuer && !*abort) {
-          cp_tc_fence_after();
-          cp_tc_issue_l2(tc[s], hb[s], ones, w);
-          cp_tc_commit(mb[s]);
+        for (int s = 0; s < 2; ++s) {           // ep1: layer-1 output -> layer 2
+          const bool ok = cp_tc_wait(mb[s], ph[s], abort);
+          cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
+          cp_tc_publish(pb[s]);
         }
-      }
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {           // ep2: layer-2 output -> layer 3
-        const bool ok = cp_tc_wait(mb[s], ph[s], abort);
-        cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
-        cp_tc_publish(bar_id);
-        if (issuer && !*abort) {
-          cp_tc_fence_after();
-          cp_tc_issue_l3(tc[s], hb[s], ones, w);
-          cp_tc_commit(mb[s]);
+        for (int s = 0; s < 2; ++s) {           // ep2: layer-2 output -> layer 3
+          const bool ok = cp_tc_wait(mb[s], ph[s], abort);
+          cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
+          cp_tc_publish(pb[s]);
         }
-      }
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {           // ep3: coupling update, next coupling's layer 1
-        const bool ok = cp_tc_wait(mb[s], ph[s], abort);
-        float o[4] = {0.f, 0.f, 0.f, 0.f};
-        if (ok) cp_tc_ld4(tc[s] + lane_base, o);
-        const CpCoupling k = cp_coupling(c);
+        for (int s = 0; s < 2; ++s) {           // ep3: coupling update, next coupling's layer 1
+          const bool ok = cp_tc_wait(mb[s], ph[s], abort);
+          float o[4] = {0.f, 0.f, 0.f, 0.f};
+          if (ok) cp_tc_ld4(tc[s] + lane_base, o);
+          const CpCoupling k = cp_coupling(c);
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          if (j >= k.nt) break;
-          const float sc = cp_tc_softclamp(o[j]), sh = o[k.nt + j];
-          const int d = k.tr[j];
-          const float zn = fmaf(cp_sel3(t[s], d), __expf(sc), sh);
-          if (d == 0) t[s].z0 = zn;
-          else if (d == 1) t[s].z1 = zn;
-          else t[s].z2 = zn;
-          t[s].ld += sc;
-        }
-        if (c + 1 < CP_FLOW_NC) {
-          cp_tc_write_in(hb[s], row, c + 1, t[s]);
-          cp_tc_publish(bar_id);
-          if (issuer && !*abort) {
-            cp_tc_fence_after();
-            cp_tc_issue_l1(tc[s], hb[s], w + CP_TC_PER);
-            cp_tc_commit(mb[s]);
+          for (int j = 0; j < 2; ++j) {
+            if (j >= k.nt) break;
+            const float sc = cp_tc_softclamp(o[j]), sh = o[k.nt + j];
+            const int d = k.tr[j];
+            const float zn = fmaf(cp_sel3(t[s], d), __expf(sc), sh);
+            if (d == 0) t[s].z0 = zn;
+            else if (d == 1) t[s].z1 = zn;
+            else t[s].z2 = zn;
+            t[s].ld += sc;
+          }
+          if (c + 1 < CP_FLOW_NC) {
+            cp_tc_write_in(hb[s], row, c + 1, t[s]);
+            cp_tc_publish(pb[s]);
           }
         }
       }
-    }
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-      float v0, v1, v2;
-      float ld = t[s].ld;
-      ld += cp_tc_sigmoid(t[s].z0, v0);
-      ld += cp_tc_sigmoid(t[s].z1, v1);
-      ld += cp_tc_sigmoid(t[s].z2, v2);
-      if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+      for (int s = 0; s < 2; ++s) {
+        float v0, v1, v2;
+        float ld = t[s].ld;
+        ld += cp_tc_sigmoid(t[s].z0, v0);
+        ld += cp_tc_sigmoid(t[s].z1, v1);
+        ld += cp_tc_sigmoid(t[s].z2, v2);
+        if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+      }
+      if (cp_bar_wg_or(bar_id, *abort != 0)) break;
     }
-    if (cp_bar_wg_or(bar_id, *abort != 0)) break;
+    if (row == 0 && *abort) atomicOr(status, 1);
   }
-  if (issuer && *abort) atomicOr(status, 1);
   cp_tc_fence_before();
   __syncthreads();
   if (warp == 0) {

@@ -110,6 +110,23 @@ __device__ __forceinline__ void cp_mbar_init(uint32_t mbar, uint32_t count)
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 __device__ __forceinline__ void cp_mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void cp_mbar_arrive(uint32_t mbar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+// non-blocking test of the phase `parity` of an mbarrier
+__device__ __forceinline__ bool cp_mbar_test(uint32_t mbar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
 // Bounded wait for the phase `parity` of an mbarrier (try_wait suspends the thread in hardware
 // until the phase completes or a short time limit): gives up after CP_TC_WAIT_CYCLES clock cycles
 // (about 1 s) or when *abort (shared, per warpgroup) is set by another thread that gave up; on
