@@ -109,6 +109,37 @@ CP_HD void cp_acc2(float& s, float& c, float v)
   c += e;
 }
 
+// Two-lane FP32 arithmetic for the two beams: on sm_100 one packed instruction (FADD2 / FMUL2 /
+// FFMA2) does both lanes, each lane rounded exactly like the scalar operation; on the host, two
+// scalar operations.
+struct CpF2 {
+  float x, y;
+};
+CP_HD CpF2 cp_f2(float a, float b) { CpF2 r; r.x = a; r.y = b; return r; }
+CP_HD CpF2 cp_f2s(float a) { return cp_f2(a, a); }
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float2 cp_tof2(CpF2 a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ CpF2 cp_fromf2(float2 a) { return cp_f2(a.x, a.y); }
+CP_HD CpF2 cp_add2(CpF2 a, CpF2 b) { return cp_fromf2(__fadd2_rn(cp_tof2(a), cp_tof2(b))); }
+CP_HD CpF2 cp_sub2(CpF2 a, CpF2 b) { return cp_fromf2(__fadd2_rn(cp_tof2(a), make_float2(-b.x, -b.y))); }
+CP_HD CpF2 cp_mul2(CpF2 a, CpF2 b) { return cp_fromf2(__fmul2_rn(cp_tof2(a), cp_tof2(b))); }
+CP_HD CpF2 cp_fma2(CpF2 a, CpF2 b, CpF2 c) { return cp_fromf2(__ffma2_rn(cp_tof2(a), cp_tof2(b), cp_tof2(c))); }
+#else
+CP_HD CpF2 cp_add2(CpF2 a, CpF2 b) { return cp_f2(a.x + b.x, a.y + b.y); }
+CP_HD CpF2 cp_sub2(CpF2 a, CpF2 b) { return cp_f2(a.x - b.x, a.y - b.y); }
+CP_HD CpF2 cp_mul2(CpF2 a, CpF2 b) { return cp_f2(a.x * b.x, a.y * b.y); }
+CP_HD CpF2 cp_fma2(CpF2 a, CpF2 b, CpF2 c) { return cp_f2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y)); }
+#endif
+// TwoSum in both lanes, and (s, c) += v with the addition's rounding error kept in c
+CP_HD void cp_acc2_2(CpF2& s, CpF2& c, CpF2 v)
+{
+  const CpF2 t = cp_add2(s, v);
+  const CpF2 bp = cp_sub2(t, s);
+  const CpF2 e = cp_add2(cp_sub2(s, cp_sub2(t, bp)), cp_sub2(v, bp));
+  s = t;
+  c = cp_add2(c, e);
+}
+
 // x-dependent quantities of one beam, from ln x = lnx + lnxLo (<= 0, lnxLo a sub-ulp correction)
 struct CpBeamX {
   float x, omx, lny, uh, ul, x1L;
@@ -192,6 +223,45 @@ CP_HD float cp_cteq_answer(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX&
   return b.x * cp_fmaf(ex, el, ex) * a.qfac;
 }
 
+// The same answer for both beams at once (lane x: beam A, lane y: beam B): every product, FMA
+// residual and TwoSum of cp_cteq_answer in two-lane arithmetic, the transcendentals per lane.
+CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX& bA, const CpBeamX& bB)
+{
+  const CpF2 lny = cp_f2(bA.lny, bB.lny), x = cp_f2(bA.x, bB.x), omx = cp_f2(bA.omx, bB.omx);
+  const CpF2 uh = cp_f2(bA.uh, bB.uh), ul = cp_f2(bA.ul, bB.ul), x1L = cp_f2(bA.x1L, bB.x1L);
+  const CpF2 p = cp_f2s(a.p);
+  const CpF2 ah = cp_mul2(p, lny);
+  const CpF2 al = cp_fma2(p, lny, cp_f2(-ah.x, -ah.y));
+  CpF2 ym1 = cp_f2(cp_expm1f(ah.x), cp_expm1f(ah.y));
+  ym1 = cp_fma2(cp_add2(cp_f2s(1.f), ym1), al, ym1);
+  const CpF2 U = cp_fma2(cp_f2s(a.af8), uh, cp_f2s(1.f));
+  const CpF2 xo = cp_mul2(x, omx);
+  const CpF2 part3 = cp_mul2(xo, cp_fma2(cp_f2s(a.af7), xo, cp_fma2(cp_f2s(a.af6), omx, cp_f2s(a.af5))));
+  const CpF2 L = c.useX1L ? x1L : cp_f2(cp_logf(bA.omx + c.eut2), cp_logf(bB.omx + c.eut2));
+  const float Ch = a.af1 * a.af8, Cl = cp_fmaf(a.af1, a.af8, -Ch);
+  const CpF2 ch = cp_f2s(Ch);
+  const CpF2 t3 = cp_mul2(ch, uh);
+  const CpF2 t3l = cp_fma2(cp_f2s(Cl), uh, cp_fma2(ch, ul, cp_fma2(ch, uh, cp_f2(-t3.x, -t3.y))));
+  const CpF2 qv = cp_mul2(cp_f2s(a.af1), ym1);
+  const CpF2 t4 = cp_mul2(qv, U), t4l = cp_fma2(qv, U, cp_f2(-t4.x, -t4.y));
+  const CpF2 Bv = cp_f2s(a.B);
+  const CpF2 t2 = cp_mul2(Bv, x), t2l = cp_fma2(Bv, x, cp_f2(-t2.x, -t2.y));
+  const CpF2 u1 = cp_f2s(c.ut1);
+  const CpF2 t6 = cp_mul2(u1, x1L), t6l = cp_fma2(u1, x1L, cp_f2(-t6.x, -t6.y));
+  const CpF2 a2 = cp_f2s(a.af2);
+  const CpF2 t7 = cp_mul2(a2, L), t7l = cp_fma2(a2, L, cp_f2(-t7.x, -t7.y));
+  CpF2 eh = cp_f2s(a.A);
+  CpF2 el = cp_add2(cp_add2(t2l, t3l), cp_add2(cp_add2(t4l, t6l), t7l));
+  cp_acc2_2(eh, el, t3);
+  cp_acc2_2(eh, el, t4);
+  cp_acc2_2(eh, el, t2);
+  cp_acc2_2(eh, el, part3);
+  cp_acc2_2(eh, el, t6);
+  cp_acc2_2(eh, el, t7);
+  const CpF2 ex = cp_f2(cp_expf(eh.x), cp_expf(eh.y));
+  return cp_mul2(cp_mul2(x, cp_fma2(ex, el, ex)), cp_f2s(a.qfac));
+}
+
 // CTEQ5L of a proton for both beams at one factorisation scale (PDF::xf + CTEQ5L::xfUpdate):
 // fa, fb = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.  The 8 parametrisations run as a rolled loop
 // over coefficient records `cteq` (staged in shared memory by the kernels) to keep the code
@@ -210,7 +280,8 @@ CP_HD void cp_cteq_pair(const CpCteqPoly* cteq, float Q2, float lnxA, float lnxA
   for (int i = 0; i < 8; ++i) {
     const CpCteqPoly& c = cteq[i];
     const CpCteqQ a = cp_cteq_coef(c, lnQ, Q, invQ);
-    float ra = cp_cteq_answer(c, a, A), rb = cp_cteq_answer(c, a, B);
+    const CpF2 r = cp_cteq_answer2(c, a, A, B);
+    float ra = r.x, rb = r.y;
     // parametrisation 4 is the dbar/ubar ratio; the others are x * answer
     if (i != 4) { ra *= A.x; rb *= B.x; }
 #pragma unroll

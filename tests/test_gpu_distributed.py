@@ -37,7 +37,8 @@ def test_two_shards_sum_to_the_whole():
     # with the whole pass to rounding of the grouping (1e-9 relative)
     assert np.allclose(tot[[0, 1, 3]], whole[[0, 1, 3]], rtol=1e-9)
     assert max(parts[0][2], parts[1][2]) == whole[2]
-    assert np.allclose(tot[4:], whole[4:], rtol=1e-10, atol=1e-300)
+    # per-bin sums are FP32 per warp before the FP64 block sums: agreement to FP32 rounding
+    assert np.allclose(tot[4:], whole[4:], rtol=1e-6, atol=1e-300)
 
 
 def test_histogram_quantile_equals_local_quantile():
