@@ -364,8 +364,10 @@ struct CpPoint {
   float scale;   // K0 alpha_s^2 yMax zMax / tau: w = scale * channel sum
 };
 
+// Weight and state of the point x.  With `pdf` (the 16 values fa[8], fb[8] an earlier evaluation
+// of the same point stored) the CTEQ5L evaluation is skipped.
 CP_HD float cp_had_eval(const CpHadParams& P, const CpCteqPoly* cteq, float x0, float x1, float x2,
-                        CpPoint& pt)
+                        CpPoint& pt, const float* pdf = nullptr)
 {
   // ln tau = (1 - x0) ln tauMin as a (hi, lo) pair: both factors carry their rounding
   float omx0, omx0l;
@@ -393,7 +395,12 @@ CP_HD float cp_had_eval(const CpHadParams& P, const CpCteqPoly* cteq, float x0, 
   float lnx2 = lnTau * x1;
   float lnx2L = cp_fmaf(lnTau, x1, -lnx2) + lnTauL * x1;
   float alphaS = cp_alphas(P, P.kR * pT2);
-  cp_cteq_pair(cteq, P.kF * pT2, lnx1, lnx1L, lnx2, lnx2L, pt.fa, pt.fb);
+  if (pdf) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { pt.fa[k] = pdf[k]; pt.fb[k] = pdf[8 + k]; }
+  } else {
+    cp_cteq_pair(cteq, P.kF * pT2, lnx1, lnx1L, lnx2, lnx2L, pt.fa, pt.fb);
+  }
   cp_brackets(P, tp, up, pt.b);
   float B = cp_channel_sum(P.mask, pt.b, pt.fa, pt.fb);
   pt.k.tau = tau; pt.k.yMax = yMax; pt.k.zMax = zMax; pt.k.sH = sH; pt.k.omz = omz;

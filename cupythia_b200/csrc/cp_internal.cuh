@@ -68,6 +68,8 @@ struct cp_handle {
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
   unsigned long long* d_counter = nullptr; // accepted-event counter
+  float4* d_pdfbuf = nullptr;              // per record slot: PDFs of the accepted point (K1 -> K2)
+  uint64_t pdfbuf_cap = 0;
   uint64_t last_n = 0;
   // added to every point index of the integration, production and adjoint passes (sharding)
   uint64_t point_offset = 0;

@@ -27,6 +27,7 @@ struct UnwLaunch {
   const CpCteqPoly* cteq;
   const double* wmax;          // device threshold
   CpEventRec* out;
+  float4* pdf;                 // per record slot: fa[8], fb[8] of the accepted point (K1 -> K2)
   uint64_t capacity;
   unsigned long long* counter; // events accepted so far (may exceed capacity: reported)
   double* slots;
@@ -102,11 +103,12 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
     const uint64_t p = r * stride + gtid;
     bool accept = false;
     float w = 0.f;
+    CpPoint pt;
     if (p < L.n) {
       uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
       CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
-      w = cp_had_weight(P, sCteq, m.x[0], m.x[1], m.x[2], nullptr) * m.jv;
+      w = cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt) * m.jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
       cp_kahan(s1, c1, w);
       cp_kahan(s2, c2, w * w);
@@ -128,6 +130,12 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
         // weight, pt_hat, process, point: the last 16 bytes of the record
         uint4* dst = reinterpret_cast<uint4*>(L.out + slot) + 3;
         *dst = make_uint4(__float_as_uint(ew), 0u, 0u, (uint32_t)p);
+        // the PDFs of the point, so that the record builder need not evaluate CTEQ5L again
+        float4* q = L.pdf + 4 * slot;
+        q[0] = make_float4(pt.fa[0], pt.fa[1], pt.fa[2], pt.fa[3]);
+        q[1] = make_float4(pt.fa[4], pt.fa[5], pt.fa[6], pt.fa[7]);
+        q[2] = make_float4(pt.fb[0], pt.fb[1], pt.fb[2], pt.fb[3]);
+        q[3] = make_float4(pt.fb[4], pt.fb[5], pt.fb[6], pt.fb[7]);
       }
     }
   }
@@ -149,8 +157,9 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
   }
 }
 
-// K2: dense pass over the reserved slots: re-evaluate the accepted point, pick process and
-// flavours, build the lab-frame kinematics, store the full 64-byte record.
+// K2: dense pass over the reserved slots: re-evaluate the accepted point's kinematics (its PDFs
+// come from K1's per-slot copy), pick process, flavours and colour flow, build the lab-frame
+// kinematics, store the full 64-byte record.
 __global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, const UnwLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
@@ -168,8 +177,14 @@ __global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, c
     cp_point_words(L.seed, point, L.iter, 0, wd);
     cp_point_words(L.seed, point, L.iter, 1, w2);
     CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, tail.w);
+    float pdf[16];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 v = L.pdf[4 * k + q];
+      pdf[4 * q] = v.x; pdf[4 * q + 1] = v.y; pdf[4 * q + 2] = v.z; pdf[4 * q + 3] = v.w;
+    }
     CpPoint pt;
-    cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt);
+    cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt, pdf);
     CpEventRec ev;
     cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
                   cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
@@ -207,6 +222,20 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;
   L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
+  L.pdf = nullptr;
+  if (capacity) {
+    if (capacity > h->pdfbuf_cap) {
+      if (h->d_pdfbuf) {
+        CP_CUDA(h, cudaStreamSynchronize(h->stream));
+        CP_CUDA(h, cudaFree(h->d_pdfbuf));
+        h->d_pdfbuf = nullptr;
+        h->pdfbuf_cap = 0;
+      }
+      CP_CUDA(h, cudaMalloc(&h->d_pdfbuf, sizeof(float4) * 4 * capacity));
+      h->pdfbuf_cap = capacity;
+    }
+    L.pdf = h->d_pdfbuf;
+  }
   L.flow = nullptr;
   if (h->timing) cudaEventRecord(h->tev[0], h->stream);
   if (h->flow_on) {
