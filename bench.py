@@ -191,6 +191,24 @@ class _Null:
         return False
 
 
+def d2h_bandwidth(host, dev):
+    """Plain device -> pinned host copy rate of this box (GB/s) over the e2e record buffer: the
+    bound of the host-buffer path, which moves 64 bytes per event."""
+    import torch
+    nbytes = min(host.numel(), 1 << 30)
+    src = torch.empty(nbytes, dtype=torch.uint8, device=f"cuda:{dev}")
+    dst = host.view(-1)[:nbytes]
+    dst.copy_(src, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        dst.copy_(src, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    return 3 * nbytes / (e0.elapsed_time(e1) / 1e3) / 1e9
+
+
 def oracle_sigma():
     with open(os.path.join(ROOT, "tests", "golden", "sigma_oracle.json")) as f:
         g = json.load(f)
@@ -300,6 +318,7 @@ def run_ours(a):
     stream.synchronize()
     wall = time.perf_counter() - w0
     e2e_sec = allmax(pg, max(e0.elapsed_time(e1) / 1e3, wall), dev)
+    d2h_gbs = d2h_bandwidth(host, dev)
     e2e_all = allsum(pg, e2e_events, dev)
 
     # ---- rooflines of the two dominant kernels from their live CUDA-event durations
@@ -348,7 +367,9 @@ def run_ours(a):
                           "loss_last20": float(np.mean(losses[-20:])), "adjoint_rel_var": ghist[-1]["rel_var"]},
         "kernel_ms_per_step": {k: v[0] / max(1, v[1]) for k, v in kt_f.items()},
         "e2e": {"value": e2e_all / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": GRID_BYTES,
-                "d2h_bytes_per_step": int(d2h / e2e_steps)},
+                "d2h_bytes_per_step": int(d2h / e2e_steps),
+                "d2h_copy_gbs": d2h_gbs, "events_per_s_at_copy_rate": d2h_gbs * 1e9 / RECORD_BYTES,
+                "d2h_seconds_per_step": d2h / e2e_steps / (d2h_gbs * 1e9)},
         "gpu_launches": 4 * a.steps,
         "roofline": roof, "roofline_secondary": roof2,
         "mufu_peak_tops": mufu_peak,

@@ -304,6 +304,21 @@ class Integrator:
         self._check(rc)
         return records[:min(r.n_accepted, capacity)], r.as_dict()
 
+    def unweight_scale_weights(self, n_points, iteration=0, records=None):
+        """cp_unweight with the 7-point scale variation: (records, weights [n_acc, 6], stats); the
+        weight columns are the ratios for (muR, muF) factors (2,1), (1/2,1), (1,2), (1,1/2),
+        (2,2), (1/2,1/2)."""
+        torch = _torch()
+        if records is None:
+            records = torch.empty((n_points, 64), dtype=torch.uint8, device=self.device)
+        w = torch.empty((records.shape[0], 6), dtype=torch.float32, device=self.device)
+        self._check(self.lib.cp_set_scale_weights(self.h, _ptr(w), records.shape[0]))
+        try:
+            rec, st = self.unweight(n_points, iteration=iteration, records=records)
+        finally:
+            self._check(self.lib.cp_set_scale_weights(self.h, None, 0))
+        return rec, w[:rec.shape[0]], st
+
     def generate_host(self, n_points, records_host, iteration=0, chunk=1 << 24):
         """Production pass into a host uint8 tensor/array of shape [capacity, 64]."""
         r = cp_unweight_result()

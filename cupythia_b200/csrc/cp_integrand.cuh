@@ -355,6 +355,7 @@ CP_HD float cp_channel_sum(const float mask[5], const CpBrackets& b, const float
 // ------------------------------------------------------------------------------------------
 struct CpKin {
   float tau, yMax, zMax, sH, omz, opz, lnx1, lnx2, pT2, alphaS;
+  float lnx1L, lnx2L;   // sub-ulp corrections of ln x1, ln x2
 };
 
 struct CpPoint {
@@ -405,8 +406,37 @@ CP_HD float cp_had_eval(const CpHadParams& P, const CpCteqPoly* cteq, float x0, 
   float B = cp_channel_sum(P.mask, pt.b, pt.fa, pt.fb);
   pt.k.tau = tau; pt.k.yMax = yMax; pt.k.zMax = zMax; pt.k.sH = sH; pt.k.omz = omz;
   pt.k.opz = opz; pt.k.lnx1 = lnx1; pt.k.lnx2 = lnx2; pt.k.pT2 = pT2; pt.k.alphaS = alphaS;
+  pt.k.lnx1L = lnx1L; pt.k.lnx2L = lnx2L;
   pt.scale = (zMax > 0.f) ? P.K0 * (alphaS * alphaS) * yMax * zMax * invTau : 0.f;
   return pt.scale * B;
+}
+
+// Scale-variation ratios of an evaluated point, the 7-point variation of mu_R and mu_F around
+// the nominal scales (mu^2 = k pT^2, SigmaProcess::store2Kin, pythia8317/src/SigmaProcess.cc:
+// 906-922): out = w(muR', muF') / w(muR, muF) for (muR', muF') / (muR, muF) = (2, 1), (1/2, 1),
+// (1, 2), (1, 1/2), (2, 2), (1/2, 1/2).  The brackets carry no scale, alpha_s^2 carries mu_R and
+// the two PDFs mu_F, so a mu_R ratio is (alpha_s' / alpha_s)^2 and a mu_F ratio the channel sum
+// with CTEQ5L at the varied scale over the nominal one; the combined points are the products.
+CP_HD void cp_scale_ratios(const CpHadParams& P, const CpCteqPoly* cteq, const CpPoint& pt, float out[6])
+{
+  const float B0 = cp_channel_sum(P.mask, pt.b, pt.fa, pt.fb);
+  if (!(B0 > 0.f) || !(pt.k.alphaS > 0.f)) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) out[j] = 1.f;
+    return;
+  }
+  const float f2[2] = {4.f, 0.25f};
+  float rR[2], rF[2];
+#pragma unroll 1
+  for (int j = 0; j < 2; ++j) {
+    const float a = cp_alphas(P, P.kR * f2[j] * pt.k.pT2) / pt.k.alphaS;
+    rR[j] = a * a;
+    float fa[8], fb[8];
+    cp_cteq_pair(cteq, P.kF * f2[j] * pt.k.pT2, pt.k.lnx1, pt.k.lnx1L, pt.k.lnx2, pt.k.lnx2L, fa, fb);
+    rF[j] = cp_channel_sum(P.mask, pt.b, fa, fb) / B0;
+  }
+  out[0] = rR[0]; out[1] = rR[1]; out[2] = rF[0]; out[3] = rF[1];
+  out[4] = rR[0] * rF[0]; out[5] = rR[1] * rF[1];
 }
 
 CP_HD float cp_had_weight(const CpHadParams& P, const CpCteqPoly* cteq, float x0, float x1, float x2,

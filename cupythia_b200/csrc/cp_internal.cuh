@@ -70,6 +70,8 @@ struct cp_handle {
   unsigned long long* d_counter = nullptr; // accepted-event counter
   float4* d_pdfbuf = nullptr;              // per record slot: PDFs of the accepted point (K1 -> K2)
   uint64_t pdfbuf_cap = 0;
+  float* scalew = nullptr;                 // caller's scale-variation weights (6 per record), or null
+  uint64_t scalew_cap = 0;
   uint64_t last_n = 0;
   // added to every point index of the integration, production and adjoint passes (sharding)
   uint64_t point_offset = 0;

@@ -28,6 +28,7 @@ struct UnwLaunch {
   const double* wmax;          // device threshold
   CpEventRec* out;
   float4* pdf;                 // per record slot: fa[8], fb[8] of the accepted point (K1 -> K2)
+  float* scalew;               // per record slot: 6 scale-variation ratios, or null
   uint64_t capacity;
   unsigned long long* counter; // events accepted so far (may exceed capacity: reported)
   double* slots;
@@ -160,6 +161,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
 // K2: dense pass over the reserved slots: re-evaluate the accepted point's kinematics (its PDFs
 // come from K1's per-slot copy), pick process, flavours and colour flow, build the lab-frame
 // kinematics, store the full 64-byte record.
+template <bool SCALEW>
 __global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, const UnwLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
@@ -188,6 +190,14 @@ __global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, c
     CpEventRec ev;
     cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
                   cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
+    if (SCALEW) {
+      float r[6];
+      cp_scale_ratios(P, sCteq, pt, r);
+      float2* sw = reinterpret_cast<float2*>(L.scalew + 6 * k);
+      sw[0] = make_float2(r[0], r[1]);
+      sw[1] = make_float2(r[2], r[3]);
+      sw[2] = make_float2(r[4], r[5]);
+    }
     const uint4* src = reinterpret_cast<const uint4*>(&ev);
     uint4* dst = reinterpret_cast<uint4*>(L.out + k);
 #pragma unroll
@@ -210,7 +220,7 @@ static int unw_blocks(cp_handle* h)
 
 // Enqueue one production pass on h->stream (no host synchronisation).
 static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, cp_event* out,
-                            uint64_t capacity, double* red_dst)
+                            uint64_t capacity, double* red_dst, float* scalew = nullptr)
 {
   const int blocks = unw_blocks(h);
   int rc = cp_ensure_slots(h, (size_t)blocks * CP_UNW_SLOT);
@@ -223,6 +233,7 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
   L.pdf = nullptr;
+  L.scalew = scalew;
   if (capacity) {
     if (capacity > h->pdfbuf_cap) {
       if (h->d_pdfbuf) {
@@ -252,7 +263,8 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
   if (capacity) {
-    k_unw_build<<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
+    if (L.scalew) k_unw_build<true><<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
+    else k_unw_build<false><<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
     CP_LAUNCH_CHECK(h, "k_unw_build");
   }
   if (h->timing) {
@@ -306,7 +318,9 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: no threshold (cp_weight_quantile or cp_set_wmax)");
   CP_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), h->stream));
-  int rc = unweight_enqueue(h, 0, n_points, iter, records_dev, capacity, h->d_red);
+  if (h->scalew && capacity > h->scalew_cap)
+    return cp_fail(h, CP_ERR_INVALID, "cp_unweight: record capacity exceeds the scale-weight buffer (cp_set_scale_weights)");
+  int rc = unweight_enqueue(h, 0, n_points, iter, records_dev, capacity, h->d_red, h->scalew);
   if (rc) return rc;
   double red[8];
   unsigned long long cnt = 0;
@@ -409,6 +423,19 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   if (out) fill_unw(tot, (double)n_points, wm[0], out);
   if (total_acc > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_generate_host: record buffer too small");
   if (tot[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
+  return CP_OK;
+}
+
+// Scale-variation weights of the production pass: with a buffer set, cp_unweight also writes
+// 6 floats per record slot (the ratios of cp_scale_ratios) into it; null switches them off.
+// cp_generate_host does not write them.
+extern "C" int cp_set_scale_weights(cp_handle* h, float* weights_dev, uint64_t capacity)
+{
+  CP_CHECK_HANDLE(h);
+  if (weights_dev && ((uintptr_t)weights_dev & 7))
+    return cp_fail(h, CP_ERR_INVALID, "cp_set_scale_weights: buffer must be 8-byte aligned");
+  h->scalew = weights_dev;
+  h->scalew_cap = weights_dev ? capacity : 0;
   return CP_OK;
 }
 

@@ -225,6 +225,14 @@ int cp_set_wmax(cp_handle* h, double w_max);
  * Returns CP_ERR_CAPACITY (with the counts filled in) when more events were accepted than fit. */
 int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_event* records_dev,
                 uint64_t capacity, cp_unweight_result* out_host);
+/* Scale-variation weights (the fused reweighting of cuPythia/pipeline/reweight.cu:36-51 and
+ * pipeline/generate.cu:49-54, extended to mu_F): with a device buffer of capacity >= the record
+ * capacity set, cp_unweight also writes 6 floats per record, the event's weight ratios
+ * w(muR', muF') / w(muR, muF) for (muR'/muR, muF'/muF) = (2,1), (1/2,1), (1,2), (1,1/2), (2,2),
+ * (1/2,1/2), evaluated at the event's own point (alpha_s at the varied mu_R, CTEQ5L at the
+ * varied mu_F).  The varied cross section of a sample is w_max / n x sum(event weight x ratio).
+ * weights_dev = NULL switches them off; cp_generate_host does not write them. */
+int cp_set_scale_weights(cp_handle* h, float* weights_dev, uint64_t capacity);
 /* The same production pass delivering the records to HOST memory (pinned for overlap), in
  * chunks of `chunk` points whose device-to-host copies overlap the next chunk's compute. */
 int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t chunk,
