@@ -125,6 +125,7 @@ SIGNATURES = {
     "cp_flow_sample": [_P, _u64, _u64, _u32, _u32, _P],
     "cp_flow_enable": [_P, _i],
     "cp_flow_select_kernel": [_P, _i],
+    "cp_flow_test_stall": [_P, _i],
     "cp_colour_tags": [C.c_uint16, C.c_uint16, _P, _P],
     "cp_write_lhef": [C.POINTER(cp_config), _P, _u64, _d, _d, C.c_char_p],
     "cp_flow_train": [_P, _i, _u64, _d, _P],

@@ -219,7 +219,7 @@ __device__ __forceinline__ void cp_tc_hidden_out(uint32_t taddr, uint32_t hbuf, 
 __global__ void __launch_bounds__(CP_TC_THREADS, 1)
     k_flow_fwd_tc(const uint4* __restrict__ img_g, const double* __restrict__ edges, int nb, uint64_t seed,
                   uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* __restrict__ out,
-                  int* __restrict__ status)
+                  int* __restrict__ status, int stall)
 {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = cp_smem_u32(smem_raw);
@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   if (warp >= 4 * CP_TC_WG) {
     // ---- issuing warps: warp 16 + g serves warpgroup g; one lane scans its two publish barriers
     const int g = warp - 4 * CP_TC_WG;
-    if ((tid & 31) == 0) {
+    if ((tid & 31) == 0 && !stall) {     // stall: test hook, no MMA is ever issued
       const uint64_t q0 = (uint64_t)blockIdx.x * CP_TC_WG + g;
       const uint64_t cnt = q0 < npairs ? (npairs - q0 + stride - 1) / stride : 0;
       uint32_t rem0 = (uint32_t)(3 * CP_FLOW_NC * cnt), rem1 = rem0, pos0 = 0, pos1 = 0, pph0 = 0, pph1 = 0;
@@ -425,7 +425,7 @@ int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter,
   if (grid < 1) return CP_OK;
   k_flow_fwd_tc<<<grid, CP_TC_THREADS, CP_TC_SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_edges,
                                                                  h->nb, h->cfg.seed, point0, n, iter, stream, out,
-                                                                 h->d_flow_status);
+                                                                 h->d_flow_status, h->flow_stall);
   CP_LAUNCH_CHECK(h, "k_flow_fwd_tc");
   return CP_OK;
 }
@@ -440,4 +440,14 @@ int cp_flow_tc_status(cp_handle* h)
   if (!s) return CP_OK;
   CP_CUDA(h, cudaMemset(h->d_flow_status, 0, sizeof(int)));
   return cp_fail(h, CP_ERR_TIMEOUT, "k_flow_fwd_tc: a tensor-core wait expired (results of this pass are invalid)");
+}
+
+// Test hook of the failure path: with on != 0 the issuing warps issue nothing, so every bounded
+// wait of the epilogue expires (about one second of clock), the kernel raises its status word and
+// releases its TMEM, and the call returns CP_ERR_TIMEOUT with the context still usable.
+extern "C" int cp_flow_test_stall(cp_handle* h, int on)
+{
+  CP_CHECK_HANDLE(h);
+  h->flow_stall = on ? 1 : 0;
+  return CP_OK;
 }

@@ -283,6 +283,10 @@ int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uin
  * accumulators over 128-point tiles (default), 1 = warp-level mma.sync tiles.  Both compute the
  * same map; CP_ERR_TIMEOUT from a flow-routed call means a bounded tensor-core wait expired. */
 int cp_flow_select_kernel(cp_handle* h, int which);
+/* Test hook of the failure path of the tcgen05 forward (no reference counterpart): with on != 0
+ * the kernel issues no MMA, every bounded wait expires after about one second, the kernel
+ * releases its tensor memory and the call returns CP_ERR_TIMEOUT; the handle stays usable. */
+int cp_flow_test_stall(cp_handle* h, int on);
 /* Routes cp_vegas_iteration / cp_integrate / cp_point_weights / cp_unweight / cp_generate_host
  * through the flow (on = 1) or the Philox words directly (on = 0). */
 int cp_flow_enable(cp_handle* h, int on);

@@ -177,3 +177,23 @@ def test_training_lowers_the_weight_variance():
     print("relative variance VEGAS %.3e  flow+VEGAS %.3e  loss %.4f -> %.4f" % (rv_base, rv_flow, loss[0], loss[-1]))
     assert rv_flow < rv_base
     assert abs(flow["sigma"] - base["sigma"]) < 5 * np.hypot(flow["sigma_err"], base["sigma_err"])
+
+
+def test_expired_tensor_core_wait_is_reported_and_recoverable(integ):
+    """Failure detection without a GPU fault: the test hook stops MMA issue, so the epilogue's
+    bounded waits expire (about 1 s); the call must return CP_ERR_TIMEOUT (4), and the next call
+    on the same handle must succeed with the normal result."""
+    import cupythia_b200 as cp
+    integ.reset_grid()
+    integ.flow_init(7)
+    integ.flow_kernel("tcgen05")
+    ref = integ.flow_sample(0, 4096, 3, 0).cpu().numpy()
+    integ.lib.cp_flow_test_stall(integ.h, 1)
+    try:
+        with pytest.raises(cp.CpError) as e:
+            integ.flow_sample(0, 4096, 3, 0)
+        assert e.value.code == 4
+    finally:
+        integ.lib.cp_flow_test_stall(integ.h, 0)
+    again = integ.flow_sample(0, 4096, 3, 0).cpu().numpy()
+    assert np.array_equal(again, ref)
