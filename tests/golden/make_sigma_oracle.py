@@ -1,8 +1,8 @@
 """Generates tests/golden/sigma_oracle.json: the FP64 oracle's cross section of the dijet
 configuration (pp 13 TeV, pT_hat > 20 GeV, CTEQ5L, alpha_s(mZ) = 0.13 first order, the five
 HardQCD processes): 10 classic VEGAS iterations of 2^22 points (alpha 1.5, 3 x 50 bins) on the
-oracle, then one pass of 2^27 points on the adapted grid (Philox seed 42, counter iteration 1000).
-bench.py reports the pull of its estimate against this value.  Runtime: about a minute on 8 cores.
+oracle, then one pass of 2^28 points on the adapted grid (Philox seed 42, counter iteration 1000).
+bench.py reports the pull of its estimate against this value.  Runtime: about two minutes on 8 cores.
 
     python tests/golden/make_sigma_oracle.py
 """
@@ -33,7 +33,7 @@ def main():
         L.cpo_had_accumulate(C.byref(cfg), oracle.dptr(edges), NB, SEED, it, 0, 1 << 22, oracle.dptr(sums),
                              oracle.dptr(hist), threads)
         L.cpo_vegas_refine(oracle.dptr(edges), oracle.dptr(hist), 3, NB, 1.5)
-    n = 1 << 27
+    n = 1 << 28
     sums = np.zeros(2)
     L.cpo_had_accumulate(C.byref(cfg), oracle.dptr(edges), NB, SEED, 1000, 0, n, oracle.dptr(sums), None, threads)
     mean = sums[0] / n
