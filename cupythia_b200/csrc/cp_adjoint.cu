@@ -200,15 +200,17 @@ static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream,
   if (n < 2) return cp_fail(h, CP_ERR_INVALID, "cp_adjoint: n_points < 2");
   const int nb = h->nb, width = CP_ADJ_HEAD + 12 * nb;
   const size_t dyn = sizeof(float) * CP_ADJ_WARPS * 12 * nb;
-  static int per_sm = -1;
-  if (per_sm < 0) {
-    if (cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(sizeof(float) * CP_ADJ_WARPS * 12 * CP_MAX_BINS)) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, CP_ADJ_THREADS, dyn) != cudaSuccess ||
+  // the attribute is per device: set it on every call (host-side, cheap)
+  CP_CUDA(h, cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(float) * CP_ADJ_WARPS * 12 * CP_MAX_BINS)));
+  if (h->adj_per_sm < 0) {
+    int per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, CP_ADJ_THREADS, dyn) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
+    h->adj_per_sm = per_sm;
   }
-  const int blocks = h->num_sms * per_sm;
+  const int blocks = h->num_sms * h->adj_per_sm;
   const size_t out_n = 10 + 6 * (nb + 1);
   int rc = cp_ensure_slots(h, (size_t)blocks * width + width + out_n);
   if (rc) return rc;

@@ -152,13 +152,14 @@ int cp_flow_buffer(cp_handle* h, uint64_t n)
 int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out)
 {
   if (h->flow_kernel == 0) return cp_flow_tc_enqueue(h, point0, n, iter, stream, out);
-  static int per_sm = -1;
-  if (per_sm < 0) {
+  if (h->flow_per_sm < 0) {
+    int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_fwd, CP_THREADS, flow_fwd_smem()) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
+    h->flow_per_sm = per_sm;
   }
-  k_flow_fwd<<<h->num_sms * per_sm, CP_THREADS, flow_fwd_smem(), h->stream>>>(
+  k_flow_fwd<<<h->num_sms * h->flow_per_sm, CP_THREADS, flow_fwd_smem(), h->stream>>>(
       h->d_flow_pk, h->d_flow_bias, h->d_edges, h->nb, h->cfg.seed, point0, n, iter, stream, out);
   CP_LAUNCH_CHECK(h, "k_flow_fwd");
   return CP_OK;

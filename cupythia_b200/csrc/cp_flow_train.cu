@@ -537,12 +537,9 @@ extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double l
   if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
   if (n_steps < 1 || batch < 64 || batch > (1ull << 24) || (batch & 31))
     return cp_fail(h, CP_ERR_INVALID, "cp_flow_train: batch must be a multiple of 32 in [64, 2^24]");
-  static bool attr = false;
-  if (!attr) {
-    CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
-    CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
-    attr = true;
-  }
+  // per-device attributes: set on every call (host-side, cheap)
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
   void* mem = nullptr;
   const size_t bytes = train_bytes(batch);
   CP_CUDA(h, cudaMalloc(&mem, bytes + sizeof(double) * (size_t)n_steps));
@@ -583,12 +580,9 @@ extern "C" int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, fl
   CP_CHECK_HANDLE(h);
   if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
   if (batch < 64 || batch > (1ull << 24) || (batch & 31)) return cp_fail(h, CP_ERR_INVALID, "bad batch");
-  static bool attr = false;
-  if (!attr) {
-    CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
-    CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
-    attr = true;
-  }
+  // per-device attributes: set on every call (host-side, cheap)
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
   void* mem = nullptr;
   const size_t bytes = train_bytes(batch);
   CP_CUDA(h, cudaMalloc(&mem, bytes + sizeof(double)));

@@ -62,8 +62,9 @@ struct cp_handle {
   int64_t kin_n = 0, kin_cap = 0;
   float *d_x1 = nullptr, *d_x2 = nullptr, *d_sH = nullptr, *d_tH = nullptr;
   float *d_as = nullptr, *d_q2r = nullptr, *d_q2f = nullptr;
-  // launch shape of the persistent integrand kernels
+  // launch shapes (resident blocks per SM on this handle's device; -1 until first use)
   int had_blocks = 0;
+  int adj_per_sm = -1, flow_per_sm = -1, unw_per_sm = -1;
   // weight histogram of the last iteration and the unweighting threshold (device)
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q

@@ -209,13 +209,14 @@ __global__ void k_set_wmax(double* wmax, double v) { wmax[0] = v; }
 
 static int unw_blocks(cp_handle* h)
 {
-  static int per_sm = -1;
-  if (per_sm < 0) {
+  if (h->unw_per_sm < 0) {
+    int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unw_accept, CP_THREADS, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
+    h->unw_per_sm = per_sm;
   }
-  return h->num_sms * per_sm;
+  return h->num_sms * h->unw_per_sm;
 }
 
 // Enqueue one production pass on h->stream (no host synchronisation).
