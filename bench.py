@@ -155,6 +155,10 @@ def measured_peaks():
 # algorithmic work per point of the two dominant kernels
 FP32_FLOP_PER_POINT = 3278.0      # k_unw_accept: FADD + FMUL + 2 FFMA per point (ncu SASS counters, profiles/)
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
+# DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
+# launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points
+TRAFFIC_PER_POINT = {"k_unw_accept": (508976640 + 708100352) / 2 ** 24,
+                     "k_flow_fwd_tc": (108544 + 209209344) / 2 ** 24}
 
 
 def production(it, n, records, k0, warmup, steps, pg, dev, stream, clocks=None):
@@ -332,11 +336,13 @@ def run_ours(a):
     r_acc = {"bound": "fp32", "kernel": "k_unw_accept", "achieved": roof_acc, "peak": fp32_peak,
              "unit": "TFLOP/s", "frac": roof_acc / fp32_peak,
              "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks)",
-             "flop_per_point": FP32_FLOP_PER_POINT, "traffic": None, "ms_per_launch": acc_ms / acc_n}
-    r_flow = {"bound": "tensor", "kernel": "k_flow_fwd", "achieved": roof_flow, "peak": bf16_peak,
+             "flop_per_point": FP32_FLOP_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_unw_accept"] * n,
+             "ms_per_launch": acc_ms / acc_n}
+    r_flow = {"bound": "tensor", "kernel": "k_flow_fwd_tc", "achieved": roof_flow, "peak": bf16_peak,
               "unit": "TFLOP/s", "frac": roof_flow / bf16_peak,
               "peak_source": "MEASURED_PEAKS.json bf16 sustained (%s)" % src,
-              "flop_per_point": FLOW_FLOP_PER_POINT, "traffic": None, "ms_per_launch": flow_ms / flow_n}
+              "flop_per_point": FLOW_FLOP_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_flow_fwd_tc"] * n,
+              "ms_per_launch": flow_ms / flow_n}
     roof, roof2 = (r_acc, r_flow) if acc_ms >= flow_ms else (r_flow, r_acc)
 
     line = {
@@ -430,7 +436,7 @@ def run_reference(a):
         tot_s += last["seconds"]
     v = tot_ev / tot_s
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot_s / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (Pythia RANMAR, seed 1..threads)",
