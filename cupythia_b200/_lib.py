@@ -88,6 +88,7 @@ SIGNATURES = {
     "cp_destroy": [_P],
     "cp_set_stream": [_P, _P],
     "cp_set_point_offset": [_P, _u64],
+    "cp_pick_state_batch": [_P, _i, _P, _P, _P],
     "cp_set_scale_weights": [_P, _P, _u64],
     "cp_vegas_accumulate": [_P, _u64, _u32, _P],
     "cp_vegas_refine_sums": [_P, _P, _d, _d, C.POINTER(cp_result)],

@@ -365,6 +365,32 @@ __global__ void k_sigma(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n
   }
 }
 
+// pickInState + setIdColAcol of one process over the stored batch: per point the uniforms
+// r = (pair, new flavour, colour topology, gg -> gg orientation); PDFs at Q2Fac of the batch.
+__global__ void k_pick_state(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n, int k,
+                             const float* __restrict__ x1, const float* __restrict__ x2,
+                             const float* __restrict__ sH, const float* __restrict__ tH,
+                             const float* __restrict__ q2f, const float4* __restrict__ r,
+                             short4* __restrict__ ids, uint16_t* __restrict__ colour)
+{
+  __shared__ CpCteqPoly cteq[8];
+  cp_stage_cteq(cteq, cteq_g);
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float s = sH[i], t = tH[i], u = -(s + t);
+    const float tp = t / s, up = u / s;
+    CpPoint pt;
+    cp_brackets(P, tp, up, pt.b);
+    cp_cteq_pair(cteq, q2f[i], logf(x1[i]), 0.f, logf(x2[i]), 0.f, pt.fa, pt.fb);
+    const float4 ri = r[i];
+    int id[4];
+    cp_pick_pair(P, k, pt, ri.x, ri.y, id);
+    ids[i] = make_short4((short)id[0], (short)id[1], (short)id[2], (short)id[3]);
+    colour[i] = (uint16_t)cp_colour_flow(111 + k, id, tp, up, ri.z, ri.w);
+  }
+}
+
 __global__ void k_pdf(const CpCteqPoly* cteq_g, int64_t n, const float* __restrict__ x,
                       const float* __restrict__ q2, float* out)
 {
@@ -438,6 +464,22 @@ extern "C" int cp_sigma_pdf_batch(cp_handle* h, int mask, float* out)
   CP_CHECK_HANDLE(h);
   if ((mask & ~CP_PROC_ALL) || !mask) return cp_fail(h, CP_ERR_INVALID, "cp_sigma_pdf_batch: bad mask");
   return sigma_launch(h, 2, 0, 0, 0, mask, out);
+}
+
+extern "C" int cp_pick_state_batch(cp_handle* h, int code, const float* r_dev, int16_t* ids_dev, uint16_t* colour_dev)
+{
+  CP_CHECK_HANDLE(h);
+  if (code < 111 || code > 115) return cp_fail(h, CP_ERR_INVALID, "cp_pick_state_batch: code 111..115");
+  if (!h->kin_n) return CP_OK;
+  if (!r_dev || !ids_dev || !colour_dev || ((uintptr_t)r_dev & 15) || ((uintptr_t)ids_dev & 7))
+    return cp_fail(h, CP_ERR_INVALID, "cp_pick_state_batch: r (16-byte aligned) and ids (8-byte aligned) required");
+  k_pick_state<<<grid_for(h, h->kin_n), 256, 0, h->stream>>>(h->P, h->d_cteq, h->kin_n, code - 111, h->d_x1, h->d_x2,
+                                                             h->d_sH, h->d_tH, h->d_q2f,
+                                                             reinterpret_cast<const float4*>(r_dev),
+                                                             reinterpret_cast<short4*>(ids_dev), colour_dev);
+  CP_LAUNCH_CHECK(h, "k_pick_state");
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
 }
 
 extern "C" int cp_scales_batch(cp_handle* h, float* as, float* q2r, float* q2f)

@@ -550,18 +550,11 @@ CP_HD void cp_process_shares(const float mask[5], const CpBrackets& b, const flo
   c[4] = mask[4] * Dopp * b.qqbar2gg;
 }
 
-// Picks (process, id1, id2, id3, id4) from uniforms r0 (process), r1 (pair), r3 (new flavour).
-CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, float r1, float r3,
-                            int& code, int id[4])
+// pickInState of process k (0..4 = codes 111..115; SigmaProcess.cc:486-508) with uniform r1 and
+// the outgoing flavours of its setIdColAcol (new flavour of g g -> q qbar from r3,
+// SigmaQCD.cc:173): id = (in a, in b, out 3, out 4).
+CP_HD void cp_pick_pair(const CpHadParams& P, int k, const CpPoint& pt, float r1, float r3, int id[4])
 {
-  float c[5];
-  cp_process_shares(P.mask, pt.b, pt.fa, pt.fb, c);
-  float tot = c[0] + c[1] + c[2] + c[3] + c[4];
-  float t = r0 * tot;
-  int k = 0;
-  while (k < 4 && (t >= c[k] || c[k] <= 0.f)) { t -= c[k]; ++k; }
-  if (c[k] <= 0.f) { k = 0; while (k < 4 && !(c[k] > 0.f)) ++k; }
-  code = 111 + k;
   const float* A = pt.fa;
   const float* B = pt.fb;
   int a = 21, bb = 21;
@@ -639,6 +632,21 @@ CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, f
     if (qn > (int)P.nQuarkNew) qn = (int)P.nQuarkNew;
     id[2] = qn; id[3] = -qn;
   } else { id[2] = a; id[3] = bb; }
+}
+
+// Picks (process, id1, id2, id3, id4) from uniforms r0 (process), r1 (pair), r3 (new flavour).
+CP_HD void cp_pick_flavours(const CpHadParams& P, const CpPoint& pt, float r0, float r1, float r3,
+                            int& code, int id[4])
+{
+  float c[5];
+  cp_process_shares(P.mask, pt.b, pt.fa, pt.fb, c);
+  float tot = c[0] + c[1] + c[2] + c[3] + c[4];
+  float t = r0 * tot;
+  int k = 0;
+  while (k < 4 && (t >= c[k] || c[k] <= 0.f)) { t -= c[k]; ++k; }
+  if (c[k] <= 0.f) { k = 0; while (k < 4 && !(c[k] > 0.f)) ++k; }
+  code = 111 + k;
+  cp_pick_pair(P, k, pt, r1, r3, id);
 }
 
 // Colour flow of the process's setIdColAcol (pythia8317/src/SigmaQCD.cc: Sigma2gg2gg :135-148,

@@ -9,9 +9,14 @@ batch methods over device arrays:
     sigmaKin(); sigmaHat()                       sigmaHat(id1=0, id2=0)      GeV^-4
     sigmaPDF()                                   sigmaPDF()                  mb GeV^-2
     alphaSRen(), Q2Ren(), Q2Fac()                same names, arrays
+    pickInState()                                pickInState(r_pair) -> (id1, id2)
+    setIdColAcol()                               setIdColAcol(r_flavour, r_colour, r_orient)
+                                                 -> (ids [n, 4], col [n, 4], acol [n, 4])
 
 As in Pythia, ``sigmaHat`` of ``Sigma2qq2qq`` needs the incoming flavour pair; the others are
-flavour independent.  Errors raise :class:`cupythia_b200.CpError` with Pythia's meaning of
+flavour independent.  Pythia draws its own random numbers in ``pickInState`` and
+``setIdColAcol``; here the caller passes the uniforms (one per point per draw), so a batch is
+reproducible.  Errors raise :class:`cupythia_b200.CpError` with Pythia's meaning of
 "invalid input"; there is no CPU path.
 """
 import numpy as np
@@ -77,6 +82,32 @@ class Sigma2Process:
         a, r, f = self._out(), self._out(), self._out()
         self.it._check(self.it.lib.cp_scales_batch(self.it.h, _ptr(a), _ptr(r), _ptr(f)))
         return a, r, f
+
+    def _pick(self, r_pair, r_flavour, r_colour, r_orient):
+        import torch
+        r = torch.stack([self._dev(np.array(np.broadcast_to(v, (self.n,)))) for v in (r_pair, r_flavour, r_colour, r_orient)],
+                        1).contiguous()
+        ids = torch.empty((self.n, 4), dtype=torch.int16, device=self.it.device)
+        colour = torch.empty(self.n, dtype=torch.int16, device=self.it.device)
+        self.it._check(self.it.lib.cp_pick_state_batch(self.it.h, self._code, _ptr(r), _ptr(ids), _ptr(colour)))
+        return ids, colour
+
+    def pickInState(self, r_pair):
+        """Incoming flavour pair of every point of the batch (SigmaProcess::pickInState)."""
+        self._r_pair = np.asarray(r_pair, np.float32)
+        ids, _ = self._pick(self._r_pair, 0.5, 0.5, 0.5)
+        return ids[:, 0], ids[:, 1]
+
+    def setIdColAcol(self, r_flavour=0.5, r_colour=0.5, r_orient=0.5):
+        """Outgoing flavours and colour tags (the process's setIdColAcol) for the pairs of the last
+        pickInState; returns (ids [n, 4], col [n, 4], acol [n, 4]) as numpy arrays."""
+        from . import colour_tags, EVENT_DTYPE
+        ids, colour = self._pick(self._r_pair, r_flavour, r_colour, r_orient)
+        ev = np.zeros(self.n, EVENT_DTYPE)
+        ev["process"] = self._code
+        ev["colour"] = colour.cpu().numpy().view(np.uint16)
+        col, acol = colour_tags(ev)
+        return ids.cpu().numpy(), col, acol
 
     def alphaSRen(self):
         return self._scales()[0]

@@ -147,6 +147,13 @@ int cp_sigma_hat_batch(cp_handle* h, int process_code, int id1, int id2, float* 
 /* Batched sigmaPDF() (pythia8317/src/SigmaProcess.cc:423-480) summed over the processes of
  * proc_mask: sum over pairs of CONVERT2MB sigmaHat xf_a(x1) xf_b(x2), mb GeV^-2. */
 int cp_sigma_pdf_batch(cp_handle* h, int proc_mask, float* out_dev);
+/* SigmaProcess::pickInState (SigmaProcess.cc:486-508: the first pair of the initFlux list whose
+ * running sum of pdfSigma reaches r x the total) and setIdColAcol (SigmaQCD.cc:135-342) of
+ * process `code` over the stored batch, with PDFs at its Q2Fac.  r_dev: 4 uniforms per point
+ * (pair, new flavour of g g -> q qbar, colour topology, g g -> g g orientation; 16-byte aligned);
+ * ids_dev: 4 PDG ids per point (in a, in b, out 3, out 4; 8-byte aligned); colour_dev: the
+ * colour-flow code of the event records (cp_colour_tags). */
+int cp_pick_state_batch(cp_handle* h, int code, const float* r_dev, int16_t* ids_dev, uint16_t* colour_dev);
 /* Accessors alphaSRen(), Q2Ren(), Q2Fac() of the stored batch (SigmaProcess.h:254-257). */
 int cp_scales_batch(cp_handle* h, float* alphas_dev, float* q2ren_dev, float* q2fac_dev);
 /* CTEQ5L x f(id, x, Q2) of a proton (PDF::xf, pythia8317/src/PartonDistributions.cc:122-180):

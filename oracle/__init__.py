@@ -55,6 +55,8 @@ _SIG = {
     "cpo_had_weight_grad": (None, [C.c_void_p, _PD, _PD]),
     "cpo_had_adjoint_sums": (None, [C.c_void_p, _PD, C.c_int, _U64, _U32, _U32, _U64, _U64, _PD, C.c_int]),
     "cpo_accept": (C.c_int, [_D, _D, _U32]),
+    "cpo_pick_state": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int),
+                                 C.POINTER(C.c_int)]),
     "cpo_pick_record": (C.c_int, [C.c_void_p, _PD, _D, _D, _D, _D, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "cpo_flow_forward": (None, [C.c_void_p, _PD, _PD, _PD]),
     "cpo_flow_set_rounding": (None, [C.c_int]),
@@ -137,4 +139,12 @@ def pick_record(cfg, x, r0, r1, r3, rc, rs):
     xx = np.ascontiguousarray(np.asarray(x, np.float64))
     code = lib().cpo_pick_record(C.byref(cfg), dptr(xx), r0, r1, r3, rc, rs, ids, C.byref(col))
     return code, list(ids), col.value
+
+
+def pick_state(cfg, code, x1, x2, sH, tH, r1, r3, rc, rs):
+    """(code or 0, ids[4], colour) of the oracle's pickInState + setIdColAcol at given kinematics."""
+    ids = (C.c_int * 4)()
+    col = C.c_int()
+    got = lib().cpo_pick_state(C.byref(cfg), code, x1, x2, sH, tH, r1, r3, rc, rs, ids, C.byref(col))
+    return got, list(ids), col.value
 

@@ -265,24 +265,29 @@ double cpo_had_weight_x(const cpo_had_cfg* c, const double x[3], double tyz[3])
  * Returns the process code (0 if the point has no weight); id[4] and the colour code in the
  * record's encoding (bits 0-1 topology, bit 2 swapColAcol, bit 3 swapCol1234).
  * ------------------------------------------------------------------------------------- */
-int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3, double rc,
-                    double rs, int id[4], int* colour)
+/* Pair lists of every process at one phase-space point, in initFlux order (SigmaProcess.cc:124-193),
+ * each pair term sigmaHat(id1, id2) * xfA * xfB (the common factors dropped). */
+typedef struct {
+  int pa[5][128], pb[5][128], np[5];
+  double ps[5][128], tot[5];
+  double sH, tH, uH;
+} cpo_pairs;
+
+static void pick_lists(const cpo_had_cfg* c, double x1, double x2, double sH, double tH, cpo_pairs* L)
 {
-  double tyz[3];
-  if (!(weight_x_r(c, c->aSmZ, c->kR, c->pTmin, x, tyz) > 0.0)) return 0;
-  const double s = c->sqrtS * c->sqrtS;
-  const double tau = tyz[0], y = tyz[1], z = tyz[2];
-  const double sH = tau * s, tH = -0.5 * sH * (1.0 - z), uH = -0.5 * sH * (1.0 + z);
-  const double x1 = sqrt(tau) * exp(y), x2 = sqrt(tau) * exp(-y);
+  const double uH = -sH - tH;
   const double pT2 = tH * uH / sH;
   const double alpS = alphas_r(c->aSmZ, pT2 * c->kR);
   double A[8], B[8];
   cteq5l_r(x1, pT2 * c->kF, A);
   cteq5l_r(x2, pT2 * c->kF, B);
   const int nQ = c->nQuarkIn;
-  /* pair lists in initFlux order */
-  int pa[5][128], pb[5][128], np[5] = {0, 0, 0, 0, 0};
-  double ps[5][128], tot[5] = {0, 0, 0, 0, 0};
+  int (*pa)[128] = L->pa, (*pb)[128] = L->pb;
+  int* np = L->np;
+  double (*ps)[128] = L->ps;
+  double* tot = L->tot;
+  for (int k = 0; k < 5; ++k) { np[k] = 0; tot[k] = 0.0; }
+  L->sH = sH; L->tH = tH; L->uH = uH;
   const int bit[5] = {CPO_GG2GG, CPO_GG2QQBAR, CPO_QG2QG, CPO_QQ2QQ, CPO_QQBAR2GG};
 #define CPO_ADD(k, a, b, me)                                                       \
   do {                                                                             \
@@ -306,12 +311,20 @@ int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r
       if (q) CPO_ADD(4, q, -q, me);
   }
 #undef CPO_ADD
-  double all = 0.0;
-  for (int k = 0; k < 5; ++k) all += tot[k];
-  double t = r0 * all;
-  int k = 0;
-  while (k < 4 && (t >= tot[k] || tot[k] <= 0.0)) { t -= tot[k]; ++k; }
-  if (tot[k] <= 0.0) { k = 0; while (k < 4 && !(tot[k] > 0.0)) ++k; }
+}
+
+/* pickInState of process k with r1 (the first pair whose running sum of pair terms reaches
+ * r1 x the process total; the last pair if rounding leaves none), the new flavour of
+ * Sigma2gg2qqbar::sigmaKin (SigmaQCD.cc:173) from r3, and setIdColAcol's colour flow from rc, rs. */
+static int pick_finish(const cpo_had_cfg* c, int k, const cpo_pairs* L, double r1, double r3, double rc,
+                       double rs, int id[4], int* colour)
+{
+  const int (*pa)[128] = (const int (*)[128])L->pa, (*pb)[128] = (const int (*)[128])L->pb;
+  const int* np = L->np;
+  const double (*ps)[128] = (const double (*)[128])L->ps;
+  const double* tot = L->tot;
+  const double sH = L->sH, tH = L->tH, uH = L->uH;
+  if (np[k] == 0) return 0;
   double u = r1 * tot[k];
   int i = 0;
   for (; i < np[k] - 1; ++i) {
@@ -359,6 +372,37 @@ int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r
   }
   *colour = topo | (swapCA << 2) | (swap12 << 3);
   return 111 + k;
+}
+
+int cpo_pick_state(const cpo_had_cfg* c, int code, double x1, double x2, double sH, double tH, double r1,
+                   double r3, double rc, double rs, int id[4], int* colour)
+{
+  if (code < 111 || code > 115) return 0;
+  cpo_pairs L;
+  pick_lists(c, x1, x2, sH, tH, &L);
+  return pick_finish(c, code - 111, &L, r1, r3, rc, rs, id, colour);
+}
+
+int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3, double rc,
+                    double rs, int id[4], int* colour)
+{
+  double tyz[3];
+  if (!(weight_x_r(c, c->aSmZ, c->kR, c->pTmin, x, tyz) > 0.0)) return 0;
+  const double s = c->sqrtS * c->sqrtS;
+  const double tau = tyz[0], y = tyz[1], z = tyz[2];
+  const double sH = tau * s, tH = -0.5 * sH * (1.0 - z), uH = -0.5 * sH * (1.0 + z);
+  const double x1 = sqrt(tau) * exp(y), x2 = sqrt(tau) * exp(-y);
+  (void)uH;
+  cpo_pairs L;
+  pick_lists(c, x1, x2, sH, tH, &L);
+  const double* tot = L.tot;
+  double all = 0.0;
+  for (int k = 0; k < 5; ++k) all += tot[k];
+  double t = r0 * all;
+  int k = 0;
+  while (k < 4 && (t >= tot[k] || tot[k] <= 0.0)) { t -= tot[k]; ++k; }
+  if (tot[k] <= 0.0) { k = 0; while (k < 4 && !(tot[k] > 0.0)) ++k; }
+  return pick_finish(c, k, &L, r1, r3, rc, rs, id, colour);
 }
 
 double cpo_vegas_map(const double* edges, int nb, const uint32_t w[3], double x[3], int bins[3])

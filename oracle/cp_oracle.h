@@ -93,6 +93,9 @@ double cpo_had_density(const cpo_had_cfg* c, double tau, double y, double z);
 /* Weight of a point x in [0,1]^3 through the analytic base map (tau,y,z)(x):
  * returns f * J_base; fills tyz[3] = (tau, y, z) if non-null. */
 /* record picks (process, incoming pair, new flavour, colour flow) of an accepted point at x */
+/* pickInState + setIdColAcol of process `code` at given kinematics (x1, x2, sH, tH) */
+int    cpo_pick_state(const cpo_had_cfg* c, int code, double x1, double x2, double sH, double tH, double r1,
+                      double r3, double rc, double rs, int id[4], int* colour);
 int    cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3,
                        double rc, double rs, int id[4], int* colour);
 double cpo_had_weight_x(const cpo_had_cfg* c, const double x[3], double tyz[3]);

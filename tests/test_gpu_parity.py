@@ -252,3 +252,47 @@ def test_edge_cases(integ):
     # ragged sizes: not a multiple of the block or grid size
     w = integ.point_weights(3, 1000003 % 4099)
     assert np.all(np.isfinite(w.cpu().numpy()))
+
+
+def test_pick_in_state_and_set_id_col_acol_match_oracle():
+    import oracle
+    """The SigmaProcess surface's pickInState and setIdColAcol over a batch, per process, against
+    the oracle's restatement at the same FP32 kinematics and uniforms (<= 1 in 1000 may differ:
+    FP32 pair sums against FP64 ones at a boundary)."""
+    import ctypes as C
+
+    import cupythia_b200 as cp
+    from cupythia_b200.sigma import HARD_QCD
+    cfg = oracle.had_cfg()
+    rng = np.random.default_rng(12)
+    s = cfg.sqrtS ** 2
+    kin = []
+    while len(kin) < 3000:
+        x = rng.random(3)
+        tyz = np.zeros(3)
+        if not oracle.lib().cpo_had_weight_x(C.byref(cfg), oracle.dptr(x), oracle.dptr(tyz)) > 0:
+            continue
+        tau, y, z = tyz
+        sH = tau * s
+        kin.append((np.sqrt(tau) * np.exp(y), np.sqrt(tau) * np.exp(-y), sH, -0.5 * sH * (1 - z)))
+    kin = np.array(kin, np.float32)
+    n = len(kin)
+    with cp.Integrator() as it:
+        for cls in HARD_QCD:
+            sp = cls(integrator=it)
+            sp.set2Kin(kin[:, 0], kin[:, 1], kin[:, 2], kin[:, 3])
+            r = rng.random((n, 4)).astype(np.float32)
+            id1, id2 = sp.pickInState(r[:, 0])
+            ids, col, acol = sp.setIdColAcol(r[:, 1], r[:, 2], r[:, 3])
+            assert np.array_equal(id1.cpu().numpy(), ids[:, 0]) and np.array_equal(id2.cpu().numpy(), ids[:, 1])
+            ref = np.zeros(n, cp.EVENT_DTYPE)
+            ref_ids = np.zeros((n, 4), int)
+            for i in range(n):
+                got, rid, rcol = oracle.pick_state(cfg, sp.code(), *[float(v) for v in kin[i]], *[float(v) for v in r[i]])
+                assert got == sp.code()
+                ref_ids[i] = rid
+                ref["colour"][i] = rcol
+            ref["process"] = sp.code()
+            rc_, ra_ = cp.colour_tags(ref)
+            same = (ids == ref_ids).all(1) & (col == rc_).all(1) & (acol == ra_).all(1)
+            assert (~same).sum() <= n // 1000, (sp.name(), int((~same).sum()))
