@@ -42,7 +42,8 @@
 // ------------------------------------------------------------------------------------------
 // Uniform parameters of the hadronic integrand (built on the host in FP64, stored in FP32).
 // ------------------------------------------------------------------------------------------
-struct CpCteqPoly {
+// 144 bytes, 16-byte aligned: the kernels read one record as nine 128-bit shared-memory loads
+struct alignas(16) CpCteqPoly {
   // per parametrisation i: polynomial coefficients in sb1 = ln ln(Q/alpha_i) - 1.2
   float A[3], B[3], af1[3], af2[3], p[3], af5[3], af6[3], af7[3], af8[3];
   float lnAlpha;  // ln(alpha_i)
@@ -51,6 +52,7 @@ struct CpCteqPoly {
   float ut1;      // ut1_i
   float eut2;     // exp(ut2_i)
   int   useX1L;   // ut2_i < -100: part4 uses ln(1 - x) twice
+  int   pad[3];
 };
 
 struct CpHadParams {
@@ -262,6 +264,21 @@ CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX&
   return cp_mul2(cp_mul2(x, cp_fma2(ex, el, ex)), cp_f2s(a.qfac));
 }
 
+// one coefficient record in 128-bit loads (on the device; a plain copy on the host)
+CP_HD CpCteqPoly cp_load_poly(const CpCteqPoly* p)
+{
+#if defined(__CUDA_ARCH__)
+  CpCteqPoly c;
+  const float4* src = reinterpret_cast<const float4*>(p);
+  float4* dst = reinterpret_cast<float4*>(&c);
+#pragma unroll
+  for (int j = 0; j < (int)(sizeof(CpCteqPoly) / 16); ++j) dst[j] = src[j];
+  return c;
+#else
+  return *p;
+#endif
+}
+
 // CTEQ5L of a proton for both beams at one factorisation scale (PDF::xf + CTEQ5L::xfUpdate):
 // fa, fb = {xd, xu, xg, xubar, xdbar, xs, xc, xb}.  The 8 parametrisations run as a rolled loop
 // over coefficient records `cteq` (staged in shared memory by the kernels) to keep the code
@@ -278,7 +295,7 @@ CP_HD void cp_cteq_pair(const CpCteqPoly* cteq, float Q2, float lnxA, float lnxA
   const CpBeamX A = cp_beam_x(lnxA, lnxAL), B = cp_beam_x(lnxB, lnxBL);
 #pragma unroll 1
   for (int i = 0; i < 8; ++i) {
-    const CpCteqPoly& c = cteq[i];
+    const CpCteqPoly c = cp_load_poly(cteq + i);
     const CpCteqQ a = cp_cteq_coef(c, lnQ, Q, invQ);
     const CpF2 r = cp_cteq_answer2(c, a, A, B);
     float ra = r.x, rb = r.y;
