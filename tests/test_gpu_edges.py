@@ -1,0 +1,112 @@
+"""Edge cases of the GPU path through the C ABI: empty, tiny and ragged sizes (not multiples of
+a warp, block, tile or chunk), the largest and smallest grids, 64-bit seeds and point indices,
+and the size limits, each checked against the oracle or against the regular-size path."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def test_empty_batches_are_no_ops(integ):
+    import torch
+    assert integ.philox_words(42, 0, 0).shape == (0, 4)
+    from cupythia_b200.sigma import Sigma2qg2qg
+    sp = Sigma2qg2qg(integrator=integ)
+    sp.set2Kin([], [], [], [])
+    assert sp.sigmaPDF().numel() == 0 and sp.sigmaKin().numel() == 0
+    integ.flow_init(7)
+    out = torch.empty((1, 4), dtype=torch.float32, device="cuda")
+    import ctypes as C
+    assert integ.lib.cp_flow_sample(integ.h, 0, 0, 0, 0, C.c_void_p(out.data_ptr())) == 0
+
+
+def test_64_bit_seeds_and_point_indices_are_bit_exact(integ):
+    for seed, p0 in [(2 ** 40 + 5, 0), (42, 2 ** 33 + 7), (2 ** 64 - 1, 2 ** 63)]:
+        got = integ.philox_words(seed, p0, 37, 3, 1)
+        ref = oracle.point_words(seed, [p0 + i for i in range(37)], 3, 1)
+        assert np.array_equal(got, ref), (seed, p0)
+
+
+@pytest.mark.parametrize("n_bins", [2, 128])
+def test_smallest_and_largest_grids(n_bins):
+    """Point weights on an adapted grid of n_bins bins per dimension against the FP64 oracle."""
+    import cupythia_b200 as cp
+    with cp.Integrator(n_bins=n_bins) as it:
+        it.integrate(3, 1 << 20, alpha=1.5)
+        n = 4097                                   # ragged
+        w, x = it.point_weights(5, n, 9, with_x=True)
+        grid = it.grid
+        words = it.philox_words(it.cfg.seed, 5, n, 9, 0)
+    m = (words[:, :3] >> 8).astype(np.uint64) * n_bins
+    b = (m >> 24).astype(np.int64)
+    jv = np.prod([n_bins * (grid[d][b[:, d] + 1] - grid[d][b[:, d]]).astype(np.float32) for d in range(3)], 0)
+    ref = oracle.weight_x_batch(oracle.had_cfg(), x.cpu().numpy()) * jv
+    w = w.cpu().numpy().astype(np.float64)
+    keep = ref > 1e-12 * ref.mean()
+    assert np.max(np.abs(w[keep] - ref[keep]) / ref[keep]) < 1e-5
+
+
+def test_ragged_production_matches_its_recount():
+    """A production pass of a prime number of points: every record is a distinct accepted point
+    and the count equals the recount u w_max < w on the same FP32 weights."""
+    import cupythia_b200 as cp
+    n = 1000003
+    with cp.Integrator() as it:
+        it.integrate(4, 1 << 20, alpha=1.5)
+        it.iteration(1 << 20, 30, alpha=0.0)
+        wq = it.weight_quantile(0.999)
+        rec, st = it.unweight(n, iteration=31)
+        w = it.point_weights(0, n, 31).cpu().numpy()
+        words = it.philox_words(it.cfg.seed, 0, n, 31, 0)
+    ev = cp.events_view(rec)
+    u = (words[:, 3] >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
+    expect = np.nonzero(u * np.float32(wq) < w)[0]
+    pts = np.sort(ev["point"].astype(np.int64))
+    assert len(np.unique(pts)) == len(pts) == st["n_accepted"]
+    assert pts.max() < n
+    assert len(np.setxor1d(expect, pts)) <= 2
+
+
+def test_ragged_host_chunks_match_the_device_pass():
+    import torch
+
+    import cupythia_b200 as cp
+    n = 300007
+    with cp.Integrator() as it:
+        it.integrate(4, 1 << 20, alpha=1.5)
+        it.iteration(1 << 20, 32, alpha=0.0)
+        it.weight_quantile(0.999)
+        rec, st = it.unweight(n, iteration=33)
+        host = torch.empty((st["n_accepted"] + 8, 64), dtype=torch.uint8, pin_memory=True)
+        st2 = it.generate_host(n, host, iteration=33, chunk=65537)   # does not divide n
+    assert st2["n_accepted"] == st["n_accepted"]
+    a = cp.events_view(rec)
+    b = cp.events_view(host[:st2["n_accepted"]])
+    assert a[np.argsort(a["point"])].tobytes() == b[np.argsort(b["point"])].tobytes()
+
+
+def test_tiny_passes_and_size_limits(integ):
+    import ctypes as C
+
+    import torch
+
+    import cupythia_b200 as cp
+    r = integ.iteration(2, 40, alpha=0.0)
+    assert r["n_points"] == 2
+    integ.weight_quantile(0.999)
+    rec, st = integ.unweight(2, iteration=41)
+    assert st["n_points"] == 2 and st["n_accepted"] <= 2
+    # more than 2^32 points in one production call is refused before any launch
+    res = cp._lib.cp_unweight_result()
+    recs = torch.empty((1, 64), dtype=torch.uint8, device="cuda")
+    rc = integ.lib.cp_unweight(integ.h, (1 << 32) + 1, 0, C.c_void_p(recs.data_ptr()), 1, C.byref(res))
+    assert rc == cp._lib.CP_ERR_INVALID
+    # a misaligned record buffer is refused
+    rc = integ.lib.cp_unweight(integ.h, 1024, 0, C.c_void_p(recs.data_ptr() + 4), 1, C.byref(res))
+    assert rc == cp._lib.CP_ERR_INVALID
+    # the flow forward of a single point (far below one 128-point tile)
+    integ.flow_init(7)
+    out = integ.flow_sample(11, 1, 3, 0).cpu().numpy()
+    assert np.all(np.isfinite(out)) and np.all((out[0, :3] > 0) & (out[0, :3] < 1))
