@@ -382,7 +382,8 @@ def run_ours(a):
         "clocks": clk.summary(),
     }
     if rank == 0:
-        line["cpu_baseline"] = cpu_baseline(a.cpu_seconds)
+        if world == 1:      # the host-core baseline is timed at N = 1 only
+            line["cpu_baseline"] = cpu_baseline(a.cpu_seconds)
         print(json.dumps(line), flush=True)
     it.close()
     if pg is not None:
