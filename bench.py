@@ -367,6 +367,7 @@ def run_ours(a):
         "flow_vs_plain": value / value_plain,
         "quality": q_f,
         "adapt_seconds": adapt_plain + adapt_flow,
+        "value_with_adaptation": allsum(pg, ev_f, dev) / (sec_f + adapt_flow),
         "proposal": {"used": "flow" if use_flow else "vegas (fallback)",
                      "relative_variance_per_point": relvar},
         "flow_training": {"steps": 200, "batch": 65536, "loss_first": float(losses[0]),

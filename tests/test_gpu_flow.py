@@ -197,3 +197,22 @@ def test_expired_tensor_core_wait_is_reported_and_recoverable(integ):
         integ.lib.cp_flow_test_stall(integ.h, 0)
     again = integ.flow_sample(0, 4096, 3, 0).cpu().numpy()
     assert np.array_equal(again, ref)
+
+
+def test_diverged_flow_is_reported_as_numeric_fault():
+    """A flow with non-finite parameters (what a diverged training leaves) makes the next pass report
+    CP_ERR_NUMERIC (3) with the bad weights zeroed and counted; with the flow switched off the
+    same handle integrates normally again (VEGAS is the fallback)."""
+    import cupythia_b200 as cp
+    with cp.Integrator() as it:
+        it.integrate(3, 1 << 20, alpha=1.5)
+        it.flow_init(7)
+        it.flow_params = np.where(_used_mask(), np.float32(np.nan), np.float32(0))
+        it.flow_enable(True)
+        with pytest.raises(cp.CpError) as e:
+            it.iteration(1 << 20, 40, alpha=0.0)
+        assert e.value.code == 3
+        it.flow_enable(False)
+        r = it.iteration(1 << 20, 41, alpha=0.0)
+        assert r["n_bad"] == 0 and np.isfinite(r["sigma"]) and r["sigma"] > 0
+
