@@ -2,18 +2,18 @@
 //
 // Same map as k_flow_fwd (Philox words -> VEGAS map -> logit -> 4 affine couplings -> sigmoid),
 // with every dense layer as tcgen05.mma over 128-point tiles: A (activations) and B (weights) in
-// shared memory, the FP32 accumulator in TMEM, one elected thread per warpgroup issuing.
+// shared memory, the FP32 accumulator in TMEM.
 //
 // Launch: one persistent CTA per SM (the shared-memory footprint admits one): 4 epilogue
-// warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two 128-point tiles in
-// flight ("slots") with 64 TMEM columns and a 16 KB activation buffer each; thread r of the
-// warpgroup is row r (one point) of both tiles and TMEM lane r.  An issuing warp does nothing
-// but poll its warpgroup's two publish barriers and issue each slot's next layer, so no
-// epilogue warp ever waits on MMA issue.  Per coupling and slot the epilogue has three steps
-//   ep1: wait for layer 1, TMEM -> bias-free ReLU -> BF16 -> activation buffer, issue layer 2
-//   ep2: the same for layer 2, issue layer 3
+// warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two
+// 128-point tiles in flight ("slots") with 64 TMEM columns and a 16 KB activation buffer each;
+// thread r of the warpgroup is row r (one point) of both tiles and TMEM lane r.  An issuing warp
+// does nothing but poll its warpgroup's two publish barriers and issue each slot's next layer,
+// so no epilogue warp ever waits on MMA issue.  Per coupling and slot the epilogue has three steps
+//   ep1: wait for layer 1, TMEM -> ReLU -> BF16 -> activation buffer, publish (layer 2 follows)
+//   ep2: the same for layer 2 (layer 3 follows)
 //   ep3: wait for layer 3, read the 4 output columns, update the point, write the next
-//        coupling's layer-1 input, issue its layer 1
+//        coupling's layer-1 input, publish (its layer 1 follows)
 // and the steps of the two slots alternate, so one slot's MMAs run while the other slot's
 // epilogue runs.  The biases are part of the MMAs: layer 1 has them as input columns 14 and 15
 // (constant 1) times weight rows holding the BF16 high and low parts of the FP32 bias; layers 2
@@ -24,8 +24,8 @@
 // one arrival per warp on the slot's publish barrier); the issuing warp, seeing four arrivals,
 // issues and commits to the slot's MMA barrier, which the epilogue warps wait on before reading
 // TMEM.  Every wait is bounded (about 1 s of clock without progress); on expiry the waiting side
-// raises its warpgroup's abort flag, no further MMAs are issued for it, its warps finish their loops without waiting, the kernel sets *status and
-// releases its TMEM.
+// raises its warpgroup's abort flag, no further MMAs are issued for it, its warps finish their
+// loops without waiting, the kernel sets *status and releases its TMEM.
 #include "cp_flow.cuh"
 #include "cp_internal.cuh"
 #include "cp_tc.cuh"
@@ -45,7 +45,7 @@
 #define CP_TC_S_H (CP_TC_S_ONES + 4096)
 #define CP_TC_S_EDGE (CP_TC_S_H + CP_TC_WG * 2 * CP_TC_HBYTES)
 #define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
-#define CP_TC_SMEM (CP_TC_S_MISC + 384 + 1024)  // + slack for 1024-byte alignment of the base
+#define CP_TC_SMEM (CP_TC_S_MISC + 256 + 1024)  // mbarriers, TMEM address, abort flags; 1024-byte base alignment slack
 #define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
 #define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
 
