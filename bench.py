@@ -14,10 +14,13 @@ run before the timed region and are reported separately (adapt_seconds).
 
   value        flow+adjoint events/s, inputs resident, CUDA events on the library's stream,
                max over ranks; every rank produces a disjoint range of counter points (weak
-               scaling, no data-path collective); plain_vegas holds the same for the plain form
+               scaling, no data-path collective; the adaptation sums are all-reduced once per
+               iteration); plain_vegas holds the same for the plain form; quality: the pull
+               against the FP64 oracle sigma and the points / time the 1% error needs
   e2e          the flow+adjoint form through the host-buffer C-ABI call cp_generate_host: the
                step's inputs (VEGAS grid) copied host -> device and every event record copied
-               device -> pinned host memory inside the timed region
+               device -> pinned host memory inside the timed region; d2h_copy_gbs is the
+               box's plain device -> host copy rate, the bound of this path at 64 B per event
   roofline     the dominant kernel of the timed step from live per-kernel CUDA-event durations
                (cp_set_kernel_timing); roofline_secondary the other one
   --impl reference   stock Pythia 8.317 (ProcessLevel, the same settings) on all host cores

@@ -4,8 +4,10 @@
 // u * w_max < w (cuPythia/07_unweighting_lhe/unweight_lhe.cu:54; overweight events w > w_max
 // are kept with weight w / w_max, as Pythia keeps them, pythia8317/src/ProcessContainer.cc:
 // 383-385) and reserves a slot in the dense record array (one ballot and one global atomic per
-// warp).  K2 then runs over the reserved slots only, with every lane busy, re-evaluates those
-// points and writes their 64-byte records as four 16-byte stores.  Keeping the record builder
+// warp); beside the slot it stores the point's 16 PDF values.  K2 then runs over the reserved
+// slots only, with every lane busy, recomputes the points' kinematics and brackets (the PDFs
+// come from K1), picks process, flavours and colour flow, and writes the 64-byte records as four
+// 16-byte stores (and, on request, the 7-point scale-variation ratios).  Keeping the record builder
 // out of K1 keeps K1's code small (its instruction-cache footprint, not arithmetic, limited the
 // fused version) and its lanes converged.  The reference instead writes flags and runs a
 // separate library compaction pass (cuPythia/10_cub_compaction/cub_compaction.cu:76-80,
