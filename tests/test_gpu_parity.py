@@ -296,3 +296,21 @@ def test_pick_in_state_and_set_id_col_acol_match_oracle():
             rc_, ra_ = cp.colour_tags(ref)
             same = (ids == ref_ids).all(1) & (col == rc_).all(1) & (acol == ra_).all(1)
             assert (~same).sum() <= n // 1000, (sp.name(), int((~same).sum()))
+
+
+def test_philox_words_match_curand(integ, tmp_path):
+    """An independent pin of the counter-RNG: cuRAND's own device Philox-4x32-10
+    (curand_Philox4x32_10) with the same key (seed) and counter (point lo, point hi, iteration,
+    stream) gives bit-identical words."""
+    import os
+    import subprocess
+    src = os.path.join(os.path.dirname(os.path.abspath(__file__)), "curand_philox_probe.cu")
+    exe = str(tmp_path / "curand_philox_probe")
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O2", src, "-o", exe], check=True,
+                   capture_output=True)
+    for seed, p0, it_, st in [(42, 0, 0, 0), (42, 2 ** 32 - 3, 7, 1), (2 ** 40 + 11, 12345, 3, 2)]:
+        out = subprocess.run([exe, str(seed), str(p0), "1000", str(it_), str(st)], check=True, capture_output=True,
+                             text=True).stdout.split()
+        ref = np.array([int(v, 16) for v in out], np.uint32).reshape(-1, 4)
+        got = integ.philox_words(seed, p0, 1000, it_, st)
+        assert np.array_equal(got, ref), (seed, p0, it_, st)
