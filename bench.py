@@ -308,7 +308,7 @@ def run_ours(a):
     grid = it.grid
     for k in range(2):
         it.grid = grid
-        it.generate_host(n, host, iteration=r0 + 90000 + k, chunk=1 << 24)
+        it.generate_host(n, host, iteration=r0 + 90000 + k, chunk=1 << 21)
     barrier(pg, dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -318,7 +318,7 @@ def run_ours(a):
     d2h, e2e_events = 0, 0
     for k in range(e2e_steps):
         it.grid = grid
-        s_ = it.generate_host(n, host, iteration=r0 + 91000 + k, chunk=1 << 24)
+        s_ = it.generate_host(n, host, iteration=r0 + 91000 + k, chunk=1 << 21)
         e2e_events += s_["n_accepted"]
         d2h += s_["n_accepted"] * RECORD_BYTES
     e1.record(stream)

@@ -319,7 +319,7 @@ class Integrator:
             self._check(self.lib.cp_set_scale_weights(self.h, None, 0))
         return rec, w[:rec.shape[0]], st
 
-    def generate_host(self, n_points, records_host, iteration=0, chunk=1 << 24):
+    def generate_host(self, n_points, records_host, iteration=0, chunk=1 << 21):
         """Production pass into a host uint8 tensor/array of shape [capacity, 64]."""
         r = cp_unweight_result()
         ptr = records_host.data_ptr() if hasattr(records_host, "data_ptr") else records_host.ctypes.data

@@ -141,11 +141,19 @@ extern "C" int cp_destroy(cp_handle* h)
   if (!h) return CP_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->gen_copy) cudaStreamSynchronize(h->gen_copy);
   for (int k = 0; k < 4; ++k)
     if (h->tev[k]) cudaEventDestroy(h->tev[k]);
+  for (int k = 0; k < CP_GEN_BUFS; ++k) {
+    if (h->gen_counted[k]) cudaEventDestroy(h->gen_counted[k]);
+    if (h->gen_copied[k]) cudaEventDestroy(h->gen_copied[k]);
+  }
+  if (h->gen_copy) cudaStreamDestroy(h->gen_copy);
+  if (h->h_gen_cnt) cudaFreeHost(h->h_gen_cnt);
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
                   h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq, h->d_flow, h->d_flow_pk,
-                  h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_pdfbuf};
+                  h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_pdfbuf,
+                  h->d_gen_stage, h->d_gen_red, h->d_gen_cnt};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete h;

@@ -14,6 +14,9 @@
 #define CP_WARPS (CP_THREADS / 32)
 // per-block slot of the hadronic accumulation: sum w, sum w^2, max w, n_bad, then 3*nb hist
 #define CP_SLOT_HEAD 4
+// record staging buffers of cp_generate_host: chunk c computes into buffer c % CP_GEN_BUFS while
+// the copies of the previous chunks drain
+#define CP_GEN_BUFS 3
 
 // Weight histogram for the unweighting threshold: bin = IEEE-754 bits of w >> 18 (8 exponent
 // bits + 5 mantissa bits, monotone in w, about 2.2% wide), restricted to 2^-64 <= w < 2^64.
@@ -73,6 +76,18 @@ struct cp_handle {
   uint64_t pdfbuf_cap = 0;
   float* scalew = nullptr;                 // caller's scale-variation weights (6 per record), or null
   uint64_t scalew_cap = 0;
+  // cp_generate_host pipeline, kept between calls: CP_GEN_BUFS record staging buffers of gen_cap
+  // slots each, per-chunk reductions and counters, the counters' host copy in mapped pinned
+  // memory (written by a kernel, so that no count waits behind a record copy), the copy stream
+  // and its events
+  cp_event* d_gen_stage = nullptr;
+  uint64_t gen_cap = 0;
+  double* d_gen_red = nullptr;
+  unsigned long long* d_gen_cnt = nullptr;
+  unsigned long long* h_gen_cnt = nullptr;
+  uint64_t gen_chunks_cap = 0;
+  cudaStream_t gen_copy = nullptr;
+  cudaEvent_t gen_counted[CP_GEN_BUFS] = {}, gen_copied[CP_GEN_BUFS] = {};
   uint64_t last_n = 0;
   // added to every point index of the integration, production and adjoint passes (sharding)
   uint64_t point_offset = 0;

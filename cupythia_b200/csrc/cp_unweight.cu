@@ -337,9 +337,55 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   return CP_OK;
 }
 
-// Chunked production into HOST memory: chunk k is computed into one of two device buffers
-// while chunk k-1 is copied to the host on a second stream, so the PCIe transfer of the
-// records overlaps the integrand.  records_host should be pinned for the copies to overlap.
+// one counter, copied by a kernel into the mapped pinned host array (no copy engine involved)
+__global__ void k_gen_count(const unsigned long long* __restrict__ src, unsigned long long* dst_mapped)
+{
+  *(volatile unsigned long long*)dst_mapped = *src;
+  __threadfence_system();
+}
+
+// Buffers and streams of the host-delivery pipeline, grown on demand and kept in the handle.
+static int gen_reserve(cp_handle* h, uint64_t cap, uint64_t nchunks)
+{
+  if (cap > h->gen_cap) {
+    if (h->d_gen_stage) {
+      if (h->gen_copy) CP_CUDA(h, cudaStreamSynchronize(h->gen_copy));
+      CP_CUDA(h, cudaStreamSynchronize(h->stream));
+      CP_CUDA(h, cudaFree(h->d_gen_stage));
+      h->d_gen_stage = nullptr;
+      h->gen_cap = 0;
+    }
+    CP_CUDA(h, cudaMalloc(&h->d_gen_stage, sizeof(cp_event) * CP_GEN_BUFS * cap));
+    h->gen_cap = cap;
+  }
+  if (nchunks > h->gen_chunks_cap) {
+    CP_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (h->d_gen_red) { CP_CUDA(h, cudaFree(h->d_gen_red)); h->d_gen_red = nullptr; }
+    if (h->d_gen_cnt) { CP_CUDA(h, cudaFree(h->d_gen_cnt)); h->d_gen_cnt = nullptr; }
+    if (h->h_gen_cnt) { CP_CUDA(h, cudaFreeHost(h->h_gen_cnt)); h->h_gen_cnt = nullptr; }
+    h->gen_chunks_cap = 0;
+    CP_CUDA(h, cudaMalloc(&h->d_gen_red, sizeof(double) * 8 * nchunks));
+    CP_CUDA(h, cudaMalloc(&h->d_gen_cnt, sizeof(unsigned long long) * nchunks));
+    CP_CUDA(h, cudaHostAlloc(&h->h_gen_cnt, sizeof(unsigned long long) * nchunks, cudaHostAllocMapped));
+    h->gen_chunks_cap = nchunks;
+  }
+  if (!h->gen_copy) {
+    CP_CUDA(h, cudaStreamCreateWithFlags(&h->gen_copy, cudaStreamNonBlocking));
+    for (int b = 0; b < CP_GEN_BUFS; ++b) {
+      CP_CUDA(h, cudaEventCreateWithFlags(&h->gen_counted[b], cudaEventDisableTiming));
+      CP_CUDA(h, cudaEventCreateWithFlags(&h->gen_copied[b], cudaEventDisableTiming));
+    }
+  }
+  return CP_OK;
+}
+
+// Chunked production into HOST memory.  Chunk c is computed on the handle's stream into staging
+// buffer c % CP_GEN_BUFS (after that buffer's previous copy has drained); its accepted count
+// reaches the host through mapped pinned memory; the host enqueues chunk c + 1 before it waits
+// for that count, then enqueues chunk c's records on the copy stream.  The device therefore
+// never waits for the host, the copy engine only carries records, and with copies slower than
+// compute the copy stream runs back to back.  records_host should be pinned for the copies to
+// overlap.  On return every copy into records_host has finished.
 extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t chunk,
                                 cp_event* records_host, uint64_t capacity, cp_unweight_result* out)
 {
@@ -352,77 +398,63 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: no threshold");
   if (chunk > n_points) chunk = n_points;
   const uint64_t nchunks = (n_points + chunk - 1) / chunk;
-  // a chunk accepts at most every point; size the staging buffers for the chunk
-  const uint64_t stage_cap = chunk;
-  cp_event* stage[2] = {nullptr, nullptr};
-  double* red = nullptr;
-  unsigned long long* cnt = nullptr;
-  cudaStream_t copy = nullptr;
-  cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
-  std::vector<unsigned long long> hcnt(nchunks, 0);
+  // a chunk accepts at most every point: staging slots = chunk
+  int rc = gen_reserve(h, chunk, nchunks);
+  if (rc) return rc;
   std::vector<double> hred(nchunks * 8, 0.0);
-  int rc = CP_OK;
-  uint64_t written = 0;
+  uint64_t written = 0, total_acc = 0;
   cudaError_t e = cudaSuccess;
+  unsigned long long* const hcnt = h->h_gen_cnt;
+  unsigned long long* dcnt_mapped = nullptr;
+  // records of chunk j: wait for its count, copy what fits
+  auto drain = [&](uint64_t j) -> cudaError_t {
+    const int b = (int)(j % CP_GEN_BUFS);
+    cudaError_t x = cudaEventSynchronize(h->gen_counted[b]);
+    if (x != cudaSuccess) return x;
+    const unsigned long long cnt = *(volatile unsigned long long*)(hcnt + j);
+    total_acc += cnt;
+    uint64_t take = cnt < chunk ? cnt : chunk;
+    if (written + take > capacity) take = capacity > written ? capacity - written : 0;
+    if ((x = cudaStreamWaitEvent(h->gen_copy, h->gen_counted[b], 0)) != cudaSuccess) return x;
+    if (take && (x = cudaMemcpyAsync(records_host + written, h->d_gen_stage + (uint64_t)b * chunk,
+                                     sizeof(cp_event) * take, cudaMemcpyDeviceToHost, h->gen_copy)) != cudaSuccess)
+      return x;
+    written += take;
+    return cudaEventRecord(h->gen_copied[b], h->gen_copy);
+  };
   do {
-    if ((e = cudaMalloc(&stage[0], sizeof(cp_event) * stage_cap)) != cudaSuccess) break;
-    if ((e = cudaMalloc(&stage[1], sizeof(cp_event) * stage_cap)) != cudaSuccess) break;
-    if ((e = cudaMalloc(&red, sizeof(double) * 8 * nchunks)) != cudaSuccess) break;
-    if ((e = cudaMalloc(&cnt, sizeof(unsigned long long) * nchunks)) != cudaSuccess) break;
-    if ((e = cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking)) != cudaSuccess) break;
-    for (int b = 0; b < 2; ++b) {
-      if ((e = cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming)) != cudaSuccess) break;
-      if ((e = cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming)) != cudaSuccess) break;
-    }
-    if (e != cudaSuccess) break;
-    if ((e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * nchunks, h->stream)) != cudaSuccess) break;
-    for (uint64_t c = 0; c < nchunks && rc == CP_OK; ++c) {
-      const int b = (int)(c & 1);
+    if ((e = cudaHostGetDevicePointer((void**)&dcnt_mapped, hcnt, 0)) != cudaSuccess) break;
+    if ((e = cudaMemsetAsync(h->d_gen_cnt, 0, sizeof(unsigned long long) * nchunks, h->stream)) != cudaSuccess) break;
+    for (uint64_t c = 0; c < nchunks; ++c) {
+      const int b = (int)(c % CP_GEN_BUFS);
       const uint64_t p0 = c * chunk, n = (p0 + chunk <= n_points) ? chunk : n_points - p0;
-      if (c >= 2 && (e = cudaStreamWaitEvent(h->stream, copied[b], 0)) != cudaSuccess) break;
+      if (c >= CP_GEN_BUFS && (e = cudaStreamWaitEvent(h->stream, h->gen_copied[b], 0)) != cudaSuccess) break;
       unsigned long long* saved = h->d_counter;
-      h->d_counter = cnt + c;
-      rc = unweight_enqueue(h, p0, n, iter, stage[b], stage_cap, red + 8 * c);
+      h->d_counter = h->d_gen_cnt + c;
+      rc = unweight_enqueue(h, p0, n, iter, h->d_gen_stage + (uint64_t)b * chunk, chunk, h->d_gen_red + 8 * c);
       h->d_counter = saved;
       if (rc) break;
-      if ((e = cudaEventRecord(done[b], h->stream)) != cudaSuccess) break;
-      // the host needs this chunk's count to place its records
-      if ((e = cudaMemcpyAsync(&hcnt[c], cnt + c, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                               h->stream)) != cudaSuccess) break;
-      if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) break;
-      uint64_t take = hcnt[c] < stage_cap ? hcnt[c] : stage_cap;
-      if (written + take > capacity) take = capacity > written ? capacity - written : 0;
-      if ((e = cudaStreamWaitEvent(copy, done[b], 0)) != cudaSuccess) break;
-      if (take && (e = cudaMemcpyAsync(records_host + written, stage[b], sizeof(cp_event) * take,
-                                       cudaMemcpyDeviceToHost, copy)) != cudaSuccess) break;
-      if ((e = cudaEventRecord(copied[b], copy)) != cudaSuccess) break;
-      written += take;
+      k_gen_count<<<1, 1, 0, h->stream>>>(h->d_gen_cnt + c, dcnt_mapped + c);
+      if ((e = cudaGetLastError()) != cudaSuccess) break;
+      if ((e = cudaEventRecord(h->gen_counted[b], h->stream)) != cudaSuccess) break;
+      if (c >= 1 && (e = drain(c - 1)) != cudaSuccess) break;
     }
     if (e != cudaSuccess || rc) break;
-    if ((e = cudaStreamSynchronize(copy)) != cudaSuccess) break;
-    if ((e = cudaMemcpyAsync(hred.data(), red, sizeof(double) * 8 * nchunks, cudaMemcpyDeviceToHost,
+    if ((e = drain(nchunks - 1)) != cudaSuccess) break;
+    if ((e = cudaMemcpyAsync(hred.data(), h->d_gen_red, sizeof(double) * 8 * nchunks, cudaMemcpyDeviceToHost,
                              h->stream)) != cudaSuccess) break;
-    e = cudaStreamSynchronize(h->stream);
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) break;
+    e = cudaStreamSynchronize(h->gen_copy);
   } while (0);
-  if (copy) cudaStreamSynchronize(copy);
-  for (int b = 0; b < 2; ++b) {
-    if (done[b]) cudaEventDestroy(done[b]);
-    if (copied[b]) cudaEventDestroy(copied[b]);
-  }
-  if (copy) cudaStreamDestroy(copy);
-  if (stage[0]) cudaFree(stage[0]);
-  if (stage[1]) cudaFree(stage[1]);
-  if (red) cudaFree(red);
-  if (cnt) cudaFree(cnt);
+  // no copy into records_host may outlive the call, on the error paths too
+  cudaStreamSynchronize(h->stream);
+  cudaStreamSynchronize(h->gen_copy);
   if (e != cudaSuccess) return cp_fail_cuda(h, e, "cp_generate_host");
   if (rc) return rc;
   if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  uint64_t total_acc = 0;
-  for (uint64_t c = 0; c < nchunks; ++c) {
+  for (uint64_t c = 0; c < nchunks; ++c)
     for (int k = 0; k < 8; ++k) tot[k] = (k == 2) ? (hred[8 * c + k] > tot[k] ? hred[8 * c + k] : tot[k]) : tot[k] + hred[8 * c + k];
-    total_acc += hcnt[c];
-  }
   if (out) fill_unw(tot, (double)n_points, wm[0], out);
   if (total_acc > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_generate_host: record buffer too small");
   if (tot[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");

@@ -241,7 +241,9 @@ int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_event* record
  * weights_dev = NULL switches them off; cp_generate_host does not write them. */
 int cp_set_scale_weights(cp_handle* h, float* weights_dev, uint64_t capacity);
 /* The same production pass delivering the records to HOST memory (pinned for overlap), in
- * chunks of `chunk` points whose device-to-host copies overlap the next chunk's compute. */
+ * chunks of `chunk` points whose device-to-host copies overlap the following chunks' compute
+ * (the handle keeps 3 staging buffers of `chunk` records; 2^21 points per chunk keeps the copy
+ * engine busy back to back).  Every copy has finished when the call returns. */
 int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t chunk,
                      cp_event* records_host, uint64_t capacity, cp_unweight_result* out_host);
 
