@@ -354,7 +354,7 @@ __global__ void k_sigma(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n
       float m[5];
       for (int k = 0; k < 5; ++k) m[k] = (mask >> k) & 1 ? 1.f : 0.f;
       float fa[8], fb[8];
-      cp_cteq_pair(cteq, q2f[i], logf(x1[i]), 0.f, logf(x2[i]), 0.f, fa, fb);
+      cp_cteq_pair<1>(cteq, q2f[i], logf(x1[i]), 0.f, logf(x2[i]), 0.f, fa, fb);
       v = P.conv * pref * cp_channel_sum(m, b, fa, fb);
     } else {
       float br = 0.f;
@@ -390,7 +390,7 @@ __global__ void k_pick_state(const CpHadParams P, const CpCteqPoly* cteq_g, int6
     const float tp = t / s, up = u / s;
     CpPoint pt;
     cp_brackets(P, tp, up, pt.b);
-    cp_cteq_pair(cteq, q2f[i], logf(x1[i]), 0.f, logf(x2[i]), 0.f, pt.fa, pt.fb);
+    cp_cteq_pair<1>(cteq, q2f[i], logf(x1[i]), 0.f, logf(x2[i]), 0.f, pt.fa, pt.fb);
     const float4 ri = r[i];
     int id[4];
     cp_pick_pair(P, k, pt, ri.x, ri.y, id);
@@ -409,7 +409,7 @@ __global__ void k_pdf(const CpCteqPoly* cteq_g, int64_t n, const float* __restri
        i += (int64_t)gridDim.x * blockDim.x) {
     float f[8], g[8];
     float lx = logf(x[i]);
-    cp_cteq_pair(cteq, q2[i], lx, 0.f, lx, 0.f, f, g);
+    cp_cteq_pair<1>(cteq, q2[i], lx, 0.f, lx, 0.f, f, g);
     // id order -5..-1, 1..5, 21; f = {d, u, g, ubar, dbar, s, c, b}
     float* o = out + 11 * i;
     o[0] = f[7]; o[1] = f[6]; o[2] = f[5]; o[3] = f[3]; o[4] = f[4];

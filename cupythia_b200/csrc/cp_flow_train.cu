@@ -28,6 +28,7 @@ struct FlowTrainBufs {
   uint16_t* DO;        // [4][B][16]  bf16 d outputs (s_raw, t)
   double* sums;        // [2] sum w, sum w^2 of the batch
   double* loss;        // per-step relative second moment
+  float* gpart;        // [CP_WG_MAXBLK][CP_FLOW_NPARAM] per-block weight and bias gradients
 };
 
 __device__ __forceinline__ float cp_bf_lo(uint32_t v) { return __uint_as_float(v << 16); }
@@ -338,9 +339,11 @@ __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g
 
 // ------------------------------------------------------------------------------------------
 // 4. weight and bias gradients of one layer shape for all couplings (blockIdx.y = coupling):
-//    G[M][N] += sum_p A[p][0:M]^T B[p][0:N] on the tensor cores, and the bias gradient
-//    Gb[N] += sum_p B[p][0:N] from the same staged tiles
-//    (A, B bf16 row-major with leading dims M and N; M in {16, 64}, N in {16, 64})
+//    block b's chunk of points gives G_b[M][N] = sum_p A[p][0:M]^T B[p][0:N] on the tensor cores
+//    and the bias gradient Gb_b[N] = sum_p B[p][0:N] from the same staged tiles, stored into its
+//    own slot of the partial buffer (A, B bf16 row-major with leading dims M and N; M in {16, 64},
+//    N in {16, 64}); k_flow_gsum then adds the slots in block order, so a training run is
+//    reproducible bit for bit (no floating-point atomics).
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ void cp_ldsm_x4_t(uint32_t r[4], const void* p)
 {
@@ -350,19 +353,21 @@ __device__ __forceinline__ void cp_ldsm_x4_t(uint32_t r[4], const void* p)
 }
 
 #define CP_WG_ROWS 64   // points staged per iteration
+#define CP_WG_MAXBLK 64 // blocks per coupling and layer (the batch is cut into at most this many chunks)
 
 template <int M, int N>
 __global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__ A0, const uint16_t* __restrict__ B0,
-                                                    uint64_t n, float* __restrict__ G0, int ldg, int nvalid, int chunk,
-                                                    int bias_rel)
+                                                    uint64_t n, float* __restrict__ part, int goff, int ldg, int nvalid,
+                                                    int chunk, int bias_rel)
 {
   constexpr int MT = M / 16, NT = N / 8, TPW = (MT * NT + 3) / 4;
   __shared__ __align__(16) uint16_t sA[CP_WG_ROWS * M];
   __shared__ __align__(16) uint16_t sB[CP_WG_ROWS * N];
+  __shared__ float sBias[128];
   const int c = blockIdx.y;
   const uint16_t* A = A0 + (uint64_t)c * n * M;
   const uint16_t* B = B0 + (uint64_t)c * n * N;
-  float* G = G0 + c * CP_FLOW_PER;
+  float* G = part + (size_t)blockIdx.x * CP_FLOW_NPARAM + c * CP_FLOW_PER + goff;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
   const int mi = lane >> 3, rw = lane & 7;
   float acc[TPW][4];
@@ -417,10 +422,27 @@ __global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__
     if (t >= MT * NT) continue;
     const int mt = t / NT, nt = t % NT;
     const int m0 = mt * 16 + gid, n0 = nt * 8 + 2 * tig;
-    if (n0 < nvalid) { atomicAdd(&G[m0 * ldg + n0], acc[j][0]); atomicAdd(&G[(m0 + 8) * ldg + n0], acc[j][2]); }
-    if (n0 + 1 < nvalid) { atomicAdd(&G[m0 * ldg + n0 + 1], acc[j][1]); atomicAdd(&G[(m0 + 8) * ldg + n0 + 1], acc[j][3]); }
+    if (n0 < nvalid) { G[m0 * ldg + n0] = acc[j][0]; G[(m0 + 8) * ldg + n0] = acc[j][2]; }
+    if (n0 + 1 < nvalid) { G[m0 * ldg + n0 + 1] = acc[j][1]; G[(m0 + 8) * ldg + n0 + 1] = acc[j][3]; }
   }
-  if (bcol < nvalid) atomicAdd(&G[bias_rel + bcol], bsum);
+  // the 128 / N threads of a bias column add their row sums in thread order
+  sBias[threadIdx.x] = bsum;
+  __syncthreads();
+  if (threadIdx.x < N && threadIdx.x < nvalid) {
+    float b = 0.f;
+    for (int r = 0; r < 128 / N; ++r) b += sBias[r * N + threadIdx.x];
+    G[bias_rel + threadIdx.x] = b;
+  }
+}
+
+// G[i] += sum over the nblk block slots of the partial gradients, in block order
+__global__ void k_flow_gsum(const float* __restrict__ part, int nblk, float* __restrict__ G)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= CP_FLOW_NPARAM) return;
+  float s = 0.f;
+  for (int b = 0; b < nblk; ++b) s += part[(size_t)b * CP_FLOW_NPARAM + i];
+  G[i] += s;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -472,7 +494,8 @@ struct FlowTrainMem {
 
 static size_t train_bytes(uint64_t B)
 {
-  return B * (sizeof(float) * 12 + sizeof(float4) * 2 + 2 * CP_FLOW_NC * (16 + 64 * 4 + 16)) + 4096;
+  return B * (sizeof(float) * 12 + sizeof(float4) * 2 + 2 * CP_FLOW_NC * (16 + 64 * 4 + 16)) + 4096 +
+         sizeof(float) * CP_WG_MAXBLK * CP_FLOW_NPARAM;
 }
 
 static FlowTrainBufs carve(void* base, uint64_t B)
@@ -490,7 +513,8 @@ static FlowTrainBufs carve(void* base, uint64_t B)
   t.DO = reinterpret_cast<uint16_t*>(q); q += 2 * CP_FLOW_NC * 16 * B;
   q = reinterpret_cast<char*>(((uintptr_t)q + 255) & ~(uintptr_t)255);
   t.sums = reinterpret_cast<double*>(q); q += 64;
-  t.loss = reinterpret_cast<double*>(q);
+  t.loss = reinterpret_cast<double*>(q); q += 64;
+  t.gpart = reinterpret_cast<float*>(q);
   return t;
 }
 
@@ -515,17 +539,22 @@ static int flow_train_step(cp_handle* h, const FlowTrainBufs& t, uint64_t B, uin
   k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, B, t.zs, t.vj, t.wg, t.sums, t);
   CP_LAUNCH_CHECK(h, "k_flow_bwd");
   float* G = h->d_flow + CP_FLOW_NPARAM;
-  // about 64 blocks per coupling and layer; chunks are whole multiples of the staged rows
-  const uint64_t chunk = ((B + 63) / 64 + CP_WG_ROWS - 1) / CP_WG_ROWS * CP_WG_ROWS;
-  const dim3 grid((unsigned)((B + chunk - 1) / chunk), CP_FLOW_NC);
-  k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, B, G + CP_FLOW_W1, 64, 64, (int)chunk,
+  // at most CP_WG_MAXBLK blocks per coupling and layer; chunks are whole multiples of the staged
+  // rows.  The three launches share the grid, so together they write every entry of the
+  // partial slots 0 .. nblk-1 (all of W1, b1, W2, b2, W3, b3 of every coupling).
+  const uint64_t chunk = ((B + CP_WG_MAXBLK - 1) / CP_WG_MAXBLK + CP_WG_ROWS - 1) / CP_WG_ROWS * CP_WG_ROWS;
+  const int nblk = (int)((B + chunk - 1) / chunk);
+  const dim3 grid((unsigned)nblk, CP_FLOW_NC);
+  k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, B, t.gpart, CP_FLOW_W1, 64, 64, (int)chunk,
                                                     CP_FLOW_B1 - CP_FLOW_W1);
-  k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, B, G + CP_FLOW_W2, 64, 64, (int)chunk,
+  k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, B, t.gpart, CP_FLOW_W2, 64, 64, (int)chunk,
                                                     CP_FLOW_B2 - CP_FLOW_W2);
   // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
-  k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, B, G + CP_FLOW_W3, 8, 8, (int)chunk,
+  k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, B, t.gpart, CP_FLOW_W3, 8, 8, (int)chunk,
                                                     CP_FLOW_B3 - CP_FLOW_W3);
   CP_LAUNCH_CHECK(h, "k_flow_wgrad");
+  k_flow_gsum<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(t.gpart, nblk, G);
+  CP_LAUNCH_CHECK(h, "k_flow_gsum");
   return CP_OK;
 }
 

@@ -101,6 +101,10 @@ static inline int cp_build_had_params(const CpHadConfig& c, CpHadParams& P)
     q.ut1 = (float)UT1[i];
     q.eut2 = (float)exp(UT2[i]);
     q.useX1L = UT2[i] < -100.0 ? 1 : 0;
+    // the kernels resolve these two cases per parametrisation at compile time
+    if (q.useX1L != (cp_cteq_uses_x1l(i) ? 1 : 0) || (QMIN[i] > 0.0) != cp_cteq_has_qmin(i) ||
+        (!cp_cteq_has_qmin(i) && !(ALPHA[i] < 1.0)))
+      return 1;
   }
   double s = c.sqrtS * c.sqrtS;
   double tauMin = 4.0 * c.pTmin * c.pTmin / s;

@@ -210,7 +210,7 @@ __global__ void k_refine(double* edges, const double* red, int nb, double n, dou
 }
 
 // FP32 integrand at caller-supplied x
-__global__ void k_weight_at(const CpHadParams P, const CpCteqPoly* cteq_g, const float* __restrict__ x,
+__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_weight_at(const CpHadParams P, const CpCteqPoly* cteq_g, const float* __restrict__ x,
                             int64_t n, float* w)
 {
   __shared__ CpCteqPoly sCteq[8];

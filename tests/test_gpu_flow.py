@@ -179,6 +179,22 @@ def test_training_lowers_the_weight_variance():
     assert abs(flow["sigma"] - base["sigma"]) < 5 * np.hypot(flow["sigma_err"], base["sigma_err"])
 
 
+def test_training_is_reproducible():
+    """Two trainings from the same initialisation on the same grid end with bit-identical
+    parameters and losses: every reduction of the training step (batch moments, weight and bias
+    gradients) sums in a fixed order."""
+    import cupythia_b200 as cp
+    runs = []
+    for _ in range(2):
+        with cp.Integrator() as it:
+            it.integrate(3, 1 << 20, alpha=1.5)
+            it.flow_init(7)
+            loss = it.flow_train(10, 65536, lr=8e-3)
+            runs.append((it.flow_params.copy(), np.asarray(loss).copy()))
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert np.array_equal(runs[0][0], runs[1][0])
+
+
 def test_expired_tensor_core_wait_is_reported_and_recoverable(integ):
     """Failure detection without a GPU fault: the test hook stops MMA issue, so the epilogue's
     bounded waits expire (about 1 s); the call must return CP_ERR_TIMEOUT (4), and the next call
