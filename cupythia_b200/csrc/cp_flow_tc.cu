@@ -338,7 +338,8 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
         cp_tc_write_in(hb[s], row, 0, t[s]);
         cp_tc_publish(pb[s]);
       }
-#pragma unroll 1
+      // unrolled: each coupling's input and transformed dimensions are compile-time constants
+#pragma unroll
       for (int c = 0; c < CP_FLOW_NC; ++c) {
 #pragma unroll
         for (int s = 0; s < 2; ++s) {           // ep1: layer-1 output -> layer 2
