@@ -56,6 +56,17 @@ class ShardedIntegrator:
         self.dist.all_reduce(t, group=self.group)
         return t.tolist()
 
+    def _gather(self, value, like):
+        """value of every rank, in rank order (one all-reduce of a one-hot vector; exact for
+        integers below 2^53)"""
+        if self.world == 1:
+            return [float(value)]
+        import torch
+        t = torch.zeros(self.world, dtype=torch.float64, device=like.device)
+        t[self.rank] = float(value)
+        self.dist.all_reduce(t, group=self.group)
+        return t.tolist()
+
     # ---------------------------------------------------------------- VEGAS
     def iteration(self, n_total, iteration=0, alpha=1.5):
         offset, count = shard(n_total, self.rank, self.world)
@@ -82,13 +93,18 @@ class ShardedIntegrator:
     # ---------------------------------------------------------------- production
     def unweight(self, n_total, iteration=0, records=None):
         """Production pass over the global points [0, n_total): this rank's records (device) and
-        the pass statistics summed over ranks (accepted, overweight, n_bad; sigma combined)."""
+        the pass statistics summed over ranks (accepted, overweight, n_bad; sigma combined).
+        ``record_offset`` is the exclusive scan of the ranks' accepted counts, the index of this
+        rank's first record in the concatenation of all ranks' records in rank order (the global
+        record offsets of the reference's merged output); ``records_per_rank`` the counts."""
         offset, count = shard(n_total, self.rank, self.world)
         self.b.set_point_offset(offset)
         rec, st = self.b.unweight(count, iteration=iteration, records=records)
         acc, over, bad, sw, var = self._sum(
             [st["n_accepted"], st["n_overweight"], st["n_bad"], st["sigma"] * count,
              (st["sigma_err"] * count) ** 2], like=rec)
+        per_rank = [int(c) for c in self._gather(st["n_accepted"], like=rec)]
         glob = dict(st, n_points=n_total, n_accepted=int(acc), n_overweight=int(over), n_bad=int(bad),
-                    sigma=sw / n_total, sigma_err=math.sqrt(var) / n_total, eta=acc / n_total)
+                    sigma=sw / n_total, sigma_err=math.sqrt(var) / n_total, eta=acc / n_total,
+                    record_offset=sum(per_rank[:self.rank]), records_per_rank=per_rank)
         return rec, st, glob

@@ -98,3 +98,58 @@ def test_two_gloo_ranks_equal_one_process():
         assert np.allclose(grid, ref_grid, rtol=0, atol=1e-12)
         assert np.allclose(sig, ref_sig, rtol=1e-12)
     assert np.array_equal(res[0][0], res[1][0])   # both ranks hold the same grid
+
+
+class CountingBackend:
+    """Production surface only: a rank's pass over count points accepts count // 3 + offset % 5
+    of them (any deterministic, rank-dependent number does)."""
+
+    def __init__(self):
+        self.offset = 0
+
+    def set_point_offset(self, offset):
+        self.offset = offset
+
+    def unweight(self, count, iteration=0, records=None):
+        k = count // 3 + self.offset % 5
+        return torch.zeros((k, 64), dtype=torch.uint8), {
+            "n_accepted": k, "n_overweight": 1, "n_bad": 0, "sigma": 0.75, "sigma_err": 0.01, "eta": k / count}
+
+
+def _unweight_rank_main(rank, world, port, n_total, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        rec, st, glob = ShardedIntegrator(CountingBackend()).unweight(n_total, iteration=5)
+        out[rank] = (len(rec), glob["record_offset"], glob["records_per_rank"], glob["n_accepted"],
+                     glob["n_overweight"])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_record_offsets_are_the_exclusive_scan_of_accepted_counts():
+    n_total, world = 1000003, 3
+    expect = []
+    for r in range(world):
+        off, cnt = shard(n_total, r, world)
+        expect.append(cnt // 3 + off % 5)
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_unweight_rank_main, args=(r, world, port, n_total, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+        assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+        res = dict(out)
+    for r in range(world):
+        n_rec, rec_off, per_rank, n_acc, n_over = res[r]
+        assert n_rec == expect[r]
+        assert per_rank == expect
+        assert rec_off == sum(expect[:r])
+        assert n_acc == sum(expect) and n_over == world
+
