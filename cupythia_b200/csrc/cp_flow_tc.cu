@@ -15,7 +15,8 @@
 //   ep3: wait for layer 3, read the 4 output columns, update the point, write the next
 //        coupling's layer-1 input, publish (its layer 1 follows)
 // and the steps of the two slots alternate, so one slot's MMAs run while the other slot's
-// epilogue runs.  The biases are part of the MMAs: layer 1 has them as input columns 14 and 15
+// epilogue runs; a slot that finishes its last coupling writes its points and starts on the
+// warpgroup's next pair at once, while the other slot finishes the current one.  The biases are part of the MMAs: layer 1 has them as input columns 14 and 15
 // (constant 1) times weight rows holding the BF16 high and low parts of the FP32 bias; layers 2
 // and 3 add one K = 16 MMA of a constant block (columns 0 and 1 equal to 1) against the hi/lo
 // bias rows.  hi + lo reproduces the FP32 bias to about 2^-17 relative.
@@ -25,7 +26,8 @@
 // issues and commits to the slot's MMA barrier, which the epilogue warps wait on before reading
 // TMEM.  Every wait is bounded (about 1 s of clock without progress); on expiry the waiting side
 // raises its warpgroup's abort flag, no further MMAs are issued for it, its warps finish their
-// loops without waiting, the kernel sets *status and releases its TMEM.
+// loops without waiting, each issuing thread waits (bounded) for the MMAs it still has in flight,
+// and the kernel sets *status and releases its TMEM.
 #include "cp_flow.cuh"
 #include "cp_internal.cuh"
 #include "cp_tc.cuh"
@@ -45,11 +47,12 @@
 #define CP_TC_S_H (CP_TC_S_ONES + 4096)
 #define CP_TC_S_EDGE (CP_TC_S_H + CP_TC_WG * 2 * CP_TC_HBYTES)
 #define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
-#define CP_TC_SMEM (CP_TC_S_MISC + 256 + 1024)  // mbarriers, TMEM address, abort flags; 1024-byte base alignment slack
+#define CP_TC_SMEM (CP_TC_S_MISC + 256 + 1024)  // mbarriers, TMEM address, abort flags, final barriers; 1024-byte base alignment slack
 #define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
 #define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
 
 static_assert(CP_TC_S_H % 1024 == 0, "activation buffers must stay aligned");
+static_assert(CP_TC_PER % 16 == 0 && CP_TC_SMEM < (1 << 18), "descriptor offsets are added to the 14-bit address field");
 static_assert(CP_TC_SMEM <= 227 * 1024, "shared memory budget");
 
 constexpr uint32_t CP_TC_IDESC64 = cp_tc_idesc_bf16(64);
@@ -156,25 +159,28 @@ __device__ __forceinline__ void cp_tc_write_in(uint32_t hbuf, int row, int c, co
   cp_sts128(hbuf + 2048 + row * 16, 0u, 0u, 0u, CP_TC_ONE2);
 }
 
-__device__ __forceinline__ void cp_tc_issue_l1(uint32_t d, uint32_t hbuf, uint32_t w)
+// Descriptors are formed once per issuing thread: a = the slot's activation buffer (LBO 2048),
+// ones = the constant block, b64 / b16 = the weight image base with the LBO of the N = 64 and
+// N = 16 operands; an operand at byte offset o from a base adds o >> 4 to the start-address field
+// (every shared address here is below 2^18, so the 14-bit field never carries).  bw = the
+// coupling's image offset >> 4.
+__device__ __forceinline__ void cp_tc_issue_l1(uint32_t d, uint64_t a, uint64_t b64, uint32_t bw)
 {
-  cp_tc_mma(d, cp_tc_desc(hbuf, 2048, 128), cp_tc_desc(w + CP_TC_B1, 1024, 128), CP_TC_IDESC64, 0u);
+  cp_tc_mma(d, a, b64 + bw + (CP_TC_B1 >> 4), CP_TC_IDESC64, 0u);
 }
-__device__ __forceinline__ void cp_tc_issue_l2(uint32_t d, uint32_t hbuf, uint32_t ones, uint32_t w)
+__device__ __forceinline__ void cp_tc_issue_l2(uint32_t d, uint64_t a, uint64_t ones, uint64_t b64, uint32_t bw)
 {
 #pragma unroll
   for (int j = 0; j < 4; ++j)
-    cp_tc_mma(d, cp_tc_desc(hbuf + j * 4096, 2048, 128), cp_tc_desc(w + CP_TC_B2 + j * 2048, 1024, 128), CP_TC_IDESC64,
-              j > 0 ? 1u : 0u);
-  cp_tc_mma(d, cp_tc_desc(ones, 2048, 128), cp_tc_desc(w + CP_TC_B2B, 1024, 128), CP_TC_IDESC64, 1u);
+    cp_tc_mma(d, a + j * (4096 >> 4), b64 + bw + ((CP_TC_B2 + j * 2048) >> 4), CP_TC_IDESC64, j > 0 ? 1u : 0u);
+  cp_tc_mma(d, ones, b64 + bw + (CP_TC_B2B >> 4), CP_TC_IDESC64, 1u);
 }
-__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint32_t hbuf, uint32_t ones, uint32_t w)
+__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint64_t a, uint64_t ones, uint64_t b16, uint32_t bw)
 {
 #pragma unroll
   for (int j = 0; j < 4; ++j)
-    cp_tc_mma(d, cp_tc_desc(hbuf + j * 4096, 2048, 128), cp_tc_desc(w + CP_TC_B3 + j * 512, 256, 128), CP_TC_IDESC16,
-              j > 0 ? 1u : 0u);
-  cp_tc_mma(d, cp_tc_desc(ones, 2048, 128), cp_tc_desc(w + CP_TC_B3B, 256, 128), CP_TC_IDESC16, 1u);
+    cp_tc_mma(d, a + j * (4096 >> 4), b16 + bw + ((CP_TC_B3 + j * 512) >> 4), CP_TC_IDESC16, j > 0 ? 1u : 0u);
+  cp_tc_mma(d, ones, b16 + bw + (CP_TC_B3B >> 4), CP_TC_IDESC16, 1u);
 }
 
 // makes this warp's shared-memory writes (and its earlier TMEM reads) visible to the tensor core
@@ -230,6 +236,7 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC);   // [0, 8) MMA done, [8, 16) publish
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + CP_TC_S_MISC + 128);
   int* abort_flags = reinterpret_cast<int*>(sm + CP_TC_S_MISC + 144);
+  uint64_t* fin_bar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC + 160);   // [4] issuers' final commits
 
   const int tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, row = tid & 127;
 
@@ -247,6 +254,7 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
       cp_mbar_init(cp_smem_u32(&mbar[i]), 1);
       cp_mbar_init(cp_smem_u32(&mbar[2 * CP_TC_WG + i]), 4);
     }
+    for (int i = 0; i < CP_TC_WG; ++i) cp_mbar_init(cp_smem_u32(&fin_bar[i]), 1);
     cp_mbar_init_fence();
   }
   if (warp == 0) {
@@ -268,12 +276,16 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
     if ((tid & 31) == 0 && !stall) {     // stall: test hook, no MMA is ever issued
       const uint64_t q0 = (uint64_t)blockIdx.x * CP_TC_WG + g;
       const uint64_t cnt = q0 < npairs ? (npairs - q0 + stride - 1) / stride : 0;
-      uint32_t rem0 = (uint32_t)(3 * CP_FLOW_NC * cnt), rem1 = rem0, pos0 = 0, pos1 = 0, pph0 = 0, pph1 = 0;
+      uint32_t rem0 = (uint32_t)(3 * CP_FLOW_NC * cnt), rem1 = rem0, pph0 = 0, pph1 = 0;
+      uint32_t lay0 = 0, lay1 = 0, bw0 = 0, bw1 = 0;   // layer and coupling image offset >> 4 per slot
       const uint32_t pub0 = cp_smem_u32(&mbar[2 * CP_TC_WG + 2 * g]), pub1 = pub0 + 8;
       const uint32_t hb0 = sbase + CP_TC_S_H + (2 * g) * CP_TC_HBYTES, hb1 = hb0 + CP_TC_HBYTES;
       const uint32_t tc0 = tmem + (uint32_t)(2 * g * 64), tc1 = tc0 + 64;
       const uint32_t done0 = cp_smem_u32(&mbar[2 * g]), done1 = done0 + 8;
       volatile int* abort = abort_flags + g;
+      const uint64_t ad0 = cp_tc_desc(hb0, 2048, 128), ad1 = cp_tc_desc(hb1, 2048, 128);
+      const uint64_t adones = cp_tc_desc(ones, 2048, 128);
+      const uint64_t b64 = cp_tc_desc(sbase, 1024, 128), b16 = cp_tc_desc(sbase, 256, 128);
       long long t0 = clock64();
       while (rem0 | rem1) {
         if (*abort) break;
@@ -281,18 +293,26 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
           uint32_t& rem = s ? rem1 : rem0;
-          uint32_t& pos = s ? pos1 : pos0;
+          uint32_t& lay = s ? lay1 : lay0;
+          uint32_t& bw = s ? bw1 : bw0;
           uint32_t& pph = s ? pph1 : pph0;
           if (!rem || !cp_mbar_test(s ? pub1 : pub0, pph)) continue;
           pph ^= 1u;
           cp_tc_fence_after();
-          const uint32_t hb = s ? hb1 : hb0, tc = s ? tc1 : tc0;
-          const uint32_t w = sbase + (pos / 3) * CP_TC_PER, layer = pos % 3;
-          if (layer == 0) cp_tc_issue_l1(tc, hb, w);
-          else if (layer == 1) cp_tc_issue_l2(tc, hb, ones, w);
-          else cp_tc_issue_l3(tc, hb, ones, w);
+          const uint32_t tc = s ? tc1 : tc0;
+          const uint64_t ad = s ? ad1 : ad0;
+          if (lay == 0) {
+            cp_tc_issue_l1(tc, ad, b64, bw);
+            lay = 1;
+          } else if (lay == 1) {
+            cp_tc_issue_l2(tc, ad, adones, b64, bw);
+            lay = 2;
+          } else {
+            cp_tc_issue_l3(tc, ad, adones, b16, bw);
+            lay = 0;
+            bw = bw == (CP_FLOW_NC - 1) * (CP_TC_PER >> 4) ? 0u : bw + (CP_TC_PER >> 4);
+          }
           cp_tc_commit(s ? done1 : done0);
-          pos = pos == 3 * CP_FLOW_NC - 1 ? 0u : pos + 1;
           --rem;
           progress = true;
         }
@@ -303,6 +323,12 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
           break;
         }
       }
+      // After an abort MMAs may still be in flight: every one this thread issued has completed
+      // (bounded wait) before the CTA releases its TMEM.
+      const uint32_t fin = cp_smem_u32(&fin_bar[g]);
+      cp_tc_commit(fin);
+      volatile int fin_abort = 0;
+      if (!cp_mbar_wait_bounded(fin, 0u, &fin_abort)) *abort = 1;
     }
     __syncwarp();
   } else {
@@ -318,26 +344,32 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
       mb[s] = cp_smem_u32(&mbar[wg * 2 + s]);
       pb[s] = cp_smem_u32(&mbar[2 * CP_TC_WG + wg * 2 + s]);
     }
-    for (uint64_t q = (uint64_t)blockIdx.x * CP_TC_WG + wg; q < npairs; q += stride) {
-      CpTcPoint t[2];
-      uint64_t p[2];
+    CpTcPoint t[2];
+    uint64_t p[2];
+    // a slot's start on the pair qq: Philox words -> VEGAS map -> logit, layer-1 input, publish
+    auto start = [&](int s, uint64_t qq) {
+      p[s] = qq * 256 + s * 128 + row;
+      uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
+      if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
+      float jv = 1.f, ld = 0.f, z[3];
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        p[s] = q * 256 + s * 128 + row;
-        uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
-        if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
-        float jv = 1.f, ld = 0.f, z[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          int bin;
-          const float xv = cp_flow_vegas_in(sEdge + d * CP_MAX_BINS, nb, w[d], jv, bin);
-          ld += cp_tc_logit(xv, z[d]);
-        }
-        t[s].z0 = z[0]; t[s].z1 = z[1]; t[s].z2 = z[2];
-        t[s].ld = ld + __logf(jv);
-        cp_tc_write_in(hb[s], row, 0, t[s]);
-        cp_tc_publish(pb[s]);
+      for (int d = 0; d < 3; ++d) {
+        int bin;
+        const float xv = cp_flow_vegas_in(sEdge + d * CP_MAX_BINS, nb, w[d], jv, bin);
+        ld += cp_tc_logit(xv, z[d]);
       }
+      t[s].z0 = z[0]; t[s].z1 = z[1]; t[s].z2 = z[2];
+      t[s].ld = ld + __logf(jv);
+      cp_tc_write_in(hb[s], row, 0, t[s]);
+      cp_tc_publish(pb[s]);
+    };
+    uint64_t q = (uint64_t)blockIdx.x * CP_TC_WG + wg;
+    if (q < npairs) {
+      start(0, q);
+      start(1, q);
+    }
+    for (; q < npairs; q += stride) {
+      const uint64_t qn = q + stride;
       // unrolled: each coupling's input and transformed dimensions are compile-time constants
 #pragma unroll
       for (int c = 0; c < CP_FLOW_NC; ++c) {
@@ -373,17 +405,18 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
           if (c + 1 < CP_FLOW_NC) {
             cp_tc_write_in(hb[s], row, c + 1, t[s]);
             cp_tc_publish(pb[s]);
+          } else {
+            // the slot's points are done: output, then the slot starts on the next pair while the
+            // other slot finishes this one
+            float v0, v1, v2;
+            float ld = t[s].ld;
+            ld += cp_tc_sigmoid(t[s].z0, v0);
+            ld += cp_tc_sigmoid(t[s].z1, v1);
+            ld += cp_tc_sigmoid(t[s].z2, v2);
+            if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+            if (qn < npairs) start(s, qn);
           }
         }
-      }
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        float v0, v1, v2;
-        float ld = t[s].ld;
-        ld += cp_tc_sigmoid(t[s].z0, v0);
-        ld += cp_tc_sigmoid(t[s].z1, v1);
-        ld += cp_tc_sigmoid(t[s].z2, v2);
-        if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
       }
       if (cp_bar_wg_or(bar_id, *abort != 0)) break;
     }
