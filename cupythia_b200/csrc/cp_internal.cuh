@@ -68,6 +68,7 @@ struct cp_handle {
   // launch shapes (resident blocks per SM on this handle's device; -1 until first use)
   int had_blocks = 0;
   int adj_per_sm = -1, flow_per_sm = -1, unw_per_sm = -1;
+  int build_per_sm[2] = {-1, -1};   // record builder without / with scale weights
   // weight histogram of the last iteration and the unweighting threshold (device)
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q

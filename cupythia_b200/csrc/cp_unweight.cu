@@ -163,8 +163,9 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
 // K2: dense pass over the reserved slots: re-evaluate the accepted point's kinematics (its PDFs
 // come from K1's per-slot copy), pick process, flavours and colour flow, build the lab-frame
 // kinematics, store the full 64-byte record.
+// 4 resident blocks per SM without scale weights (64 registers), 2 with them
 template <bool SCALEW>
-__global__ void __launch_bounds__(CP_THREADS) k_unw_build(const CpHadParams P, const UnwLaunch L)
+__global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const CpHadParams P, const UnwLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
   __shared__ CpCteqPoly sCteq[8];
@@ -221,6 +222,20 @@ static int unw_blocks(cp_handle* h)
   return h->num_sms * h->unw_per_sm;
 }
 
+// The record builder loops grid-stride over the records: its grid is exactly the blocks that
+// are resident at once, so no second wave runs after the first.
+static int build_blocks(cp_handle* h, bool scalew)
+{
+  int& c = h->build_per_sm[scalew ? 1 : 0];
+  if (c < 0) {
+    int per_sm = 1;
+    const cudaError_t e = scalew ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unw_build<true>, CP_THREADS, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unw_build<false>, CP_THREADS, 0);
+    c = (e != cudaSuccess || per_sm < 1) ? 1 : per_sm;
+  }
+  return h->num_sms * c;
+}
+
 // Enqueue one production pass on h->stream (no host synchronisation).
 static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, cp_event* out,
                             uint64_t capacity, double* red_dst, float* scalew = nullptr)
@@ -266,8 +281,8 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
   if (capacity) {
-    if (L.scalew) k_unw_build<true><<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
-    else k_unw_build<false><<<h->num_sms * 4, CP_THREADS, 0, h->stream>>>(h->P, L);
+    if (L.scalew) k_unw_build<true><<<build_blocks(h, true), CP_THREADS, 0, h->stream>>>(h->P, L);
+    else k_unw_build<false><<<build_blocks(h, false), CP_THREADS, 0, h->stream>>>(h->P, L);
     CP_LAUNCH_CHECK(h, "k_unw_build");
   }
   if (h->timing) {
