@@ -110,3 +110,53 @@ def test_tiny_passes_and_size_limits(integ):
     integ.flow_init(7)
     out = integ.flow_sample(11, 1, 3, 0).cpu().numpy()
     assert np.all(np.isfinite(out)) and np.all((out[0, :3] > 0) & (out[0, :3] < 1))
+
+
+def test_host_generation_capacity_and_staging_reuse():
+    """The host-delivery call (three staging buffers kept in the handle, counts through mapped
+    pinned memory): with a record buffer smaller than the accepted count it fills the buffer with
+    real records and reports CP_ERR_CAPACITY; afterwards the handle still works, and calls that
+    grow and then shrink the chunk, with VEGAS and with the flow as proposal, deliver exactly the
+    device pass's records."""
+    import ctypes as C
+
+    import torch
+
+    import cupythia_b200 as cp
+    n = 200003
+    with cp.Integrator() as it:
+        it.integrate(4, 1 << 20, alpha=1.5)
+        it.iteration(1 << 20, 50, alpha=0.0)
+        it.weight_quantile(0.999)
+        rec, st = it.unweight(n, iteration=51)
+        dev = cp.events_view(rec)
+        by_point = {int(e["point"]): e.tobytes() for e in dev}
+        k = st["n_accepted"]
+        small = torch.zeros((k // 3, 64), dtype=torch.uint8, pin_memory=True)
+        res = cp._lib.cp_unweight_result()
+        rc = it.lib.cp_generate_host(it.h, n, 51, 1 << 14, C.c_void_p(small.data_ptr()), small.shape[0], C.byref(res))
+        assert rc == cp._lib.CP_ERR_CAPACITY and res.n_accepted == k
+        got = cp.events_view(small)
+        assert len(np.unique(got["point"])) == len(got)
+        assert all(by_point[int(e["point"])] == e.tobytes() for e in got)
+        full = torch.empty((k + 8, 64), dtype=torch.uint8, pin_memory=True)
+        for chunk in (1 << 17, 1 << 12, 100001):
+            full.zero_()
+            st2 = it.generate_host(n, full, iteration=51, chunk=chunk)
+            assert st2["n_accepted"] == k
+            h = cp.events_view(full[:k])
+            assert dev[np.argsort(dev["point"])].tobytes() == h[np.argsort(h["point"])].tobytes(), chunk
+        # the flow as proposal: its forward pass runs per chunk on the same handle
+        it.flow_init(7)
+        it.flow_train(10, 65536, lr=8e-3)
+        it.flow_enable(True)
+        it.iteration(1 << 20, 52, alpha=0.0)
+        it.weight_quantile(0.999)
+        rec_f, st_f = it.unweight(n, iteration=53)
+        host_f = torch.empty((st_f["n_accepted"] + 8, 64), dtype=torch.uint8, pin_memory=True)
+        st3 = it.generate_host(n, host_f, iteration=53, chunk=50000)
+        it.flow_enable(False)
+    assert st3["n_accepted"] == st_f["n_accepted"]
+    a = cp.events_view(rec_f)
+    b = cp.events_view(host_f[:st3["n_accepted"]])
+    assert a[np.argsort(a["point"])].tobytes() == b[np.argsort(b["point"])].tobytes()
