@@ -102,14 +102,6 @@ CP_HD void cp_twosum(float a, float b, float& s, float& e)
   float bp = s - a;
   e = (a - (s - bp)) + (b - bp);
 }
-// (s, c) += v, with the rounding error of the addition kept in c
-CP_HD void cp_acc2(float& s, float& c, float v)
-{
-  float t, e;
-  cp_twosum(s, v, t, e);
-  s = t;
-  c += e;
-}
 
 // Two-lane FP32 arithmetic for the two beams: on sm_100 one packed instruction (FADD2 / FMUL2 /
 // FFMA2) does both lanes, each lane rounded exactly like the scalar operation; on the host, two
@@ -199,42 +191,12 @@ CP_HD CpCteqQ cp_cteq_coef(const CpCteqPoly& c, float lnQ, float Q, float invQ, 
   return q;
 }
 
-// "answer" of xfUpdate (PartonDistributions.cc:1031-1046) for one parametrisation and beam:
-// x exp(exponent) (1 - Qmin/Q), with
+// "answer" of xfUpdate (PartonDistributions.cc:1031-1046) for one parametrisation, for both
+// beams at once (lane x: beam A, lane y: beam B): x exp(exponent) (1 - Qmin/Q), with
 //   exponent = A + B x + C u + af1 (y^p - 1) U + part3 + ut1 ln(1-x) + af2 L,  C = af1 af8,
 // summed with the products' FMA residuals and the additions' TwoSum errors kept in a second
-// float, and exp(hi + lo) = exp(hi) (1 + lo).
-CP_HD float cp_cteq_answer(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX& b)
-{
-  // y^p - 1 with the rounding residual of p ln y carried into first order
-  float ah = a.p * b.lny;
-  float al = cp_fmaf(a.p, b.lny, -ah);
-  float ym1 = cp_expm1f(ah);
-  ym1 = cp_fmaf(1.f + ym1, al, ym1);
-  float U = cp_fmaf(a.af8, b.uh, 1.f);
-  float part3 = b.x * b.omx * (a.af5 + a.af6 * b.omx + a.af7 * b.x * b.omx);
-  float L = c.useX1L ? b.x1L : cp_logf(b.omx + c.eut2);
-  float Ch = a.af1 * a.af8, Cl = cp_fmaf(a.af1, a.af8, -Ch);
-  float t3 = Ch * b.uh, t3l = cp_fmaf(Ch, b.uh, -t3) + Ch * b.ul + Cl * b.uh;
-  float qv = a.af1 * ym1;
-  float t4 = qv * U, t4l = cp_fmaf(qv, U, -t4);
-  float t2 = a.B * b.x, t2l = cp_fmaf(a.B, b.x, -t2);
-  float t6 = c.ut1 * b.x1L, t6l = cp_fmaf(c.ut1, b.x1L, -t6);
-  float t7 = a.af2 * L, t7l = cp_fmaf(a.af2, L, -t7);
-  float eh = a.A, el = (t2l + t3l) + (t4l + t6l + t7l);
-  cp_acc2(eh, el, t3);
-  cp_acc2(eh, el, t4);
-  cp_acc2(eh, el, t2);
-  cp_acc2(eh, el, part3);
-  cp_acc2(eh, el, t6);
-  cp_acc2(eh, el, t7);
-  float ex = cp_expf(eh);
-  return b.x * cp_fmaf(ex, el, ex) * a.qfac;
-}
-
-// The same answer for both beams at once (lane x: beam A, lane y: beam B): every product, FMA
-// residual and TwoSum of cp_cteq_answer in two-lane arithmetic, the transcendentals per lane.
-// ux = cp_cteq_uses_x1l(i).
+// float, and exp(hi + lo) = exp(hi) (1 + lo).  Every product, residual and TwoSum runs in
+// two-lane arithmetic, the transcendentals per lane.  ux = cp_cteq_uses_x1l(i).
 CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX& bA, const CpBeamX& bB, bool ux)
 {
   const CpF2 lny = cp_f2(bA.lny, bB.lny), x = cp_f2(bA.x, bB.x), omx = cp_f2(bA.omx, bB.omx);
