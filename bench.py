@@ -269,10 +269,11 @@ def run_ours(a):
         # ---- flow + adjoint form: variance-gradient grid refinement (adjoint), flow trained on
         # the integrator's weights (200 x 65536 points), w_max = q99.9 through the flow
         t0 = time.perf_counter()
-        it.set_point_offset(0)           # gradient steps and training: replicated on every rank
-        ghist = it.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
+        # variance-gradient steps with their adjoint sums exchanged, then data-parallel flow
+        # training (batch moments and gradients exchanged every step)
+        ghist = si.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
         it.flow_init(7)
-        losses = it.flow_train(200, 65536, lr=8e-3)
+        losses = si.flow_train(200, 65536, lr=8e-3)
         # proposal choice (config 5): the flow only where its weight variance beats VEGAS alone
         # on the same grid at equal points, else VEGAS is the fallback
         it.flow_enable(False)
@@ -357,8 +358,9 @@ def run_ours(a):
                    "refinement, BF16 coupling flow trained 200 x 65536 points, unweighting at q99.9",
                    "points_per_step_per_gpu": n, "adapt_points": ADAPT_ITERS * ADAPT_POINTS,
                    "l2": "256 MB buffer written between timed steps; records written per step exceed L2",
-                   "parallelism": f"dp{world}: contiguous point shards per rank; adaptation sums "
-                                  "all-reduced once per iteration, production without exchange"},
+                   "parallelism": f"dp{world}: contiguous point shards per rank; VEGAS and adjoint "
+                                  "sums all-reduced once per adaptation step, flow training data-parallel "
+                                  "(moments and gradients all-reduced per step), production without exchange"},
         "sigma_mb": comb["sigma"], "sigma_err_mb": comb["sigma_err"], "step_sigma_rel_err_max": rel_err,
         "eta": float(np.mean([s_["eta"] for s_ in st_f])), "w_max": wmax_flow,
         "weighted_points_per_s": n * a.steps * world / sec_f,

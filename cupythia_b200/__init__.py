@@ -226,20 +226,28 @@ class Integrator:
     def adapt_gradient(self, steps, n_points, lr=0.4, iteration0=0):
         """Variance-gradient adaptation: `steps` device gradient steps, halving lr whenever the
         batch variance (measured at the pre-step grid of each step) rises. Returns the history."""
-        hist = []
-        prev = None
-        for s in range(steps):
-            r = self.gradient_step(n_points, iteration=iteration0 + s, lr=lr)
-            rel = r["var"] / r["sigma"] ** 2
-            if prev is not None and rel > prev:
-                lr *= 0.5
-            prev = rel
-            hist.append({"step": s, "lr": lr, "rel_var": rel, "sigma": r["sigma"]})
-        return hist
+        return adapt_gradient_loop(self.gradient_step, steps, n_points, lr, iteration0)
 
     def gradient_step(self, n_points, iteration=0, lr=0.5):
         g = cp_grad()
         self._check(self.lib.cp_vegas_gradient_step(self.h, n_points, iteration, lr, C.byref(g)))
+        return {"sigma": g.sigma, "var": g.var}
+
+    def adjoint_accumulate(self, n_points, iteration=0, stream=0):
+        """Adjoint sums of this handle's points as a device float64 tensor (entry 8 reduces by max
+        over ranks, every other entry by sum)."""
+        torch = _torch()
+        k = C.c_int()
+        self._check(self.lib.cp_adjoint_sums_size(self.h, C.byref(k)))
+        out = torch.empty(k.value, dtype=torch.float64, device=self.device)
+        self._check(self.lib.cp_adjoint_accumulate(self.h, n_points, iteration, stream, _ptr(out)))
+        return out
+
+    def gradient_apply(self, sums, n_total, lr=0.5):
+        """Gradient record of n_total points from (rank-reduced) adjoint sums; lr > 0 also takes
+        the variance-gradient step on the grid."""
+        g = cp_grad()
+        self._check(self.lib.cp_vegas_gradient_apply(self.h, _ptr(sums), int(n_total), lr, C.byref(g)))
         return {"sigma": g.sigma, "var": g.var}
 
     # ------------------------------------------------------------------ learned proposal
@@ -275,6 +283,27 @@ class Integrator:
         loss = np.zeros(steps)
         self._check(self.lib.cp_flow_train(self.h, steps, batch, lr, loss.ctypes.data_as(C.c_void_p)))
         return loss
+
+    def flow_step_moments(self, point0, count):
+        """Phase 1 of a data-parallel training step: (sum w, sum w^2) of the batch points
+        [point0, point0 + count) as a device float64 tensor."""
+        torch = _torch()
+        out = torch.empty(2, dtype=torch.float64, device=self.device)
+        self._check(self.lib.cp_flow_step_moments(self.h, point0, count, _ptr(out)))
+        return out
+
+    def flow_step_gradient(self, moments, batch_total):
+        """Phase 2: these points' part of the batch-loss gradient (device float32 tensor) from the
+        rank-summed moments, and the batch loss."""
+        torch = _torch()
+        g = torch.empty(self.lib.cp_flow_num_params(), dtype=torch.float32, device=self.device)
+        loss = C.c_double()
+        self._check(self.lib.cp_flow_step_gradient(self.h, _ptr(moments), int(batch_total), _ptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def flow_step_update(self, grad, lr):
+        """Phase 3: Adam step with the rank-summed gradient."""
+        self._check(self.lib.cp_flow_step_update(self.h, _ptr(grad), lr))
 
     def flow_loss_grad(self, batch, iteration):
         n = self.lib.cp_flow_num_params()
@@ -349,6 +378,21 @@ class Integrator:
         self._check(self.lib.cp_partonic_weights(self.h, sqrt_shat, alphas, cmax, conv, seed,
                                                  point0, n, _ptr(w)))
         return w
+
+
+def adapt_gradient_loop(step, steps, n_points, lr, iteration0):
+    """The variance-gradient schedule over any gradient-step function step(n, iteration=, lr=)
+    (one handle, or the sharded form of cupythia_b200.distributed)."""
+    hist = []
+    prev = None
+    for s in range(steps):
+        r = step(n_points, iteration=iteration0 + s, lr=lr)
+        rel = r["var"] / r["sigma"] ** 2
+        if prev is not None and rel > prev:
+            lr *= 0.5
+        prev = rel
+        hist.append({"step": s, "lr": lr, "rel_var": rel, "sigma": r["sigma"]})
+    return hist
 
 
 EVENT_DTYPE = np.dtype([("id", "<i2", 4), ("pz_in", "<f4", 2), ("p3", "<f4", 4), ("p4", "<f4", 4),

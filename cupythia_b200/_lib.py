@@ -119,6 +119,12 @@ SIGNATURES = {
     "cp_generate_host": [_P, _u64, _u32, _u64, _P, _u64, C.POINTER(cp_unweight_result)],
     "cp_adjoint": [_P, _u64, _u32, _u32, C.POINTER(cp_grad), _P, _P],
     "cp_vegas_gradient_step": [_P, _u64, _u32, _d, C.POINTER(cp_grad)],
+    "cp_adjoint_sums_size": [_P, C.POINTER(_i)],
+    "cp_adjoint_accumulate": [_P, _u64, _u32, _u32, _P],
+    "cp_vegas_gradient_apply": [_P, _P, _u64, _d, C.POINTER(cp_grad)],
+    "cp_flow_step_moments": [_P, _u64, _u64, _P],
+    "cp_flow_step_gradient": [_P, _P, _u64, _P, _P],
+    "cp_flow_step_update": [_P, _P, _d],
     "cp_flow_num_params": [],
     "cp_flow_init": [_P, _u64],
     "cp_flow_get_params": [_P, _P, _i],

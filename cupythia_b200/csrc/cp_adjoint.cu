@@ -11,6 +11,7 @@
 // accumulated per bin (lower- and upper-edge parts, plain and w-weighted) in deterministic
 // warp-private shared-memory histograms, then FP64 block slots, then the fixed-order reduction.
 // sigma = <w>, Var = <w^2> - <w>^2, d sigma = <dw>, d Var = 2 <w dw> - 2 <w> <dw>.
+#include <vector>
 #include "cp_dual.cuh"
 #include "cp_internal.cuh"
 
@@ -193,11 +194,12 @@ __global__ void k_adjoint_finish(const double* red, int nb, double n, double* ed
   e[nb] = 1.0;
 }
 
-static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream, double lr,
-                       cp_grad* g, double* dsig_de, double* dvar_de)
+// Sums of one adjoint pass over this handle's points [offset, offset + n) into sums_out
+// (CP_ADJ_HEAD + 12 nb doubles: entry 8 is the largest weight, every other entry a sum).
+static int adjoint_accumulate(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream, double* sums_out)
 {
   CP_CHECK_HANDLE(h);
-  if (n < 2) return cp_fail(h, CP_ERR_INVALID, "cp_adjoint: n_points < 2");
+  if (n < 1) return cp_fail(h, CP_ERR_INVALID, "cp_adjoint: no points");
   const int nb = h->nb, width = CP_ADJ_HEAD + 12 * nb;
   const size_t dyn = sizeof(float) * CP_ADJ_WARPS * 12 * nb;
   // the attribute is per device: set it on every call (host-side, cheap)
@@ -211,11 +213,8 @@ static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream,
     h->adj_per_sm = per_sm;
   }
   const int blocks = h->num_sms * h->adj_per_sm;
-  const size_t out_n = 10 + 6 * (nb + 1);
-  int rc = cp_ensure_slots(h, (size_t)blocks * width + width + out_n);
+  int rc = cp_ensure_slots(h, (size_t)blocks * width);
   if (rc) return rc;
-  double* red = h->d_slots + (size_t)blocks * width;
-  double* out = red + width;
   AdjLaunch L;
   L.seed = h->cfg.seed; L.point0 = h->point_offset; L.n = n; L.iter = iter; L.stream = stream; L.nb = nb;
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.slots = h->d_slots;
@@ -229,27 +228,77 @@ static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream,
   }
   k_adjoint<<<blocks, CP_ADJ_THREADS, dyn, h->stream>>>(h->P, L);
   CP_LAUNCH_CHECK(h, "k_adjoint");
-  k_reduce_slots<0><<<(width + 7) / 8, 256, 0, h->stream>>>(h->d_slots, blocks, width, red, 8);
+  k_reduce_slots<0><<<(width + 7) / 8, 256, 0, h->stream>>>(h->d_slots, blocks, width, sums_out, 8);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
-  k_adjoint_finish<<<1, 32, 0, h->stream>>>(red, nb, (double)n, h->d_edges, lr, out);
-  CP_LAUNCH_CHECK(h, "k_adjoint_finish");
-  double* host = new double[out_n];
-  cudaError_t e = cudaMemcpyAsync(host, out, sizeof(double) * out_n, cudaMemcpyDeviceToHost, h->stream);
+  return CP_OK;
+}
+
+// Gradient record over n_total points from (rank-reduced) sums, and with lr > 0 one
+// variance-gradient step on the grid.
+static int adjoint_finish(cp_handle* h, const double* sums, double n_total, double lr, cp_grad* g,
+                          double* dsig_de, double* dvar_de)
+{
+  if (!(n_total >= 2.0)) return cp_fail(h, CP_ERR_INVALID, "cp_adjoint: n_points < 2");
+  const int nb = h->nb;
+  const size_t out_n = 10 + 6 * (nb + 1);
+  double* out = nullptr;
+  CP_CUDA(h, cudaMallocAsync(reinterpret_cast<void**>(&out), sizeof(double) * out_n, h->stream));
+  k_adjoint_finish<<<1, 32, 0, h->stream>>>(sums, nb, n_total, h->d_edges, lr, out);
+  cudaError_t e = cudaGetLastError();
+  std::vector<double> host(out_n, 0.0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), out, sizeof(double) * out_n, cudaMemcpyDeviceToHost, h->stream);
+  cudaFreeAsync(out, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  if (e != cudaSuccess) { delete[] host; return cp_fail_cuda(h, e, "cp_adjoint readback"); }
+  if (e != cudaSuccess) return cp_fail_cuda(h, e, "cp_adjoint readback");
   if (g) {
     g->sigma = host[0];
     g->var = host[1];
     for (int k = 0; k < 3; ++k) { g->dsigma[k] = host[2 + k]; g->dvar[k] = host[5 + k]; }
-    g->n_points = n;
+    g->n_points = (uint64_t)n_total;
     g->n_bad = (uint64_t)host[8];
   }
   if (dsig_de) for (int k = 0; k < 3 * (nb + 1); ++k) dsig_de[k] = host[10 + k];
   if (dvar_de) for (int k = 0; k < 3 * (nb + 1); ++k) dvar_de[k] = host[10 + 3 * (nb + 1) + k];
-  const double nbad = host[8];
-  delete[] host;
-  if (nbad > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights or gradients were zeroed");
+  if (host[8] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights or gradients were zeroed");
   return CP_OK;
+}
+
+static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream, double lr,
+                       cp_grad* g, double* dsig_de, double* dvar_de)
+{
+  CP_CHECK_HANDLE(h);
+  if (n < 2) return cp_fail(h, CP_ERR_INVALID, "cp_adjoint: n_points < 2");
+  const int width = CP_ADJ_HEAD + 12 * h->nb;
+  double* sums = nullptr;
+  CP_CUDA(h, cudaMallocAsync(reinterpret_cast<void**>(&sums), sizeof(double) * width, h->stream));
+  int rc = adjoint_accumulate(h, n, iter, stream, sums);
+  if (!rc) rc = adjoint_finish(h, sums, (double)n, lr, g, dsig_de, dvar_de);
+  cudaFreeAsync(sums, h->stream);
+  return rc;
+}
+
+extern "C" int cp_adjoint_sums_size(cp_handle* h, int* n_doubles)
+{
+  CP_CHECK_HANDLE(h);
+  if (!n_doubles) return CP_ERR_INVALID;
+  *n_doubles = CP_ADJ_HEAD + 12 * h->nb;
+  return CP_OK;
+}
+
+extern "C" int cp_adjoint_accumulate(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream,
+                                     double* sums_dev)
+{
+  CP_CHECK_HANDLE(h);
+  if (!sums_dev) return cp_fail(h, CP_ERR_INVALID, "cp_adjoint_accumulate: null sums");
+  return adjoint_accumulate(h, n_points, iter, stream, sums_dev);
+}
+
+extern "C" int cp_vegas_gradient_apply(cp_handle* h, const double* sums_dev, uint64_t n_total, double lr,
+                                       cp_grad* out)
+{
+  CP_CHECK_HANDLE(h);
+  if (!sums_dev || !(lr >= 0.0)) return cp_fail(h, CP_ERR_INVALID, "cp_vegas_gradient_apply: bad arguments");
+  return adjoint_finish(h, sums_dev, (double)n_total, lr, out, nullptr, nullptr);
 }
 
 extern "C" int cp_adjoint(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream,

@@ -39,8 +39,8 @@ __device__ __forceinline__ float cp_bf_hi(uint32_t v) { return __uint_as_float(v
 // ------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(CP_THREADS) k_flow_fwd_train(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g,
                                                                const double* __restrict__ edges, int nb,
-                                                               uint64_t seed, uint32_t iter, uint32_t stream, uint64_t n,
-                                                               float* __restrict__ zs, float4* __restrict__ vj)
+                                                               uint64_t seed, uint32_t iter, uint32_t stream, uint64_t point0,
+                                                               uint64_t n, float* __restrict__ zs, float4* __restrict__ vj)
 {
   extern __shared__ uint2 sPk[];
   float* sBias = reinterpret_cast<float*>(sPk + CP_FLOW_NC * CP_FLOW_P_FWD);
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(CP_THREADS) k_flow_fwd_train(const uint2* __re
     const bool active = p < n;
     float z[3], jv = 1.f, logdet = 0.f;
     uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
-    if (active) cp_point_words(seed, p, iter, stream, w);
+    if (active) cp_point_words(seed, point0 + p, iter, stream, w);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       int bin;
@@ -158,7 +158,7 @@ __device__ __forceinline__ void cp_store_rowfrag(uint16_t* base, int ld, uint64_
 }
 
 __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g, uint64_t n,
-                                                  const float* __restrict__ zs, const float4* __restrict__ vj,
+                                                  double n_batch, const float* __restrict__ zs, const float4* __restrict__ vj,
                                                   const float4* __restrict__ wg, const double* __restrict__ sums,
                                                   FlowTrainBufs out)
 {
@@ -168,8 +168,9 @@ __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g
   for (int j = threadIdx.x; j < CP_FLOW_NC * CP_FLOW_NB; j += blockDim.x) sBias[j] = bias_g[j];
   __syncthreads();
   const int lane = threadIdx.x & 31, gid = lane >> 2, tig = lane & 3;
-  const double sig = sums[0] / (double)n;
-  const float cnorm = (float)(2.0 / ((double)n * sig * sig));
+  // the batch's moments and size (all ranks' points when the batch is sharded)
+  const double sig = sums[0] / n_batch;
+  const float cnorm = (float)(2.0 / (n_batch * sig * sig));
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t rounds = (n + 32 * warps - 1) / (32 * warps);
   for (uint64_t r = 0; r < rounds; ++r) {
@@ -474,24 +475,28 @@ __global__ void k_flow_adam(float* __restrict__ P, float* __restrict__ G, float*
   P[i] -= lr * (m / (1.f - b1t)) / (sqrtf(v / (1.f - b2t)) + 1e-8f);
 }
 
-__global__ void k_flow_loss(const double* slots, int nblk, uint64_t n, double* sums, double* loss)
+// batch moments of this handle's points from the integrand kernel's block slots, fixed order
+__global__ void k_flow_moments(const double* slots, int nblk, double* moments)
 {
   double a = 0.0, b = 0.0;
   for (int k = 0; k < nblk; ++k) { a += slots[2 * k]; b += slots[2 * k + 1]; }
+  moments[0] = a;
+  moments[1] = b;
+}
+
+// the batch's moments (summed over ranks) for the backward pass, and its loss <w^2> / <w>^2
+__global__ void k_flow_batch_loss(const double* moments, double n, double* sums, double* loss)
+{
+  const double a = moments[0], b = moments[1];
   sums[0] = a;
   sums[1] = b;
-  const double m = a / (double)n;
-  loss[0] = (b / (double)n) / (m * m);
+  const double m = a / n;
+  loss[0] = (b / n) / (m * m);
 }
 
 // ------------------------------------------------------------------------------------------
 // host
 // ------------------------------------------------------------------------------------------
-struct FlowTrainMem {
-  void* base = nullptr;
-  uint64_t cap = 0;
-};
-
 static size_t train_bytes(uint64_t B)
 {
   return B * (sizeof(float) * 12 + sizeof(float4) * 2 + 2 * CP_FLOW_NC * (16 + 64 * 4 + 16)) + 4096 +
@@ -521,84 +526,131 @@ static FlowTrainBufs carve(void* base, uint64_t B)
 static size_t bwd_smem() { return sizeof(uint2) * CP_FLOW_NC * CP_FLOW_P_PER + sizeof(float) * CP_FLOW_NC * CP_FLOW_NB; }
 static size_t fwd_smem() { return sizeof(uint2) * CP_FLOW_NC * CP_FLOW_P_FWD + sizeof(float) * CP_FLOW_NC * CP_FLOW_NB; }
 
-// One training step over a batch of B points (counter iteration = step, Philox stream 2).
-static int flow_train_step(cp_handle* h, const FlowTrainBufs& t, uint64_t B, uint32_t step, float lr, double* loss_dev)
+// Training buffers for `count` points of a step, kept in the handle between the phases of a
+// step.  A new layout (another count) starts from zeros: columns the kernels never write (the
+// padding of the 16-wide operands) must read as zero.
+static int train_buffers(cp_handle* h, uint64_t count, FlowTrainBufs& t)
 {
-  const int nb = h->nb;
-  k_flow_fwd_train<<<h->num_sms * 2, CP_THREADS, fwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, h->d_edges, nb,
-                                                                           h->cfg.seed, step, 2, B, t.zs, t.vj);
+  if (!h->d_ftrain || count > h->ftrain_cap) {
+    if (h->d_ftrain) {
+      CP_CUDA(h, cudaStreamSynchronize(h->stream));
+      CP_CUDA(h, cudaFree(h->d_ftrain));
+      h->d_ftrain = nullptr;
+      h->ftrain_cap = 0;
+    }
+    CP_CUDA(h, cudaMalloc(&h->d_ftrain, train_bytes(count)));
+    h->ftrain_cap = count;
+    h->ftrain_count = 0;
+  }
+  if (count != h->ftrain_count) CP_CUDA(h, cudaMemsetAsync(h->d_ftrain, 0, train_bytes(count), h->stream));
+  h->ftrain_count = count;
+  t = carve(h->d_ftrain, count);
+  // per-device attributes: set on every use (host-side, cheap)
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
+  return CP_OK;
+}
+
+static void train_buffers_release(cp_handle* h)
+{
+  if (!h->d_ftrain) return;
+  cudaStreamSynchronize(h->stream);
+  cudaFree(h->d_ftrain);
+  h->d_ftrain = nullptr;
+  h->ftrain_cap = h->ftrain_count = 0;
+}
+
+// Phase 1 of a step: forward and integrand over the batch points [point0, point0 + count) at
+// counter iteration `iter` (Philox stream 2); moments[0..1] = (sum w, sum w^2) over them.
+static int flow_phase_moments(cp_handle* h, const FlowTrainBufs& t, uint64_t point0, uint64_t count, uint32_t iter,
+                              double* moments)
+{
+  k_flow_fwd_train<<<h->num_sms * 2, CP_THREADS, fwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, h->d_edges, h->nb,
+                                                                           h->cfg.seed, iter, 2, point0, count, t.zs, t.vj);
   CP_LAUNCH_CHECK(h, "k_flow_fwd_train");
   const int gblk = h->num_sms * 4;
   int rc = cp_ensure_slots(h, (size_t)2 * gblk);
   if (rc) return rc;
   const float lnTauMin = (float)log(4.0 * h->cfg.pt_hat_min * h->cfg.pt_hat_min / (h->cfg.sqrt_s * h->cfg.sqrt_s));
-  k_flow_igrad<<<gblk, 128, 0, h->stream>>>(h->P, h->d_cteq, B, lnTauMin, t.vj, t.wg, h->d_slots);
+  k_flow_igrad<<<gblk, 128, 0, h->stream>>>(h->P, h->d_cteq, count, lnTauMin, t.vj, t.wg, h->d_slots);
   CP_LAUNCH_CHECK(h, "k_flow_igrad");
-  k_flow_loss<<<1, 1, 0, h->stream>>>(h->d_slots, gblk, B, t.sums, loss_dev);
-  CP_LAUNCH_CHECK(h, "k_flow_loss");
-  k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, B, t.zs, t.vj, t.wg, t.sums, t);
+  k_flow_moments<<<1, 1, 0, h->stream>>>(h->d_slots, gblk, moments);
+  CP_LAUNCH_CHECK(h, "k_flow_moments");
+  return CP_OK;
+}
+
+// Phase 2: this handle's points' part of the gradient of the batch loss, from the batch's
+// moments over n_batch points, into the gradient buffer G (cleared first); loss_dev = the loss.
+static int flow_phase_gradient(cp_handle* h, const FlowTrainBufs& t, uint64_t count, const double* moments,
+                               uint64_t n_batch, double* loss_dev)
+{
+  k_flow_batch_loss<<<1, 1, 0, h->stream>>>(moments, (double)n_batch, t.sums, loss_dev);
+  CP_LAUNCH_CHECK(h, "k_flow_batch_loss");
+  k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, count, (double)n_batch, t.zs,
+                                                          t.vj, t.wg, t.sums, t);
   CP_LAUNCH_CHECK(h, "k_flow_bwd");
   float* G = h->d_flow + CP_FLOW_NPARAM;
   // at most CP_WG_MAXBLK blocks per coupling and layer; chunks are whole multiples of the staged
   // rows.  The three launches share the grid, so together they write every entry of the
   // partial slots 0 .. nblk-1 (all of W1, b1, W2, b2, W3, b3 of every coupling).
-  const uint64_t chunk = ((B + CP_WG_MAXBLK - 1) / CP_WG_MAXBLK + CP_WG_ROWS - 1) / CP_WG_ROWS * CP_WG_ROWS;
-  const int nblk = (int)((B + chunk - 1) / chunk);
+  const uint64_t chunk = ((count + CP_WG_MAXBLK - 1) / CP_WG_MAXBLK + CP_WG_ROWS - 1) / CP_WG_ROWS * CP_WG_ROWS;
+  const int nblk = (int)((count + chunk - 1) / chunk);
   const dim3 grid((unsigned)nblk, CP_FLOW_NC);
-  k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, B, t.gpart, CP_FLOW_W1, 64, 64, (int)chunk,
+  k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, count, t.gpart, CP_FLOW_W1, 64, 64, (int)chunk,
                                                     CP_FLOW_B1 - CP_FLOW_W1);
-  k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, B, t.gpart, CP_FLOW_W2, 64, 64, (int)chunk,
+  k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, count, t.gpart, CP_FLOW_W2, 64, 64, (int)chunk,
                                                     CP_FLOW_B2 - CP_FLOW_W2);
   // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
-  k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, B, t.gpart, CP_FLOW_W3, 8, 8, (int)chunk,
+  k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, count, t.gpart, CP_FLOW_W3, 8, 8, (int)chunk,
                                                     CP_FLOW_B3 - CP_FLOW_W3);
   CP_LAUNCH_CHECK(h, "k_flow_wgrad");
+  CP_CUDA(h, cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream));
   k_flow_gsum<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(t.gpart, nblk, G);
   CP_LAUNCH_CHECK(h, "k_flow_gsum");
   return CP_OK;
 }
 
+// Phase 3: Adam step h->flow_t + 1 on the gradient in G (which it clears), BF16 repack.
+static int flow_phase_update(cp_handle* h, double lr)
+{
+  float* G = h->d_flow + CP_FLOW_NPARAM;
+  const long step = h->flow_t + 1;
+  k_flow_adam<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(
+      h->d_flow, G, G + CP_FLOW_NPARAM, G + 2 * CP_FLOW_NPARAM, (float)lr, (float)pow(0.9, (double)step),
+      (float)pow(0.999, (double)step));
+  CP_LAUNCH_CHECK(h, "k_flow_adam");
+  const int rc = cp_flow_repack(h);
+  if (rc) return rc;
+  h->flow_t = step;
+  return CP_OK;
+}
+
 // Trains the flow for n_steps batches of `batch` points on the current VEGAS grid; loss_host
-// (n_steps doubles, may be NULL) receives <w^2>/<w>^2 of each batch before its update.
+// (n_steps doubles, may be NULL) receives <w^2>/<w>^2 of each batch before its update.  Step s
+// draws its batch at counter iteration flow_t (the number of updates so far), points 0..batch-1.
 extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host)
 {
   CP_CHECK_HANDLE(h);
   if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
   if (n_steps < 1 || batch < 64 || batch > (1ull << 24) || (batch & 31))
     return cp_fail(h, CP_ERR_INVALID, "cp_flow_train: batch must be a multiple of 32 in [64, 2^24]");
-  // per-device attributes: set on every call (host-side, cheap)
-  CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
-  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
-  void* mem = nullptr;
-  const size_t bytes = train_bytes(batch);
-  CP_CUDA(h, cudaMalloc(&mem, bytes + sizeof(double) * (size_t)n_steps));
-  FlowTrainBufs t = carve(mem, batch);
-  double* losses = reinterpret_cast<double*>(static_cast<char*>(mem) + bytes);
-  int rc = CP_OK;
-  cudaError_t e = cudaMemsetAsync(mem, 0, bytes, h->stream);
-  if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_train memset");
-  float* G = h->d_flow + CP_FLOW_NPARAM;
-  if (!rc) e = cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream);
+  h->ftrain_count = 0;   // a fresh layout: the buffers start from zeros
+  FlowTrainBufs t;
+  int rc = train_buffers(h, batch, t);
+  if (rc) return rc;
+  double* losses = nullptr;
+  CP_CUDA(h, cudaMalloc(&losses, sizeof(double) * (size_t)n_steps));
   for (int s = 0; s < n_steps && rc == CP_OK; ++s) {
-    rc = flow_train_step(h, t, batch, (uint32_t)(h->flow_t + s), (float)lr, losses + s);
-    if (rc) break;
-    const long step = h->flow_t + s + 1;
-    k_flow_adam<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(
-        h->d_flow, G, G + CP_FLOW_NPARAM, G + 2 * CP_FLOW_NPARAM, (float)lr,
-        (float)pow(0.9, (double)step), (float)pow(0.999, (double)step));
-    e = cudaGetLastError();
-    if (e != cudaSuccess) { rc = cp_fail_cuda(h, e, "k_flow_adam"); break; }
-    rc = cp_flow_repack(h);
+    rc = flow_phase_moments(h, t, 0, batch, (uint32_t)h->flow_t, t.sums);
+    if (!rc) rc = flow_phase_gradient(h, t, batch, t.sums, batch, losses + s);
+    if (!rc) rc = flow_phase_update(h, lr);
   }
-  if (!rc) {
-    h->flow_t += n_steps;
-    if (loss_host) e = cudaMemcpyAsync(loss_host, losses, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_train readback");
-  } else {
-    cudaStreamSynchronize(h->stream);
-  }
-  cudaFree(mem);
+  cudaError_t e = cudaSuccess;
+  if (!rc && loss_host) e = cudaMemcpyAsync(loss_host, losses, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (!rc && e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_train readback");
+  cudaFree(losses);
+  train_buffers_release(h);
   return rc;
 }
 
@@ -609,27 +661,66 @@ extern "C" int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, fl
   CP_CHECK_HANDLE(h);
   if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
   if (batch < 64 || batch > (1ull << 24) || (batch & 31)) return cp_fail(h, CP_ERR_INVALID, "bad batch");
-  // per-device attributes: set on every call (host-side, cheap)
-  CP_CUDA(h, cudaFuncSetAttribute(k_flow_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bwd_smem()));
-  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_smem()));
-  void* mem = nullptr;
-  const size_t bytes = train_bytes(batch);
-  CP_CUDA(h, cudaMalloc(&mem, bytes + sizeof(double)));
-  FlowTrainBufs t = carve(mem, batch);
-  double* loss = reinterpret_cast<double*>(static_cast<char*>(mem) + bytes);
+  h->ftrain_count = 0;
+  FlowTrainBufs t;
+  int rc = train_buffers(h, batch, t);
+  if (rc) return rc;
   float* G = h->d_flow + CP_FLOW_NPARAM;
-  cudaError_t e = cudaMemsetAsync(mem, 0, bytes, h->stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream);
-  int rc = e == cudaSuccess ? flow_train_step(h, t, batch, iter, 0.f, loss) : cp_fail_cuda(h, e, "memset");
+  rc = flow_phase_moments(h, t, 0, batch, iter, t.sums);
+  if (!rc) rc = flow_phase_gradient(h, t, batch, t.sums, batch, t.loss);
+  cudaError_t e = cudaSuccess;
   if (!rc) {
     e = cudaMemcpyAsync(grad_host, G, sizeof(float) * CP_FLOW_NPARAM, cudaMemcpyDeviceToHost, h->stream);
-    if (e == cudaSuccess && loss_host) e = cudaMemcpyAsync(loss_host, loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess && loss_host) e = cudaMemcpyAsync(loss_host, t.loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_loss_grad readback");
-  } else {
-    cudaStreamSynchronize(h->stream);
   }
-  cudaFree(mem);
+  train_buffers_release(h);
   return rc;
+}
+
+// ------------------------------------------------------------------------------------------
+// Data-parallel training: one step in three calls, the caller summing over ranks in between.
+// ------------------------------------------------------------------------------------------
+extern "C" int cp_flow_step_moments(cp_handle* h, uint64_t point0, uint64_t count, double* moments_dev)
+{
+  CP_CHECK_HANDLE(h);
+  if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
+  if (count < 1 || count > (1ull << 24) || !moments_dev)
+    return cp_fail(h, CP_ERR_INVALID, "cp_flow_step_moments: count must be in [1, 2^24]");
+  FlowTrainBufs t;
+  int rc = train_buffers(h, count, t);
+  if (rc) return rc;
+  return flow_phase_moments(h, t, point0, count, (uint32_t)h->flow_t, moments_dev);
+}
+
+extern "C" int cp_flow_step_gradient(cp_handle* h, const double* moments_dev, uint64_t batch_total, float* grad_dev,
+                                     double* loss_host)
+{
+  CP_CHECK_HANDLE(h);
+  if (!h->d_ftrain || !h->ftrain_count || !moments_dev || batch_total < h->ftrain_count)
+    return cp_fail(h, CP_ERR_INVALID, "cp_flow_step_gradient: call cp_flow_step_moments first (batch_total >= count)");
+  FlowTrainBufs t = carve(h->d_ftrain, h->ftrain_count);
+  int rc = flow_phase_gradient(h, t, h->ftrain_count, moments_dev, batch_total, t.loss);
+  if (rc) return rc;
+  if (grad_dev)
+    CP_CUDA(h, cudaMemcpyAsync(grad_dev, h->d_flow + CP_FLOW_NPARAM, sizeof(float) * CP_FLOW_NPARAM,
+                               cudaMemcpyDeviceToDevice, h->stream));
+  if (loss_host) {
+    CP_CUDA(h, cudaMemcpyAsync(loss_host, t.loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  }
+  return CP_OK;
+}
+
+extern "C" int cp_flow_step_update(cp_handle* h, const float* grad_dev, double lr)
+{
+  CP_CHECK_HANDLE(h);
+  if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
+  if (!(lr > 0.0)) return cp_fail(h, CP_ERR_INVALID, "cp_flow_step_update: lr must be positive");
+  if (grad_dev)
+    CP_CUDA(h, cudaMemcpyAsync(h->d_flow + CP_FLOW_NPARAM, grad_dev, sizeof(float) * CP_FLOW_NPARAM,
+                               cudaMemcpyDeviceToDevice, h->stream));
+  return flow_phase_update(h, lr);
 }

@@ -100,7 +100,11 @@ struct cp_handle {
   float4* d_flow_buf = nullptr;
   uint64_t flow_buf_cap = 0;
   int flow_on = 0;
-  long flow_t = 0;
+  long flow_t = 0;                         // optimiser updates so far (a step's batch iteration)
+  // training buffers of the current step (per-point forward state and GEMM operands for
+  // ftrain_count points), kept between the phases of a data-parallel step
+  void* d_ftrain = nullptr;
+  uint64_t ftrain_cap = 0, ftrain_count = 0;
   // tensor-core (tcgen05) forward: shared-memory weight image, bounded-wait status flag;
   // flow_kernel 0 = tcgen05 kernel, 1 = the warp-level mma.sync kernel
   uint8_t* d_flow_tc = nullptr;

@@ -7,14 +7,22 @@ union of the shards is exactly the single-device run.  The path has one exchange
 iteration: the pass sums (sum w, sum w^2, n_bad, 3 x n_bins per-bin sums of w^2; about 1.2 KB)
 are all-reduced by sum, the largest weight by max, and every rank then refines the same grid
 from the same numbers.  The unweighting threshold comes from the weight histogram summed over
-ranks, so every rank accepts against the same w_max.  Production passes need no exchange:
-each rank compacts its own events; only the per-pass counts are summed for reporting.
+ranks, so every rank accepts against the same w_max.  A variance-gradient step exchanges the
+adjoint sums of its pass the same way (entry 8, the largest weight, by max).  Flow training is
+data-parallel: each step's batch is shared out, the batch moments (2 doubles) and then the
+gradient (one float per parameter) are all-reduced, and every rank takes the same Adam step.
+Production passes need no exchange on their data path: each rank compacts its own events; the
+per-pass counts are summed for reporting and exclusive-scanned into record offsets.
 
-The compute backend is any object with the ``Integrator`` methods ``set_point_offset``,
-``accumulate``, ``refine``, ``weight_histogram``, ``quantile_from_histogram`` and ``unweight``;
-the reductions run on whatever device its tensors live on (NCCL for CUDA tensors, gloo for CPU).
+The compute backend is any object with the ``Integrator`` methods the calls use:
+``set_point_offset``, ``accumulate``, ``refine``, ``weight_histogram``,
+``quantile_from_histogram``, ``unweight``, ``adjoint_accumulate``, ``gradient_apply`` and
+``flow_step_moments`` / ``flow_step_gradient`` / ``flow_step_update``; the reductions run on
+whatever device its tensors live on (NCCL for CUDA tensors, gloo for CPU).
 """
 import math
+
+import numpy as np
 
 __all__ = ["shard", "ShardedIntegrator"]
 
@@ -38,14 +46,15 @@ class ShardedIntegrator:
         self.world = self.dist.get_world_size(group) if self.dist else 1
 
     # ---------------------------------------------------------------- reductions
-    def _reduce_sums(self, sums):
+    def _reduce_sums(self, sums, max_index=2):
+        """sum over ranks, except entry max_index (the largest weight): max"""
         if self.world == 1:
             return sums
-        wmax = sums[2:3].clone()
-        sums[2] = 0
+        wmax = sums[max_index:max_index + 1].clone()
+        sums[max_index] = 0
         self.dist.all_reduce(sums, group=self.group)
         self.dist.all_reduce(wmax, op=self.dist.ReduceOp.MAX, group=self.group)
-        sums[2:3] = wmax
+        sums[max_index:max_index + 1] = wmax
         return sums
 
     def _sum(self, values, like):
@@ -89,6 +98,40 @@ class ShardedIntegrator:
         if self.world > 1:
             self.dist.all_reduce(hist, group=self.group)
         return self.b.quantile_from_histogram(hist, q)
+
+    # ---------------------------------------------------------------- variance-gradient steps
+    def gradient_step(self, n_total, iteration=0, lr=0.5):
+        """One variance-gradient step with its adjoint pass sharded: one exchange of the adjoint
+        sums (10 + 12 n_bins doubles), then every rank takes the same step on its grid."""
+        offset, count = shard(n_total, self.rank, self.world)
+        self.b.set_point_offset(offset)
+        sums = self._reduce_sums(self.b.adjoint_accumulate(count, iteration), max_index=8)
+        return self.b.gradient_apply(sums, n_total, lr)
+
+    def adapt_gradient(self, steps, n_points, lr=0.4, iteration0=0):
+        """Integrator.adapt_gradient with every step sharded."""
+        from . import adapt_gradient_loop
+        return adapt_gradient_loop(self.gradient_step, steps, n_points, lr, iteration0)
+
+    # ---------------------------------------------------------------- flow training
+    def flow_train(self, steps, batch=65536, lr=1e-3):
+        """Integrator.flow_train data-parallel: each step's batch [0, batch) is shared out in
+        contiguous ranges; two exchanges per step (the batch moments, 2 doubles, then the gradient,
+        one float per parameter) and every rank takes the same Adam step.  One rank reproduces
+        Integrator.flow_train bit for bit."""
+        if batch < self.world:
+            raise ValueError("flow_train: fewer batch points than ranks")
+        offset, count = shard(batch, self.rank, self.world)
+        losses = np.zeros(steps)
+        for s in range(steps):
+            m = self.b.flow_step_moments(offset, count)
+            if self.world > 1:
+                self.dist.all_reduce(m, group=self.group)
+            g, losses[s] = self.b.flow_step_gradient(m, batch)
+            if self.world > 1:
+                self.dist.all_reduce(g, group=self.group)
+            self.b.flow_step_update(g, lr)
+        return losses
 
     # ---------------------------------------------------------------- production
     def unweight(self, n_total, iteration=0, records=None):

@@ -273,6 +273,17 @@ int cp_adjoint(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream, 
  * ln(bin width) -= lr * G / max|G|, G = dVar/dln(width), per dimension (the most sensitive bin
  * changes by exp(+-lr)); the alternative to the classic refinement of cp_vegas_iteration. */
 int cp_vegas_gradient_step(cp_handle* h, uint64_t n_points, uint32_t iter, double lr, cp_grad* out_host);
+/* The same step data-parallel, with one exchange (the reference shards its passes by point range,
+ * cuPythia/common/rng.cuh:5-19, and merges on the host; here the ranks sum device arrays):
+ * cp_adjoint_accumulate writes the adjoint sums of this handle's points [offset, offset +
+ * n_points) (cp_set_point_offset) to sums_dev, *n_doubles = cp_adjoint_sums_size of them; the
+ * caller reduces them over ranks (entry 8, the largest weight, by max, every other entry by sum);
+ * cp_vegas_gradient_apply then forms the gradient record of all n_total points and, with lr > 0,
+ * takes the grid step (lr = 0: the record only, as cp_adjoint).  One rank: the two calls are
+ * cp_vegas_gradient_step. */
+int cp_adjoint_sums_size(cp_handle* h, int* n_doubles);
+int cp_adjoint_accumulate(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream, double* sums_dev);
+int cp_vegas_gradient_apply(cp_handle* h, const double* sums_dev, uint64_t n_total, double lr, cp_grad* out_host);
 
 /* ---------------------------------------------------------------- learned proposal -- */
 /* A RealNVP-style flow on [0,1]^3 after the VEGAS map (between it and the base phase-space map):
@@ -305,6 +316,23 @@ int cp_flow_enable(cp_handle* h, int on);
 int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host);
 /* The training gradient of one batch (counter iteration iter, stream 2) without an update. */
 int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, float* grad_host, double* loss_host);
+/* Data-parallel training (no reference counterpart): one step of cp_flow_train in three calls,
+ * the ranks summing device arrays between them.  The step's batch is points [0, batch_total) of
+ * counter iteration = updates so far, stream 2; each rank takes a contiguous share.
+ *  1. cp_flow_step_moments: forward and integrand over the batch points [point0, point0 + count);
+ *     moments_dev[0..1] = (sum w, sum w^2) over them.  Sum moments_dev over ranks.
+ *  2. cp_flow_step_gradient: these points' part of the gradient of the batch loss
+ *     <w^2>/<w>^2 (from the summed moments over batch_total points) into grad_dev
+ *     (cp_flow_num_params() floats, may be NULL); loss_host (may be NULL) = the batch loss.
+ *     Sum grad_dev over ranks.
+ *  3. cp_flow_step_update: Adam step (learning rate lr) with the summed gradient (grad_dev NULL:
+ *     the handle's own gradient of step 2) and the BF16 repack.
+ * The per-point state of step 1 stays in the handle until step 2.  One rank with point0 = 0 and
+ * count = batch_total reproduces a step of cp_flow_train bit for bit. */
+int cp_flow_step_moments(cp_handle* h, uint64_t point0, uint64_t count, double* moments_dev);
+int cp_flow_step_gradient(cp_handle* h, const double* moments_dev, uint64_t batch_total, float* grad_dev,
+                          double* loss_host);
+int cp_flow_step_update(cp_handle* h, const float* grad_dev, double lr);
 
 /* ---------------------------------------------------------------- record consumers -- */
 /* Host-only (no GPU needed).  Colour tags (1..4, 0 = none) of the four partons of a record from
