@@ -116,7 +116,9 @@ extern "C" int cp_create(const cp_config* cfg, cp_handle** out)
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { delete h; return CP_ERR_CUDA; }
   if (cfg->device < 0 || cfg->device >= ndev) { delete h; return CP_ERR_INVALID; }
   h->device = cfg->device;
-  if (cudaSetDevice(h->device) != cudaSuccess) { delete h; return CP_ERR_CUDA; }
+  CpDeviceGuard guard(h->device);
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != h->device) { delete h; return CP_ERR_CUDA; }
   cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
   bool ok = cudaMalloc(&h->d_edges, sizeof(double) * 3 * (CP_MAX_BINS + 1)) == cudaSuccess &&
             cudaMalloc(&h->d_red, sizeof(double) * (CP_SLOT_HEAD + 3 * CP_MAX_BINS)) == cudaSuccess &&
@@ -139,7 +141,7 @@ extern "C" int cp_create(const cp_config* cfg, cp_handle** out)
 extern "C" int cp_destroy(cp_handle* h)
 {
   if (!h) return CP_OK;
-  cudaSetDevice(h->device);
+  CpDeviceGuard guard(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gen_copy) cudaStreamSynchronize(h->gen_copy);
   for (int k = 0; k < 4; ++k)

@@ -131,8 +131,28 @@ int cp_flow_tc_repack(cp_handle* h);
 int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out);
 int cp_flow_tc_status(cp_handle* h);
 
-#define CP_CHECK_HANDLE(h) \
-  do { if (!(h)) return CP_ERR_INVALID; } while (0)
+// Makes `dev` the calling thread's current device for the rest of the scope and restores the
+// caller's device at its end, so one host thread can drive handles on several GPUs.
+struct CpDeviceGuard {
+  int prev = -1;
+  explicit CpDeviceGuard(int dev)
+  {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != dev && cudaSetDevice(dev) == cudaSuccess) prev = cur;
+  }
+  ~CpDeviceGuard()
+  {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  CpDeviceGuard(const CpDeviceGuard&) = delete;
+  CpDeviceGuard& operator=(const CpDeviceGuard&) = delete;
+};
+
+// Entry check of every handle call (a statement at function scope): a null handle is invalid;
+// otherwise the handle's device is current until the function returns.
+#define CP_CHECK_HANDLE(h)             \
+  if (!(h)) return CP_ERR_INVALID;     \
+  CpDeviceGuard cp_device_guard_((h)->device)
 #define CP_CUDA(h, call)                                        \
   do {                                                          \
     cudaError_t e_ = (call);                                    \
