@@ -464,15 +464,18 @@ int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter,
   return CP_OK;
 }
 
-// Reads and clears the device status of the tensor-core flow kernel (after the stream has
-// been synchronised): CP_ERR_TIMEOUT if a bounded wait expired since the last check.
+// Reads and clears the device status of the tensor-core flow kernel, in order on the handle's
+// stream (which may be a non-blocking stream): CP_ERR_TIMEOUT if a bounded wait expired since
+// the last check.
 int cp_flow_tc_status(cp_handle* h)
 {
   if (!h->d_flow_status) return CP_OK;
   int s = 0;
-  CP_CUDA(h, cudaMemcpy(&s, h->d_flow_status, sizeof(int), cudaMemcpyDeviceToHost));
+  CP_CUDA(h, cudaMemcpyAsync(&s, h->d_flow_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
   if (!s) return CP_OK;
-  CP_CUDA(h, cudaMemset(h->d_flow_status, 0, sizeof(int)));
+  CP_CUDA(h, cudaMemsetAsync(h->d_flow_status, 0, sizeof(int), h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return cp_fail(h, CP_ERR_TIMEOUT, "k_flow_fwd_tc: a tensor-core wait expired (results of this pass are invalid)");
 }
 
