@@ -333,6 +333,36 @@ class Integrator:
         self._check(rc)
         return records[:min(r.n_accepted, capacity)], r.as_dict()
 
+    def to_device_events(self, records, n_events=None, max_part=4, n_var=1, scale_ratios=None, events=None, e0=0):
+        """Hand records (device uint8 [n, 64]) over to the reference pipeline's device event
+        record (DeviceEvents): a dict of device tensors, one per member, allocated like the
+        reference's allocEvents for n_events events (default: the records) unless `events` (such
+        a dict) is given; events e0 .. e0 + n - 1 are filled."""
+        torch = _torch()
+        n = records.shape[0]
+        if events is None:
+            ne = n_events if n_events is not None else n
+            npart = ne * max_part
+            dev = self.device
+            events = {"nEvents": ne, "maxPart": max_part, "nVar": n_var}
+            for f in ("px", "py", "pz", "e", "m"):
+                events[f] = torch.zeros(npart, dtype=torch.float64, device=dev)
+            for f in ("pdg", "status", "col", "acol", "mo1", "mo2", "d1", "d2"):
+                events[f] = torch.zeros(npart, dtype=torch.int32, device=dev)
+            events["nPart"] = torch.zeros(ne, dtype=torch.int32, device=dev)
+            events["seed"] = torch.zeros(ne, dtype=torch.int64, device=dev)
+            for f in ("scale", "x1", "x2"):
+                events[f] = torch.zeros(ne, dtype=torch.float64, device=dev)
+            for f in ("flavA", "flavB"):
+                events[f] = torch.zeros(ne, dtype=torch.int32, device=dev)
+            events["active"] = torch.ones(ne, dtype=torch.uint8, device=dev)
+            events["weight"] = torch.zeros(ne * n_var, dtype=torch.float64, device=dev)
+        ev = _lib.cp_device_events(events["nEvents"], events["maxPart"], events["nVar"],
+                                   *[_ptr(events[f]) for f, _ in _lib.cp_device_events._fields_[3:]])
+        self._check(self.lib.cp_records_to_device_events(
+            self.h, _ptr(records), n, _ptr(scale_ratios) if scale_ratios is not None else None, C.byref(ev), e0))
+        return events
+
     def unweight_scale_weights(self, n_points, iteration=0, records=None):
         """cp_unweight with the 7-point scale variation: (records, weights [n_acc, 6], stats); the
         weight columns are the ratios for (muR, muF) factors (2,1), (1/2,1), (1,2), (1,1/2),

@@ -73,6 +73,14 @@ class cp_grad(C.Structure):
     ]
 
 
+class cp_device_events(C.Structure):
+    """The reference pipeline's DeviceEvents (cuPythia/pipeline/event.cuh:20-31), member for member."""
+    _fields_ = [("nEvents", C.c_int), ("maxPart", C.c_int), ("nVar", C.c_int)] + [
+        (f, C.c_void_p) for f in ("px", "py", "pz", "e", "m", "pdg", "status", "col", "acol", "mo1", "mo2",
+                                  "d1", "d2", "nPart", "seed", "scale", "x1", "x2", "flavA", "flavB",
+                                  "active", "weight")]
+
+
 _P = C.c_void_p
 _u64 = C.c_uint64
 _u32 = C.c_uint32
@@ -125,6 +133,7 @@ SIGNATURES = {
     "cp_flow_step_moments": [_P, _u64, _u64, _P],
     "cp_flow_step_gradient": [_P, _P, _u64, _P, _P],
     "cp_flow_step_update": [_P, _P, _d],
+    "cp_records_to_device_events": [_P, _P, _u64, _P, C.POINTER(cp_device_events), _u64],
     "cp_flow_num_params": [],
     "cp_flow_init": [_P, _u64],
     "cp_flow_get_params": [_P, _P, _i],

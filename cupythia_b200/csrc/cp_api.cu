@@ -249,13 +249,6 @@ __global__ void k_philox_words(uint64_t seed, uint64_t p0, uint64_t n, uint32_t 
   }
 }
 
-__device__ __forceinline__ uint64_t cp_splitmix64(uint64_t x)
-{
-  x += 0x9E3779B97F4A7C15ULL;
-  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
-  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
-  return x ^ (x >> 31);
-}
 __device__ __forceinline__ double cp_u01(uint64_t u) { return (double)(u >> 11) * (1.0 / 9007199254740992.0); }
 
 __global__ void k_splitmix(uint64_t seed, uint64_t nthr, uint64_t kper, double* out)

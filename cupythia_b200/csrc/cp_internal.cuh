@@ -39,6 +39,48 @@ __host__ __device__ __forceinline__ float cp_qbin_hi(int b)
   return f;
 }
 
+// Colour tags (1..4, 0 = none) of the four partons of a record from its process code (111..115)
+// and encoded colour flow, as the process's setIdColAcol sets them (pythia8317/src/SigmaQCD.cc:
+// 135-342: the topologies in the order of its setColAcol calls, then swapCol1234 (bit 3) and
+// swapColAcol (bit 2)).  Returns false for a code / flow pair no process produces.  Host and
+// device.
+__host__ __device__ inline bool cp_colour_expand(uint16_t process, uint16_t colour, int col[4], int acol[4])
+{
+  // (col1, acol1, col2, acol2, col3, acol3, col4, acol4) per process and topology
+  constexpr int8_t topo_tab[5][3][8] = {
+      {{1, 2, 2, 3, 1, 4, 4, 3}, {1, 2, 3, 1, 3, 4, 4, 2}, {1, 2, 3, 4, 1, 4, 3, 2}},   // 111 g g -> g g
+      {{1, 2, 2, 3, 1, 0, 0, 3}, {1, 2, 3, 1, 3, 0, 0, 2}, {0, 0, 0, 0, 0, 0, 0, 0}},   // 112 g g -> q qbar
+      {{1, 0, 2, 1, 3, 0, 2, 3}, {1, 0, 2, 3, 2, 0, 1, 3}, {0, 0, 0, 0, 0, 0, 0, 0}},   // 113 q g -> q g
+      {{1, 0, 2, 0, 2, 0, 1, 0}, {1, 0, 0, 1, 2, 0, 0, 2}, {1, 0, 2, 0, 1, 0, 2, 0}},   // 114 q q -> q q
+      {{1, 0, 0, 2, 1, 3, 3, 2}, {1, 0, 0, 2, 3, 2, 1, 3}, {0, 0, 0, 0, 0, 0, 0, 0}}};  // 115 q qbar -> g g
+  if (process < 111 || process > 115) return false;
+  const int topo = colour & 3;
+  if (topo > 2 || (topo == 2 && process != 111 && process != 114)) return false;
+  int c[4], a[4];
+  for (int k = 0; k < 4; ++k) {
+    c[k] = topo_tab[process - 111][topo][2 * k];
+    a[k] = topo_tab[process - 111][topo][2 * k + 1];
+  }
+  if (colour & 8) {   // swapCol1234: partons 1 <-> 2 and 3 <-> 4
+    int x;
+    x = c[0]; c[0] = c[1]; c[1] = x;  x = a[0]; a[0] = a[1]; a[1] = x;
+    x = c[2]; c[2] = c[3]; c[3] = x;  x = a[2]; a[2] = a[3]; a[3] = x;
+  }
+  if (colour & 4)     // swapColAcol
+    for (int k = 0; k < 4; ++k) { const int x = c[k]; c[k] = a[k]; a[k] = x; }
+  for (int k = 0; k < 4; ++k) { col[k] = c[k]; acol[k] = a[k]; }
+  return true;
+}
+
+// SplitMix64 finaliser (cuPythia/common/rng.cuh:47-53); host and device
+__host__ __device__ __forceinline__ uint64_t cp_splitmix64(uint64_t x)
+{
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
 // Per-iteration record written by the device refinement kernel (FP64).
 struct CpIterDev {
   double sumw, sumw2, wmax, nbad, n, sigma, err, pad;

@@ -14,32 +14,10 @@
 #include <cstring>
 #include "cp_internal.cuh"
 
-// colour topologies in the order of the setColAcol calls of each process's setIdColAcol
-// (pythia8317/src/SigmaQCD.cc), (col1, acol1, col2, acol2, col3, acol3, col4, acol4)
-static const int8_t kTopo[5][3][8] = {
-    {{1, 2, 2, 3, 1, 4, 4, 3}, {1, 2, 3, 1, 3, 4, 4, 2}, {1, 2, 3, 4, 1, 4, 3, 2}},   // 111 g g -> g g
-    {{1, 2, 2, 3, 1, 0, 0, 3}, {1, 2, 3, 1, 3, 0, 0, 2}, {0, 0, 0, 0, 0, 0, 0, 0}},   // 112 g g -> q qbar
-    {{1, 0, 2, 1, 3, 0, 2, 3}, {1, 0, 2, 3, 2, 0, 1, 3}, {0, 0, 0, 0, 0, 0, 0, 0}},   // 113 q g -> q g
-    {{1, 0, 2, 0, 2, 0, 1, 0}, {1, 0, 0, 1, 2, 0, 0, 2}, {1, 0, 2, 0, 1, 0, 2, 0}},   // 114 q q -> q q
-    {{1, 0, 0, 2, 1, 3, 3, 2}, {1, 0, 0, 2, 3, 2, 1, 3}, {0, 0, 0, 0, 0, 0, 0, 0}}};  // 115 q qbar -> g g
-
 extern "C" int cp_colour_tags(uint16_t process, uint16_t colour, int col[4], int acol[4])
 {
-  if (process < 111 || process > 115 || !col || !acol) return CP_ERR_INVALID;
-  const int topo = colour & 3;
-  if (topo > 2 || (topo == 2 && process != 111 && process != 114)) return CP_ERR_INVALID;
-  const int8_t* t = kTopo[process - 111][topo];
-  int c[4], a[4];
-  for (int k = 0; k < 4; ++k) { c[k] = t[2 * k]; a[k] = t[2 * k + 1]; }
-  if (colour & 8) {   // swapCol1234: partons 1 <-> 2 and 3 <-> 4
-    int x;
-    x = c[0]; c[0] = c[1]; c[1] = x;  x = a[0]; a[0] = a[1]; a[1] = x;
-    x = c[2]; c[2] = c[3]; c[3] = x;  x = a[2]; a[2] = a[3]; a[3] = x;
-  }
-  if (colour & 4)     // swapColAcol
-    for (int k = 0; k < 4; ++k) { const int x = c[k]; c[k] = a[k]; a[k] = x; }
-  for (int k = 0; k < 4; ++k) { col[k] = c[k]; acol[k] = a[k]; }
-  return CP_OK;
+  if (!col || !acol) return CP_ERR_INVALID;
+  return cp_colour_expand(process, colour, col, acol) ? CP_OK : CP_ERR_INVALID;
 }
 
 // LHEF tag of a colour index (0 = none)

@@ -334,6 +334,36 @@ int cp_flow_step_gradient(cp_handle* h, const double* moments_dev, uint64_t batc
                           double* loss_host);
 int cp_flow_step_update(cp_handle* h, const float* grad_dev, double lr);
 
+/* ---------------------------------------------------------------- device hand-off --- */
+/* The reference pipeline's device-resident event record (cuPythia/pipeline/event.cuh:20-31,
+ * struct DeviceEvents): the same members in the same order and types, so a DeviceEvents built by
+ * the reference's allocEvents (event.cuh:33-48) can be passed by address.  Particle p of event e
+ * is at e * maxPart + p; every pointer is device memory owned by the caller. */
+typedef struct cp_device_events {
+  int nEvents, maxPart, nVar;          /* nVar >= 1 weights per event (slot 0 nominal)      */
+  double *px, *py, *pz, *e, *m;        /* [nEvents * maxPart]                               */
+  int *pdg, *status, *col, *acol, *mo1, *mo2, *d1, *d2;
+  int *nPart;                          /* [nEvents]                                         */
+  uint64_t *seed;
+  double *scale, *x1, *x2;
+  int *flavA, *flavB;
+  unsigned char *active;
+  double *weight;                      /* [nEvents * nVar]                                  */
+} cp_device_events;
+/* Hands n records (dev) over to events [e0, e0 + n) of `ev`, on the device, as the reference's
+ * hard-process stage fills an event with addParticle (cuPythia/pipeline/generate.cu:30-48,
+ * event.cuh:59-71): the two incoming partons (status -21, mothers -1, momentum (0, 0, pz, |pz|))
+ * and the two outgoing ones (status 23, mothers 0 and 1), massless, daughters -1, colour tags
+ * 500 + the record's colour flow tags (0 = none); nPart = 4, seed = the event key
+ * splitmix64(config seed ^ point * 0x9E3779B97F4A7C15) of the record's point (the per-event key
+ * of cuPythia/pipeline/generate.cu:33), scale = sqrt(k_fac) pT_hat (the factorisation scale),
+ * x1, x2 = the incoming energies over sqrt(s)/2, flavA, flavB = the incoming ids, active = 1, and
+ * weight slot 0 = the record weight.  With scale_ratios_dev (6 floats per record, as
+ * cp_set_scale_weights writes them) slots 1 .. nVar-1 (nVar <= 7) hold weight x ratio k-1;
+ * without it nVar must be 1.  Requires maxPart >= 4 and e0 + n <= nEvents. */
+int cp_records_to_device_events(cp_handle* h, const cp_event* records_dev, uint64_t n,
+                                const float* scale_ratios_dev, const cp_device_events* ev, uint64_t e0);
+
 /* ---------------------------------------------------------------- record consumers -- */
 /* Host-only (no GPU needed).  Colour tags (1..4, 0 = none) of the four partons of a record from
  * its process code and encoded colour flow, as the process's setIdColAcol sets them

@@ -79,3 +79,82 @@ def test_lhef_of_device_records_reads_back_in_pythia(production, tmp_path):
     assert out["max_imbalance_gev"] < 0.05, out
     assert out["by_code"] == [int((ev[:n]["process"] == c).sum()) for c in range(111, 116)]
     assert abs(out["sigma_gen_mb"] / st["sigma"] - 1) < 1e-6
+
+
+def _splitmix64(x):
+    x = (x + np.uint64(0x9E3779B97F4A7C15))
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def test_device_event_hand_off():
+    """Records (with the 7-point scale ratios) handed over to the reference pipeline's device
+    event record: every member equals the host-side expansion of the same records bit for bit
+    (incoming status -21 with mothers -1, outgoing 23 with mothers 0 and 1, colour tags 500 + the
+    record's setIdColAcol tags, the event key, scale, x1, x2, flavours, weight vector); events
+    outside [e0, e0 + n) stay untouched; bad shapes are refused."""
+    import ctypes as C
+
+    import torch
+
+    import cupythia_b200 as cp
+    n_pts = 1 << 20
+    with cp.Integrator() as it:
+        it.integrate(5, 1 << 20, alpha=1.5)
+        it.iteration(n_pts, 80, alpha=0.0)
+        it.weight_quantile(0.999)
+        rec, ratios, st = it.unweight_scale_weights(n_pts, iteration=81)
+        n = rec.shape[0]
+        e0 = 3
+        ev = it.to_device_events(rec, n_events=n + 5, n_var=7, scale_ratios=ratios.contiguous(), e0=e0)
+        # refused: more than one weight without ratios, too few particle slots, too many events
+        res = []
+        for kw in ({"n_var": 2}, {"max_part": 3}, {"n_events": n - 1}):
+            try:
+                it.to_device_events(rec, **kw)
+                res.append(0)
+            except cp.CpError as err:
+                res.append(1 if err.code == cp._lib.CP_ERR_INVALID else 2)
+        cfg = it.cfg
+        host = {k: (v.cpu().numpy() if hasattr(v, "cpu") else v) for k, v in ev.items()}
+        r = cp.events_view(rec)
+        rt = ratios.cpu().numpy()
+    assert res == [1, 1, 1]
+    mp = 4
+    idx = (e0 + np.arange(n))[:, None] * mp + np.arange(4)[None, :]
+    pz_in = r["pz_in"].astype(np.float64)
+    px = np.zeros((n, 4)); py = np.zeros((n, 4)); pz = np.zeros((n, 4)); en = np.zeros((n, 4))
+    pz[:, :2] = pz_in
+    en[:, :2] = np.abs(pz_in)
+    for k, key in ((2, "p3"), (3, "p4")):
+        p = r[key].astype(np.float64)
+        px[:, k], py[:, k], pz[:, k], en[:, k] = p[:, 0], p[:, 1], p[:, 2], p[:, 3]
+    c, a = cp.colour_tags(r)
+    col = np.where(c > 0, 500 + c, 0).astype(np.int32)
+    acol = np.where(a > 0, 500 + a, 0).astype(np.int32)
+    assert np.array_equal(host["px"][idx], px) and np.array_equal(host["py"][idx], py)
+    assert np.array_equal(host["pz"][idx], pz) and np.array_equal(host["e"][idx], en)
+    assert np.all(host["m"][idx] == 0)
+    assert np.array_equal(host["pdg"][idx], r["id"].astype(np.int32))
+    assert np.array_equal(host["status"][idx], np.tile([-21, -21, 23, 23], (n, 1)))
+    assert np.array_equal(host["mo1"][idx], np.tile([-1, -1, 0, 0], (n, 1)))
+    assert np.array_equal(host["mo2"][idx], np.tile([-1, -1, 1, 1], (n, 1)))
+    assert np.all(host["d1"][idx] == -1) and np.all(host["d2"][idx] == -1)
+    assert np.array_equal(host["col"][idx], col) and np.array_equal(host["acol"][idx], acol)
+    e = e0 + np.arange(n)
+    assert np.all(host["nPart"][e] == 4) and np.all(host["active"][e] == 1)
+    key = _splitmix64(np.uint64(cfg.seed) ^ (r["point"].astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)))
+    assert np.array_equal(host["seed"][e].view(np.uint64), key)
+    assert np.array_equal(host["scale"][e], np.sqrt(cfg.k_fac) * r["pt_hat"].astype(np.float64))
+    assert np.array_equal(host["x1"][e], np.abs(pz_in[:, 0]) * (2.0 / cfg.sqrt_s))
+    assert np.array_equal(host["x2"][e], np.abs(pz_in[:, 1]) * (2.0 / cfg.sqrt_s))
+    assert np.array_equal(host["flavA"][e], r["id"][:, 0].astype(np.int32))
+    assert np.array_equal(host["flavB"][e], r["id"][:, 1].astype(np.int32))
+    w = host["weight"].reshape(-1, 7)[e]
+    wt = r["weight"].astype(np.float64)
+    assert np.array_equal(w[:, 0], wt)
+    assert np.array_equal(w[:, 1:], wt[:, None] * rt.astype(np.float64))
+    # events before e0 and after e0 + n are as allocated
+    out = np.r_[0:e0, e0 + n:n + 5]
+    assert np.all(host["nPart"][out] == 0) and np.all(host["weight"].reshape(-1, 7)[out] == 0)
