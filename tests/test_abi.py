@@ -50,3 +50,23 @@ def test_no_silent_cpu_path_without_gpu():
     import cupythia_b200 as cp
     with pytest.raises(cp.CpError):
         cp.Integrator()
+
+
+def test_device_event_struct_layout_matches_ctypes(tmp_path):
+    """cp_device_events as a C compiler lays it out (the reference's DeviceEvents member order)
+    equals the ctypes mirror the Python layer passes."""
+    import ctypes as C
+    import subprocess
+
+    from cupythia_b200 import _lib
+    fields = [f for f, _ in _lib.cp_device_events._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "cupythia_b200.h"\nint main(void) {\n'
+                   '  printf("%zu", sizeof(cp_device_events));\n' +
+                   "".join(f'  printf(" %zu", offsetof(cp_device_events, {f}));\n' for f in fields) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(_lib.cp_device_events)] + [getattr(_lib.cp_device_events, f).offset for f in fields]
+    assert got == want
