@@ -144,8 +144,7 @@ extern "C" int cp_destroy(cp_handle* h)
   CpDeviceGuard guard(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->gen_copy) cudaStreamSynchronize(h->gen_copy);
-  for (int k = 0; k < 4; ++k)
-    if (h->tev[k]) cudaEventDestroy(h->tev[k]);
+  for (cudaEvent_t e : h->tpool) cudaEventDestroy(e);
   for (int k = 0; k < CP_GEN_BUFS; ++k) {
     if (h->gen_counted[k]) cudaEventDestroy(h->gen_counted[k]);
     if (h->gen_copied[k]) cudaEventDestroy(h->gen_copied[k]);
@@ -155,7 +154,8 @@ extern "C" int cp_destroy(cp_handle* h)
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
                   h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq, h->d_flow, h->d_flow_pk,
                   h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_pdfbuf,
-                  h->d_gen_stage, h->d_gen_red, h->d_gen_cnt, h->d_ftrain};
+                  h->d_gen_stage, h->d_gen_red, h->d_gen_cnt, h->d_ftrain, h->d_tails, h->d_bcount,
+                  h->d_rsum, h->d_roff, h->d_unw_red};
   for (void* b : bufs)
     if (b) cudaFree(b);
   delete h;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 #include <string.h>
 #include "../../include/cupythia_b200.h"
 #include "cp_params.h"
@@ -115,8 +116,16 @@ struct cp_handle {
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
   unsigned long long* d_counter = nullptr; // accepted-event counter
-  float4* d_pdfbuf = nullptr;              // per record slot: PDFs of the accepted point (K1 -> K2)
+  // production staging for pdfbuf_cap points (K1 -> K2): PDFs and record tails per point, accepted
+  // counts per 32-point block, totals and output offsets per 1024-point range; per-chunk sums
+  float4* d_pdfbuf = nullptr;
+  uint4* d_tails = nullptr;
+  uint8_t* d_bcount = nullptr;
+  unsigned* d_rsum = nullptr;
+  unsigned long long* d_roff = nullptr;
   uint64_t pdfbuf_cap = 0;
+  double* d_unw_red = nullptr;
+  uint64_t unw_red_cap = 0;
   float* scalew = nullptr;                 // caller's scale-variation weights (6 per record), or null
   uint64_t scalew_cap = 0;
   // cp_generate_host pipeline, kept between calls: CP_GEN_BUFS record staging buffers of gen_cap
@@ -156,7 +165,7 @@ struct cp_handle {
   // optional per-kernel timing of the production pass (CUDA events on the handle's stream):
   // 0 = flow forward, 1 = accept (K1), 2 = record build (K2)
   int timing = 0;
-  cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> tpool;          // production timing events: 2 + 3 per chunk
   double t_ms[3] = {0, 0, 0};
   uint64_t t_launches[3] = {0, 0, 0};
   std::string err;

@@ -1,17 +1,21 @@
 // cp_unweight.cu -- production pass: unweighting and on-device compaction into 64-byte records.
 //
-// K1 draws, maps and evaluates each point exactly like the VEGAS pass, accepts it when
+// K1 draws, maps and evaluates each point exactly like the VEGAS pass and accepts it when
 // u * w_max < w (cuPythia/07_unweighting_lhe/unweight_lhe.cu:54; overweight events w > w_max
 // are kept with weight w / w_max, as Pythia keeps them, pythia8317/src/ProcessContainer.cc:
-// 383-385) and reserves a slot in the dense record array (one ballot and one global atomic per
-// warp); beside the slot it stores the point's 16 PDF values.  K2 then runs over the reserved
-// slots only, with every lane busy, recomputes the points' kinematics and brackets (the PDFs
-// come from K1), picks process, flavours and colour flow, and writes the 64-byte records as four
-// 16-byte stores (and, on request, the 7-point scale-variation ratios).  Keeping the record builder
-// out of K1 keeps K1's code small (its instruction-cache footprint, not arithmetic, limited the
-// fused version) and its lanes converged.  The reference instead writes flags and runs a
-// separate library compaction pass (cuPythia/10_cub_compaction/cub_compaction.cu:76-80,
-// cuPythia/pipeline/generate.cu:97-104).
+// 383-385).  Per 32-point block (one warp's points) it stores the number accepted and adds it to
+// its 1024-point range's total (an integer atomic: exact in any order), and packs the accepted
+// points' record tails and 16 PDF values, in point order, at the front of the block's staging
+// slots.  A one-block scan of the range totals gives each range's output offset, so the records
+// come out in point order, exactly as the reference's library compaction orders them
+// (cub::DeviceSelect::Flagged, cuPythia/10_cub_compaction/cub_compaction.cu:76-80,
+// cuPythia/pipeline/generate.cu:97-104), without any block waiting on another.  K2 takes one
+// range per warp, spreads its accepted points over the lanes (every lane busy), recomputes the
+// points' kinematics and brackets (the PDFs come from K1), picks process, flavours and colour
+// flow, and writes the 64-byte records as four 16-byte stores (and, on request, the 7-point
+// scale-variation ratios).  Keeping the record builder out of K1 keeps K1's code small and its
+// lanes converged.  Staging grows with the points of a pass, so passes run in chunks of at most
+// CP_UNW_CHUNK points.
 //
 // Random numbers: the accept draw is word 3 of the point's Philox block (stream 0); accepted
 // points draw a second block from stream 1 for the process / pair / azimuth / new-flavour picks
@@ -20,6 +24,8 @@
 #include "cp_internal.cuh"
 
 #define CP_UNW_SLOT 8   // sum w, sum w^2, max w, n_bad, n_acc, sum event weight, n_over, unused
+#define CP_UNW_CHUNK (1ull << 24)   // points per production chunk (staging: 80 B per point)
+#define CP_UNW_RANGE 32             // 32-point blocks per record-builder warp (1024 points)
 
 struct UnwLaunch {
   uint64_t seed, point0, n;
@@ -29,10 +35,14 @@ struct UnwLaunch {
   const CpCteqPoly* cteq;
   const double* wmax;          // device threshold
   CpEventRec* out;
-  float4* pdf;                 // per record slot: fa[8], fb[8] of the accepted point (K1 -> K2)
-  float* scalew;               // per record slot: 6 scale-variation ratios, or null
+  float4* pdf;                 // staging per point: fa[8], fb[8] of the accepted points (K1 -> K2)
+  uint4* tails;                // staging per point: the record's last 16 bytes, or null (no records)
+  uint8_t* bcount;             // accepted points per 32-point block
+  unsigned* rsum;              // accepted points per 1024-point range (zeroed before K1)
+  const unsigned long long* roff;   // output index of the first record of each range
+  uint64_t nblk, nrange;
+  float* scalew;               // per record: 6 scale-variation ratios, or null
   uint64_t capacity;
-  unsigned long long* counter; // events accepted so far (may exceed capacity: reported)
   double* slots;
   const float4* flow;          // flow output (v, ln J) per in-call point, or null
 };
@@ -84,8 +94,9 @@ __device__ __forceinline__ void cp_stage_edges(float2 (*sEdge)[CP_MAX_BINS], con
   }
 }
 
-// K1: weight, accept, reserve a record slot (one ballot and one atomic per warp) and store the
-// point's in-call index and event weight in that slot; K2 fills in the rest of the record.
+// K1: weight, accept; per 32-point block the accepted count (also added to its range's total),
+// and each accepted point's record tail (event weight, in-call point index) and PDFs packed at
+// the front of the block's staging slots in point order; K2 fills in the rest of the record.
 __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const CpHadParams P, const UnwLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
@@ -119,26 +130,27 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
       accept = cp_u24(wd[3]) * wmax < w;
     }
     const unsigned ball = __ballot_sync(0xffffffffu, accept);
-    if (ball == 0u) continue;
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(L.counter, (unsigned long long)__popc(ball));
-    base = __shfl_sync(0xffffffffu, base, 0);
+    // the warp's 32 points are one block: p0 is a multiple of 32 (stride and block slices are)
+    const uint64_t p0 = p - (uint64_t)lane;
+    if (L.tails && lane == 0 && p0 < L.n) {
+      L.bcount[p0 >> 5] = (uint8_t)__popc(ball);
+      if (ball) atomicAdd(&L.rsum[p0 >> 10], (unsigned)__popc(ball));   // integer sum: order-free
+    }
     if (accept) {
-      const uint64_t slot = base + __popc(ball & ((1u << lane) - 1u));
       const float ew = w > wmax ? w / wmax : 1.f;
       ++nacc;
       nover += w > wmax ? 1u : 0u;
       cp_kahan(se, ce, ew);
-      if (slot < L.capacity) {
+      if (L.tails) {
+        const uint64_t q = p0 + (uint64_t)__popc(ball & ((1u << lane) - 1u));
         // weight, pt_hat, process, point: the last 16 bytes of the record
-        uint4* dst = reinterpret_cast<uint4*>(L.out + slot) + 3;
-        *dst = make_uint4(__float_as_uint(ew), 0u, 0u, (uint32_t)p);
+        L.tails[q] = make_uint4(__float_as_uint(ew), 0u, 0u, (uint32_t)p);
         // the PDFs of the point, so that the record builder need not evaluate CTEQ5L again
-        float4* q = L.pdf + 4 * slot;
-        q[0] = make_float4(pt.fa[0], pt.fa[1], pt.fa[2], pt.fa[3]);
-        q[1] = make_float4(pt.fa[4], pt.fa[5], pt.fa[6], pt.fa[7]);
-        q[2] = make_float4(pt.fb[0], pt.fb[1], pt.fb[2], pt.fb[3]);
-        q[3] = make_float4(pt.fb[4], pt.fb[5], pt.fb[6], pt.fb[7]);
+        float4* f = L.pdf + 4 * q;
+        f[0] = make_float4(pt.fa[0], pt.fa[1], pt.fa[2], pt.fa[3]);
+        f[1] = make_float4(pt.fa[4], pt.fa[5], pt.fa[6], pt.fa[7]);
+        f[2] = make_float4(pt.fb[0], pt.fb[1], pt.fb[2], pt.fb[3]);
+        f[3] = make_float4(pt.fb[4], pt.fb[5], pt.fb[6], pt.fb[7]);
       }
     }
   }
@@ -160,9 +172,48 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
   }
 }
 
-// K2: dense pass over the reserved slots: re-evaluate the accepted point's kinematics (its PDFs
-// come from K1's per-slot copy), pick process, flavours and colour flow, build the lab-frame
-// kinematics, store the full 64-byte record.
+// Output offsets: roff[r] = *base_io + the records of the ranges before r; then *base_io +=
+// the chunk's records.  One block of 1024 threads scans the range totals in tiles of 1024
+// (coalesced loads, warp shuffles, one running carry): fixed order.
+__global__ void __launch_bounds__(1024) k_unw_scan(const unsigned* __restrict__ rsum, uint64_t nrange,
+                                                   unsigned long long* base_io, unsigned long long* __restrict__ roff)
+{
+  __shared__ unsigned long long wsum[32];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  unsigned long long carry = *base_io;
+  for (uint64_t i0 = 0; i0 < nrange; i0 += 1024) {
+    const uint64_t i = i0 + t;
+    const unsigned long long v = i < nrange ? rsum[i] : 0ull;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      unsigned long long z = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      wsum[lane] = z;
+    }
+    __syncthreads();
+    if (i < nrange) roff[i] = carry + (w ? wsum[w - 1] : 0ull) + x - v;
+    carry += wsum[31];
+    __syncthreads();   // wsum is rewritten by the next tile
+  }
+  __syncthreads();     // every thread has read *base_io
+  if (t == 0) *base_io = carry;
+}
+
+// K2: one warp per 1024-point range (32 blocks): the lanes' block counts, scanned across the
+// warp, spread the range's accepted points over the lanes in point order; each lane re-evaluates
+// its point's kinematics (the PDFs come from K1's staging), picks process, flavours and colour
+// flow, builds the lab-frame kinematics and stores the full 64-byte record at its output index.
 // 4 resident blocks per SM without scale weights (64 registers), 2 with them
 template <bool SCALEW>
 __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const CpHadParams P, const UnwLaunch L)
@@ -172,39 +223,61 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
   cp_stage_edges(sEdge, L.edges, L.nb);
   cp_stage_cteq(sCteq, L.cteq);
   __syncthreads();
-  const unsigned long long acc = *L.counter;
-  const uint64_t nrec = acc < L.capacity ? acc : L.capacity;
-  for (uint64_t k = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x; k < nrec;
-       k += (uint64_t)gridDim.x * CP_THREADS) {
-    const uint4 tail = reinterpret_cast<const uint4*>(L.out + k)[3];
-    const uint64_t point = L.point0 + tail.w;
-    uint32_t wd[4], w2[4];
-    cp_point_words(L.seed, point, L.iter, 0, wd);
-    cp_point_words(L.seed, point, L.iter, 1, w2);
-    CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, tail.w);
-    float pdf[16];
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = (uint64_t)gridDim.x * (CP_THREADS / 32);
+  for (uint64_t R = ((uint64_t)blockIdx.x * CP_THREADS + threadIdx.x) >> 5; R < L.nrange; R += nwarps) {
+    const uint64_t blk = R * CP_UNW_RANGE + lane;
+    const unsigned c = blk < L.nblk ? (unsigned)L.bcount[blk] : 0u;
+    unsigned incl = c;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float4 v = L.pdf[4 * k + q];
-      pdf[4 * q] = v.x; pdf[4 * q + 1] = v.y; pdf[4 * q + 2] = v.z; pdf[4 * q + 3] = v.w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
     }
-    CpPoint pt;
-    cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt, pdf);
-    CpEventRec ev;
-    cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
-                  cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
-    if (SCALEW) {
-      float r[6];
-      cp_scale_ratios(P, sCteq, pt, r);
-      float2* sw = reinterpret_cast<float2*>(L.scalew + 6 * k);
-      sw[0] = make_float2(r[0], r[1]);
-      sw[1] = make_float2(r[2], r[3]);
-      sw[2] = make_float2(r[4], r[5]);
-    }
-    const uint4* src = reinterpret_cast<const uint4*>(&ev);
-    uint4* dst = reinterpret_cast<uint4*>(L.out + k);
+    const unsigned excl = incl - c;
+    const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    const unsigned long long base = L.roff[R];
+    for (unsigned j0 = 0; j0 < total; j0 += 32) {
+      const unsigned j = j0 + lane;
+      // this lane's entry lies in the first block whose inclusive count exceeds j
+      int b = 0;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) dst[q] = src[q];
+      for (int st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(0xffffffffu, incl, b + st - 1) <= j) b += st;
+      const unsigned ex = __shfl_sync(0xffffffffu, excl, b);
+      const uint64_t k = base + j;   // output record
+      if (j >= total || k >= L.capacity) continue;
+      const uint64_t q = (R * CP_UNW_RANGE + b) * 32 + (j - ex);   // staging slot
+      const uint4 tail = L.tails[q];
+      const uint64_t point = L.point0 + tail.w;
+      uint32_t wd[4], w2[4];
+      cp_point_words(L.seed, point, L.iter, 0, wd);
+      cp_point_words(L.seed, point, L.iter, 1, w2);
+      CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, tail.w);
+      float pdf[16];
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const float4 v = L.pdf[4 * q + f];
+        pdf[4 * f] = v.x; pdf[4 * f + 1] = v.y; pdf[4 * f + 2] = v.z; pdf[4 * f + 3] = v.w;
+      }
+      CpPoint pt;
+      cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt, pdf);
+      CpEventRec ev;
+      cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
+                    cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
+      if (SCALEW) {
+        float r[6];
+        cp_scale_ratios(P, sCteq, pt, r);
+        float2* sw = reinterpret_cast<float2*>(L.scalew + 6 * k);
+        sw[0] = make_float2(r[0], r[1]);
+        sw[1] = make_float2(r[2], r[3]);
+        sw[2] = make_float2(r[4], r[5]);
+      }
+      const uint4* src = reinterpret_cast<const uint4*>(&ev);
+      uint4* dst = reinterpret_cast<uint4*>(L.out + k);
+#pragma unroll
+      for (int f = 0; f < 4; ++f) dst[f] = src[f];
+    }
   }
 }
 
@@ -236,67 +309,125 @@ static int build_blocks(cp_handle* h, bool scalew)
   return h->num_sms * c;
 }
 
-// Enqueue one production pass on h->stream (no host synchronisation).
-static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, cp_event* out,
-                            uint64_t capacity, double* red_dst, float* scalew = nullptr)
+// Staging of a production chunk of n points: record tails and PDFs per point, accepted counts
+// per 32-point block, totals and output offsets per 1024-point range.
+static int unw_staging(cp_handle* h, uint64_t n)
 {
+  if (n <= h->pdfbuf_cap) return CP_OK;
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  void* old[] = {h->d_pdfbuf, h->d_tails, h->d_bcount, h->d_roff, h->d_rsum};
+  for (void* b : old)
+    if (b) CP_CUDA(h, cudaFree(b));
+  h->d_pdfbuf = nullptr; h->d_tails = nullptr; h->d_bcount = nullptr; h->d_roff = nullptr; h->d_rsum = nullptr;
+  h->pdfbuf_cap = 0;
+  const uint64_t nblk = (n + 31) / 32, nrange = (nblk + CP_UNW_RANGE - 1) / CP_UNW_RANGE;
+  CP_CUDA(h, cudaMalloc(&h->d_pdfbuf, sizeof(float4) * 4 * n));
+  CP_CUDA(h, cudaMalloc(&h->d_tails, sizeof(uint4) * n));
+  CP_CUDA(h, cudaMalloc(&h->d_bcount, nblk));
+  CP_CUDA(h, cudaMalloc(&h->d_roff, sizeof(unsigned long long) * nrange));
+  CP_CUDA(h, cudaMalloc(&h->d_rsum, sizeof(unsigned) * nrange));
+  h->pdfbuf_cap = n;
+  return CP_OK;
+}
+
+// Per-kernel timing events of a pass: the flow forward's pair, then 3 per chunk (before the
+// accept kernel, after it, after the record builder); created on first use.
+static int timing_reserve(cp_handle* h, size_t nsub)
+{
+  if (!h->timing) return CP_OK;
+  while (h->tpool.size() < 2 + 3 * nsub) {
+    cudaEvent_t e;
+    CP_CUDA(h, cudaEventCreate(&e));
+    h->tpool.push_back(e);
+  }
+  return CP_OK;
+}
+
+// Adds the kernel durations of one pass (after its last event) and counts the pass once per
+// kernel that ran.
+static void timing_collect(cp_handle* h, size_t nsub, bool flow, bool build)
+{
+  if (!h->timing || nsub == 0 || h->tpool.size() < 2 + 3 * nsub) return;
+  if (cudaEventSynchronize(h->tpool[2 + 3 * nsub - 1]) != cudaSuccess) return;
+  float a = 0.f;
+  if (flow && cudaEventElapsedTime(&a, h->tpool[0], h->tpool[1]) == cudaSuccess) h->t_ms[0] += a;
+  for (size_t c = 0; c < nsub; ++c) {
+    float b = 0.f, d = 0.f;
+    cudaEventElapsedTime(&b, h->tpool[2 + 3 * c], h->tpool[2 + 3 * c + 1]);
+    cudaEventElapsedTime(&d, h->tpool[2 + 3 * c + 1], h->tpool[2 + 3 * c + 2]);
+    h->t_ms[1] += b; h->t_ms[2] += d;
+  }
+  h->t_launches[0] += flow ? 1 : 0;
+  h->t_launches[1] += 1;
+  h->t_launches[2] += build ? 1 : 0;
+}
+
+// Enqueue one production chunk of n <= CP_UNW_CHUNK points on h->stream (no host
+// synchronisation).  Its records go to out[*base_dev ...] in point order (records at or beyond
+// `capacity` are counted, not stored) and *base_dev advances by the chunk's accepted points;
+// red_dst receives the chunk's sums.  With the flow on, flow_pre holds the flow output of the
+// chunk's points (the caller ran the forward pass for the whole pass), or is null and the chunk
+// runs its own.  tslot >= 0 records the chunk's timing events.
+static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, cp_event* out,
+                            uint64_t capacity, double* red_dst, float* scalew, unsigned long long* base_dev,
+                            const float4* flow_pre, int tslot)
+{
+  if (n > CP_UNW_CHUNK) return cp_fail(h, CP_ERR_INVALID, "production chunk above CP_UNW_CHUNK points");
   const int blocks = unw_blocks(h);
   int rc = cp_ensure_slots(h, (size_t)blocks * CP_UNW_SLOT);
   if (rc) return rc;
-  if (n > (1ull << 32)) return cp_fail(h, CP_ERR_INVALID, "at most 2^32 points per production call");
   point0 += h->point_offset;
   UnwLaunch L;
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.nb = h->nb;
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;
   L.out = reinterpret_cast<CpEventRec*>(out);
-  L.capacity = capacity; L.counter = h->d_counter; L.slots = h->d_slots;
-  L.pdf = nullptr;
+  L.capacity = capacity; L.slots = h->d_slots;
+  L.pdf = nullptr; L.tails = nullptr; L.bcount = nullptr; L.roff = nullptr; L.rsum = nullptr;
+  L.nblk = (n + 31) / 32;
+  L.nrange = (L.nblk + CP_UNW_RANGE - 1) / CP_UNW_RANGE;
   L.scalew = scalew;
   if (capacity) {
-    if (capacity > h->pdfbuf_cap) {
-      if (h->d_pdfbuf) {
-        CP_CUDA(h, cudaStreamSynchronize(h->stream));
-        CP_CUDA(h, cudaFree(h->d_pdfbuf));
-        h->d_pdfbuf = nullptr;
-        h->pdfbuf_cap = 0;
-      }
-      CP_CUDA(h, cudaMalloc(&h->d_pdfbuf, sizeof(float4) * 4 * capacity));
-      h->pdfbuf_cap = capacity;
-    }
-    L.pdf = h->d_pdfbuf;
+    rc = unw_staging(h, n);
+    if (rc) return rc;
+    L.pdf = h->d_pdfbuf; L.tails = h->d_tails; L.bcount = h->d_bcount; L.roff = h->d_roff; L.rsum = h->d_rsum;
+    CP_CUDA(h, cudaMemsetAsync(h->d_rsum, 0, sizeof(unsigned) * L.nrange, h->stream));
   }
   L.flow = nullptr;
-  if (h->timing) cudaEventRecord(h->tev[0], h->stream);
   if (h->flow_on) {
-    rc = cp_flow_buffer(h, n);
-    if (rc) return rc;
-    rc = cp_flow_forward_enqueue(h, point0, n, iter, 0, h->d_flow_buf);
-    if (rc) return rc;
-    L.flow = h->d_flow_buf;
+    if (flow_pre) {
+      L.flow = flow_pre;
+    } else {
+      rc = cp_flow_buffer(h, n);
+      if (rc) return rc;
+      rc = cp_flow_forward_enqueue(h, point0, n, iter, 0, h->d_flow_buf);
+      if (rc) return rc;
+      L.flow = h->d_flow_buf;
+    }
   }
-  if (h->timing) cudaEventRecord(h->tev[1], h->stream);
+  cudaEvent_t* ev = (h->timing && tslot >= 0 && h->tpool.size() >= 2 + 3 * (size_t)(tslot + 1)) ? &h->tpool[2 + 3 * tslot] : nullptr;
+  if (ev) cudaEventRecord(ev[0], h->stream);
   k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
   CP_LAUNCH_CHECK(h, "k_unw_accept");
-  if (h->timing) cudaEventRecord(h->tev[2], h->stream);
+  if (ev) cudaEventRecord(ev[1], h->stream);
   k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
   if (capacity) {
+    k_unw_scan<<<1, 1024, 0, h->stream>>>(h->d_rsum, L.nrange, base_dev, h->d_roff);
+    CP_LAUNCH_CHECK(h, "k_unw_scan");
     if (L.scalew) k_unw_build<true><<<build_blocks(h, true), CP_THREADS, 0, h->stream>>>(h->P, L);
     else k_unw_build<false><<<build_blocks(h, false), CP_THREADS, 0, h->stream>>>(h->P, L);
     CP_LAUNCH_CHECK(h, "k_unw_build");
   }
-  if (h->timing) {
-    cudaEventRecord(h->tev[3], h->stream);
-    if (cudaEventSynchronize(h->tev[3]) == cudaSuccess) {
-      float a = 0.f, b = 0.f, c = 0.f;
-      cudaEventElapsedTime(&a, h->tev[0], h->tev[1]);
-      cudaEventElapsedTime(&b, h->tev[1], h->tev[2]);
-      cudaEventElapsedTime(&c, h->tev[2], h->tev[3]);
-      h->t_ms[0] += a; h->t_ms[1] += b; h->t_ms[2] += c;
-      h->t_launches[0] += h->flow_on ? 1 : 0; h->t_launches[1] += 1; h->t_launches[2] += capacity ? 1 : 0;
-    }
-  }
+  if (ev) cudaEventRecord(ev[2], h->stream);
   return CP_OK;
+}
+
+// sums of the chunks of a pass: every entry added, the largest weight (entry 2) by max
+static void combine_chunks(const double* hred, uint64_t nsub, double tot[8])
+{
+  for (int k = 0; k < 8; ++k) tot[k] = 0.0;
+  for (uint64_t c = 0; c < nsub; ++c)
+    for (int k = 0; k < 8; ++k) tot[k] = (k == 2) ? (hred[8 * c + k] > tot[k] ? hred[8 * c + k] : tot[k]) : tot[k] + hred[8 * c + k];
 }
 
 static void fill_unw(const double* red, double n, double wmax, cp_unweight_result* o)
@@ -335,17 +466,47 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   CP_CUDA(h, cudaMemcpyAsync(wm, h->d_wmax, sizeof wm, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: no threshold (cp_weight_quantile or cp_set_wmax)");
-  CP_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), h->stream));
+  if (n_points > (1ull << 32)) return cp_fail(h, CP_ERR_INVALID, "at most 2^32 points per production call");
   if (h->scalew && capacity > h->scalew_cap)
     return cp_fail(h, CP_ERR_INVALID, "cp_unweight: record capacity exceeds the scale-weight buffer (cp_set_scale_weights)");
-  int rc = unweight_enqueue(h, 0, n_points, iter, records_dev, capacity, h->d_red, h->scalew);
+  // chunks of at most CP_UNW_CHUNK points; the running record count (d_counter) places each
+  // chunk's records after the previous chunk's
+  const uint64_t nsub = (n_points + CP_UNW_CHUNK - 1) / CP_UNW_CHUNK;
+  if (nsub > h->unw_red_cap) {
+    CP_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (h->d_unw_red) CP_CUDA(h, cudaFree(h->d_unw_red));
+    h->d_unw_red = nullptr;
+    h->unw_red_cap = 0;
+    CP_CUDA(h, cudaMalloc(&h->d_unw_red, sizeof(double) * 8 * nsub));
+    h->unw_red_cap = nsub;
+  }
+  int rc = timing_reserve(h, nsub);
   if (rc) return rc;
-  double red[8];
+  CP_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), h->stream));
+  // the flow forward once for the whole pass (16 B per point), then the chunks
+  if (h->flow_on) {
+    rc = cp_flow_buffer(h, n_points);
+    if (rc) return rc;
+    if (h->timing) cudaEventRecord(h->tpool[0], h->stream);
+    rc = cp_flow_forward_enqueue(h, h->point_offset, n_points, iter, 0, h->d_flow_buf);
+    if (rc) return rc;
+    if (h->timing) cudaEventRecord(h->tpool[1], h->stream);
+  }
+  for (uint64_t c = 0; c < nsub; ++c) {
+    const uint64_t p0 = c * CP_UNW_CHUNK, n = p0 + CP_UNW_CHUNK <= n_points ? CP_UNW_CHUNK : n_points - p0;
+    rc = unweight_enqueue(h, p0, n, iter, records_dev, capacity, h->d_unw_red + 8 * c, h->scalew, h->d_counter,
+                          h->flow_on ? h->d_flow_buf + p0 : nullptr, (int)c);
+    if (rc) return rc;
+  }
+  std::vector<double> hred(8 * nsub, 0.0);
   unsigned long long cnt = 0;
-  CP_CUDA(h, cudaMemcpyAsync(red, h->d_red, sizeof red, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaMemcpyAsync(hred.data(), h->d_unw_red, sizeof(double) * 8 * nsub, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaMemcpyAsync(&cnt, h->d_counter, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  timing_collect(h, nsub, h->flow_on != 0, capacity > 0);
   if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
+  double red[8];
+  combine_chunks(hred.data(), nsub, red);
   if (out) fill_unw(red, (double)n_points, wm[0], out);
   if (cnt > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_unweight: record buffer too small (n_accepted reported)");
   if (red[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
@@ -412,6 +573,7 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: no threshold");
   if (chunk > n_points) chunk = n_points;
+  if (chunk > CP_UNW_CHUNK) chunk = CP_UNW_CHUNK;
   const uint64_t nchunks = (n_points + chunk - 1) / chunk;
   // a chunk accepts at most every point: staging slots = chunk
   int rc = gen_reserve(h, chunk, nchunks);
@@ -444,10 +606,8 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
       const int b = (int)(c % CP_GEN_BUFS);
       const uint64_t p0 = c * chunk, n = (p0 + chunk <= n_points) ? chunk : n_points - p0;
       if (c >= CP_GEN_BUFS && (e = cudaStreamWaitEvent(h->stream, h->gen_copied[b], 0)) != cudaSuccess) break;
-      unsigned long long* saved = h->d_counter;
-      h->d_counter = h->d_gen_cnt + c;
-      rc = unweight_enqueue(h, p0, n, iter, h->d_gen_stage + (uint64_t)b * chunk, chunk, h->d_gen_red + 8 * c);
-      h->d_counter = saved;
+      rc = unweight_enqueue(h, p0, n, iter, h->d_gen_stage + (uint64_t)b * chunk, chunk, h->d_gen_red + 8 * c,
+                            nullptr, h->d_gen_cnt + c, nullptr, -1);
       if (rc) break;
       k_gen_count<<<1, 1, 0, h->stream>>>(h->d_gen_cnt + c, dcnt_mapped + c);
       if ((e = cudaGetLastError()) != cudaSuccess) break;
@@ -467,9 +627,8 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   if (e != cudaSuccess) return cp_fail_cuda(h, e, "cp_generate_host");
   if (rc) return rc;
   if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
-  double tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (uint64_t c = 0; c < nchunks; ++c)
-    for (int k = 0; k < 8; ++k) tot[k] = (k == 2) ? (hred[8 * c + k] > tot[k] ? hred[8 * c + k] : tot[k]) : tot[k] + hred[8 * c + k];
+  double tot[8];
+  combine_chunks(hred.data(), nchunks, tot);
   if (out) fill_unw(tot, (double)n_points, wm[0], out);
   if (total_acc > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_generate_host: record buffer too small");
   if (tot[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
@@ -495,8 +654,6 @@ extern "C" int cp_set_scale_weights(cp_handle* h, float* weights_dev, uint64_t c
 extern "C" int cp_set_kernel_timing(cp_handle* h, int on)
 {
   CP_CHECK_HANDLE(h);
-  if (on && !h->tev[0])
-    for (int k = 0; k < 4; ++k) CP_CUDA(h, cudaEventCreate(&h->tev[k]));
   h->timing = on ? 1 : 0;
   return CP_OK;
 }

@@ -1,10 +1,11 @@
 // cub_compaction -- stage driver of the accepted-event compaction
 // (cuPythia/10_cub_compaction/cub_compaction.cu:59-100): same argv (number of candidates),
 // VALIDATION line and exit codes.  The reference flags candidates and runs a library
-// DeviceSelect; here the production pass compacts on the device as it accepts (one ballot and
-// one atomic per warp).  Validation: the number of records equals an independent recount of
-// u w_max < w over the same points (weights from cp_point_weights, u from the Philox words),
-// up to FP32 evaluation differences of 1 in 10^5, and every record's point index is distinct.
+// DeviceSelect; here the production pass compacts on the device as it accepts (per-block counts,
+// one scan, records in point order like DeviceSelect's).  Validation: the number of records
+// equals an independent recount of u w_max < w over the same points (weights from
+// cp_point_weights, u from the Philox words), up to FP32 evaluation differences of 1 in 10^5,
+// and the records' point indices increase strictly (distinct, in point order).
 //   Run: cub_compaction [nCandidates=16777216]
 #include <algorithm>
 #include <vector>
@@ -58,17 +59,17 @@ int main(int argc, char** argv)
   }
   std::vector<uint32_t> pts(u.n_accepted);
   for (uint64_t i = 0; i < u.n_accepted; ++i) pts[i] = rec[i].point;
-  std::sort(pts.begin(), pts.end());
-  const bool distinct = std::adjacent_find(pts.begin(), pts.end()) == pts.end();
+  // strictly increasing: distinct points, in the point order of the reference's selection
+  const bool distinct = std::adjacent_find(pts.begin(), pts.end(), [](uint32_t a, uint32_t b) { return b <= a; }) == pts.end();
   const uint64_t diff = u.n_accepted > recount ? u.n_accepted - recount : recount - u.n_accepted;
   printf("On-device compaction of accepted events (%llu candidates, w_max = q99.9 = %.4e mb)\n",
          (unsigned long long)n, wmax);
-  printf("  accepted (compacted) = %llu   independent recount = %llu   records distinct: %s\n",
+  printf("  accepted (compacted) = %llu   independent recount = %llu   records in point order: %s\n",
          (unsigned long long)u.n_accepted, (unsigned long long)recount, distinct ? "yes" : "no");
   printf("  production pass %.2f ms  (%.3e candidates/s, %.3e records/s)\n", drv_ms(t0, t1),
          n / (drv_ms(t0, t1) / 1e3), u.n_accepted / (drv_ms(t0, t1) / 1e3));
   const bool ok = distinct && u.n_accepted > 0 && diff <= std::max<uint64_t>(2, n / 100000);
-  printf("VALIDATION: %s (compacted count == independent count, records distinct)\n", ok ? "PASS" : "FAIL");
+  printf("VALIDATION: %s (compacted count == independent count, records in point order)\n", ok ? "PASS" : "FAIL");
   cudaFree(d_rec);
   cudaFree(d_w);
   cudaFree(d_words);

@@ -228,8 +228,11 @@ int cp_set_wmax(cp_handle* h, double w_max);
  * integrand -> accept (u w_max < w; overweight events kept with weight w / w_max) -> compaction
  * of accepted events into records_dev (capacity records).  Replaces the unweighting kernels
  * (cuPythia/07_unweighting_lhe/unweight_lhe.cu:42-57, cuPythia/pipeline/generate.cu:56-62) and
- * the flag + library compaction (cuPythia/10_cub_compaction/cub_compaction.cu:36-46,76-80).
- * Returns CP_ERR_CAPACITY (with the counts filled in) when more events were accepted than fit. */
+ * the flag + library compaction (cuPythia/10_cub_compaction/cub_compaction.cu:36-46,76-80),
+ * with the same output order: the records of the accepted points in point order, the same on
+ * every run.  Returns CP_ERR_CAPACITY (with the counts filled in) when more events were accepted
+ * than fit; the first `capacity` records in point order are stored.  Device staging: 80 bytes per
+ * point of a chunk of at most 2^24 points (1.3 GB), kept in the handle. */
 int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_event* records_dev,
                 uint64_t capacity, cp_unweight_result* out_host);
 /* Scale-variation weights (the fused reweighting of cuPythia/pipeline/reweight.cu:36-51 and
@@ -243,7 +246,8 @@ int cp_set_scale_weights(cp_handle* h, float* weights_dev, uint64_t capacity);
 /* The same production pass delivering the records to HOST memory (pinned for overlap), in
  * chunks of `chunk` points whose device-to-host copies overlap the following chunks' compute
  * (the handle keeps 3 staging buffers of `chunk` records; 2^21 points per chunk keeps the copy
- * engine busy back to back).  Every copy has finished when the call returns. */
+ * engine busy back to back; at most 2^24).  The records arrive in point order, byte-identical
+ * to cp_unweight's.  Every copy has finished when the call returns. */
 int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t chunk,
                      cp_event* records_host, uint64_t capacity, cp_unweight_result* out_host);
 
@@ -379,8 +383,9 @@ int cp_write_lhef(const cp_config* cfg, const cp_event* events_host, uint64_t n,
                   double sigma_err_mb, const char* path);
 
 /* ---------------------------------------------------------------- measurement ------ */
-/* Per-kernel CUDA-event timing of the production pass (cp_unweight / cp_generate_host): slot 0
- * the flow forward, 1 the accept kernel, 2 the record builder (with the slot reduction).
+/* Per-kernel CUDA-event timing of cp_unweight: slot 0 the flow forward, 1 the accept kernel,
+ * 2 the record builder (with the slot reduction and the output-offset scan), summed over the
+ * pass's chunks; launches3 counts the passes that ran each kernel.
  * No reference counterpart (the reference times whole stages with a host clock,
  * cuPythia/03_fused_resident_me/fused_gg2gg.cu:93-100). */
 int cp_set_kernel_timing(cp_handle* h, int on);

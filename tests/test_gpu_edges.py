@@ -63,8 +63,9 @@ def test_ragged_production_matches_its_recount():
     ev = cp.events_view(rec)
     u = (words[:, 3] >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
     expect = np.nonzero(u * np.float32(wq) < w)[0]
-    pts = np.sort(ev["point"].astype(np.int64))
-    assert len(np.unique(pts)) == len(pts) == st["n_accepted"]
+    pts = ev["point"].astype(np.int64)
+    assert np.all(np.diff(pts) > 0)   # point order
+    assert len(pts) == st["n_accepted"]
     assert pts.max() < n
     assert len(np.setxor1d(expect, pts)) <= 2
 
@@ -84,7 +85,7 @@ def test_ragged_host_chunks_match_the_device_pass():
     assert st2["n_accepted"] == st["n_accepted"]
     a = cp.events_view(rec)
     b = cp.events_view(host[:st2["n_accepted"]])
-    assert a[np.argsort(a["point"])].tobytes() == b[np.argsort(b["point"])].tobytes()
+    assert a.tobytes() == b.tobytes()   # the same records in the same (point) order
 
 
 def test_tiny_passes_and_size_limits(integ):
@@ -130,22 +131,20 @@ def test_host_generation_capacity_and_staging_reuse():
         it.weight_quantile(0.999)
         rec, st = it.unweight(n, iteration=51)
         dev = cp.events_view(rec)
-        by_point = {int(e["point"]): e.tobytes() for e in dev}
         k = st["n_accepted"]
         small = torch.zeros((k // 3, 64), dtype=torch.uint8, pin_memory=True)
         res = cp._lib.cp_unweight_result()
         rc = it.lib.cp_generate_host(it.h, n, 51, 1 << 14, C.c_void_p(small.data_ptr()), small.shape[0], C.byref(res))
         assert rc == cp._lib.CP_ERR_CAPACITY and res.n_accepted == k
         got = cp.events_view(small)
-        assert len(np.unique(got["point"])) == len(got)
-        assert all(by_point[int(e["point"])] == e.tobytes() for e in got)
+        assert got.tobytes() == dev[:len(got)].tobytes()   # the first records in point order
         full = torch.empty((k + 8, 64), dtype=torch.uint8, pin_memory=True)
         for chunk in (1 << 17, 1 << 12, 100001):
             full.zero_()
             st2 = it.generate_host(n, full, iteration=51, chunk=chunk)
             assert st2["n_accepted"] == k
             h = cp.events_view(full[:k])
-            assert dev[np.argsort(dev["point"])].tobytes() == h[np.argsort(h["point"])].tobytes(), chunk
+            assert dev.tobytes() == h.tobytes(), chunk
         # the flow as proposal: its forward pass runs per chunk on the same handle
         it.flow_init(7)
         it.flow_train(10, 65536, lr=8e-3)
@@ -159,4 +158,4 @@ def test_host_generation_capacity_and_staging_reuse():
     assert st3["n_accepted"] == st_f["n_accepted"]
     a = cp.events_view(rec_f)
     b = cp.events_view(host_f[:st3["n_accepted"]])
-    assert a[np.argsort(a["point"])].tobytes() == b[np.argsort(b["point"])].tobytes()
+    assert a.tobytes() == b.tobytes()
