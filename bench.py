@@ -160,7 +160,7 @@ FP32_FLOP_PER_POINT = 3278.0      # k_unw_accept: FADD + FMUL + 2 FFMA per point
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
 # launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points
-TRAFFIC_PER_POINT = {"k_unw_accept": (508976640 + 708100352) / 2 ** 24,
+TRAFFIC_PER_POINT = {"k_unw_accept": (276745216 + 575733760) / 2 ** 24,
                      "k_flow_fwd_tc": (108544 + 209209344) / 2 ** 24}
 
 
