@@ -210,10 +210,12 @@ __global__ void __launch_bounds__(1024) k_unw_scan(const unsigned* __restrict__ 
   if (t == 0) *base_io = carry;
 }
 
-// K2: one warp per 1024-point range (32 blocks): the lanes' block counts, scanned across the
-// warp, spread the range's accepted points over the lanes in point order; each lane re-evaluates
-// its point's kinematics (the PDFs come from K1's staging), picks process, flavours and colour
-// flow, builds the lab-frame kinematics and stores the full 64-byte record at its output index.
+// K2: work units of a quarter range (8 blocks, 256 points: 65,536 per 2^24-point chunk, so the
+// warps' shares differ by about 1%).  A warp loads its range's 32 block counts, scans them with
+// shuffles and spreads the accepted points of its quarter over the lanes in point order; each
+// lane re-evaluates its point's kinematics (the PDFs come from K1's staging), picks process,
+// flavours and colour flow, builds the lab-frame kinematics and stores the full 64-byte record
+// at its output index.
 // 4 resident blocks per SM without scale weights (64 registers), 2 with them
 template <bool SCALEW>
 __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const CpHadParams P, const UnwLaunch L)
@@ -225,7 +227,9 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = (uint64_t)gridDim.x * (CP_THREADS / 32);
-  for (uint64_t R = ((uint64_t)blockIdx.x * CP_THREADS + threadIdx.x) >> 5; R < L.nrange; R += nwarps) {
+  for (uint64_t U = ((uint64_t)blockIdx.x * CP_THREADS + threadIdx.x) >> 5; U < 4 * L.nrange; U += nwarps) {
+    const uint64_t R = U >> 2;
+    const int quarter = (int)(U & 3);
     const uint64_t blk = R * CP_UNW_RANGE + lane;
     const unsigned c = blk < L.nblk ? (unsigned)L.bcount[blk] : 0u;
     unsigned incl = c;
@@ -235,9 +239,11 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
       if (lane >= o) incl += v;
     }
     const unsigned excl = incl - c;
-    const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+    // this quarter's entries of the range: [first, total)
+    const unsigned first = __shfl_sync(0xffffffffu, excl, 8 * quarter);
+    const unsigned total = __shfl_sync(0xffffffffu, incl, 8 * quarter + 7);
     const unsigned long long base = L.roff[R];
-    for (unsigned j0 = 0; j0 < total; j0 += 32) {
+    for (unsigned j0 = first; j0 < total; j0 += 32) {
       const unsigned j = j0 + lane;
       // this lane's entry lies in the first block whose inclusive count exceeds j
       int b = 0;
