@@ -156,6 +156,7 @@ def measured_peaks():
 
 # --------------------------------------------------------------------------- our arm
 # algorithmic work per point of the two dominant kernels
+UNW_CHUNK = 1 << 24               # points per production chunk of the library (accept/scan/build launches)
 FP32_FLOP_PER_POINT = 3278.0      # k_unw_accept: FADD + FMUL + 2 FFMA per point (ncu SASS counters, profiles/)
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
@@ -382,7 +383,9 @@ def run_ours(a):
                 "d2h_bytes_per_step": int(d2h / e2e_steps),
                 "d2h_copy_gbs": d2h_gbs, "events_per_s_at_copy_rate": d2h_gbs * 1e9 / RECORD_BYTES,
                 "d2h_seconds_per_step": d2h / e2e_steps / (d2h_gbs * 1e9)},
-        "gpu_launches": 4 * a.steps,
+        # per step: the flow forward once, then per 2^24-point chunk the accept kernel, the slot
+        # reduction, the output-offset scan and the record builder
+        "gpu_launches": a.steps * ((1 if use_flow else 0) + 4 * ((n + UNW_CHUNK - 1) // UNW_CHUNK)),
         "roofline": roof, "roofline_secondary": roof2,
         "mufu_peak_tops": mufu_peak,
         "clocks": clk.summary(),
