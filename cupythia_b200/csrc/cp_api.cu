@@ -154,7 +154,7 @@ extern "C" int cp_destroy(cp_handle* h)
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
                   h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq, h->d_flow, h->d_flow_pk,
                   h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_pdfbuf,
-                  h->d_gen_stage, h->d_gen_red, h->d_gen_cnt, h->d_ftrain, h->d_tails, h->d_bcount,
+                  h->d_gen_stage, h->d_gen_red, h->d_gen_cnt, h->d_ftrain, h->d_tails, h->d_bmask,
                   h->d_rsum, h->d_roff, h->d_unw_red};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -511,17 +511,6 @@ extern "C" int cp_pdf_batch(cp_handle* h, const float* x, const float* q2, int64
 // ------------------------------------------------------------------------------------------
 // partonic gg -> gg, FP64 (cuPythia/03_fused_resident_me/fused_gg2gg.cu:28-51)
 // ------------------------------------------------------------------------------------------
-__device__ __forceinline__ double cp_gg2gg_d(double sH, double tH, double uH, double aS)
-{
-  // reciprocal-precompute form of Sigma2gg2gg::sigmaKin (pipeline/physics.cuh:9-16)
-  double is = 1.0 / sH, it = 1.0 / tH, iu = 1.0 / uH;
-  double rts = tH * is, rst = sH * it, rus = uH * is, rsu = sH * iu, rtu = tH * iu, rut = uH * it;
-  double a = 2.25 * (rts * rts + 2. * rts + 3. + 2. * rst + rst * rst);
-  double b = 2.25 * (rus * rus + 2. * rus + 3. + 2. * rsu + rsu * rsu);
-  double c = 2.25 * (rtu * rtu + 2. * rtu + 3. + 2. * rut + rut * rut);
-  return (M_PI * is * is) * (aS * aS) * 0.5 * (a + b + c);
-}
-
 struct PartonicArgs {
   double s, aS, cMax, scale;  // scale = (2 cMax)(s/2) conv
   uint64_t seed, p0, n;       // Philox mode: points; SplitMix mode: reference threads
@@ -530,33 +519,69 @@ struct PartonicArgs {
   double* w_out;
 };
 
-__device__ __forceinline__ double partonic_w(const PartonicArgs& a, double u)
+// Sigma2gg2gg::sigmaKin (pythia8317/src/SigmaQCD.cc:115-129; pipeline/physics.cuh:9-16) for a fixed
+// s-hat.  With s + t + u = 0 the three brackets sigTS + sigUS + sigTU sum to
+// (9/2) (3 - t u / s^2 - s u / t^2 - s t / u^2), the textbook form of the g g -> g g matrix element,
+// which takes one FP64 reciprocal (of t u; 1/t = u / (t u), 1/u = t / (t u)) and about half the
+// operations of the bracket form.  With u = -s - t rounded as the reference rounds it, the two
+// forms agree to 1.1e-15 relative over |cos theta| < 0.9.  The prefactor (pi / s^2) alpha_s^2 / 2
+// is the same for every draw and is formed once.
+struct CpGG2GG {
+  double s, is2, pre, cMax;
+  __device__ __forceinline__ CpGG2GG(double s_, double aS, double cMax_) : s(s_), cMax(cMax_)
+  {
+    const double is = 1.0 / s;
+    is2 = is * is;
+    pre = M_PI * is * is * (aS * aS) * 0.5 * 4.5;
+  }
+  // dsigma/dt at cos theta = (2 u01 - 1) cMax
+  __device__ __forceinline__ double operator()(double u01) const
+  {
+    const double c = (2.0 * u01 - 1.0) * cMax;
+    const double tH = -0.5 * s * (1.0 - c), uH = -s - tH;
+    const double tu = tH * uH, itu = 1.0 / tu;
+    const double it = uH * itu, iu = tH * itu;
+    return pre * (3.0 - tu * is2 - (s * uH) * (it * it) - (s * tH) * (iu * iu));
+  }
+};
+
+__device__ __forceinline__ double cp_philox_u01_d(uint64_t seed, uint64_t point)
 {
-  double c = (2.0 * u - 1.0) * a.cMax;
-  double t = -0.5 * a.s * (1.0 - c);
-  return cp_gg2gg_d(a.s, t, -a.s - t, a.aS) * a.scale;
+  uint32_t wd[4];
+  cp_point_words(seed, point, 0, 0, wd);
+  const uint64_t v = ((uint64_t)wd[1] << 32) | wd[0];
+  return (double)(v >> 11) * (1.0 / 9007199254740992.0);
 }
 
-template <int MODE>  // 0 Philox sums, 1 SplitMix sums, 2 Philox per-point weights
-__global__ void __launch_bounds__(CP_THREADS) k_partonic(const PartonicArgs a)
+// MODE 0: Philox sums over points; 1: SplitMix64 sums over the reference's (thread, draw) pairs;
+// 2: Philox per-point weights.  Sums are of dsigma/dt; each block scales its slot by `scale`.
+template <int MODE>
+__global__ void __launch_bounds__(CP_THREADS, 5) k_partonic(const PartonicArgs a)
 {
   __shared__ double sRed[CP_WARPS][3];
+  const CpGG2GG f(a.s, a.aS, a.cMax);
   double s1 = 0.0, s2 = 0.0, wm = 0.0;
-  const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
-  for (uint64_t i = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x; i < a.n; i += stride) {
-    if (MODE == 1) {
-      uint64_t ctr = a.seed + i * 0x100000001B3ULL;
-      for (uint64_t k = 0; k < a.kper; ++k) {
-        double w = partonic_w(a, cp_u01(cp_splitmix64(ctr++)));
-        s1 += w; s2 += w * w; wm = fmax(wm, w);
-      }
-    } else {
-      uint32_t wd[4];
-      cp_point_words(a.seed, a.p0 + i, 0, 0, wd);
-      uint64_t v = ((uint64_t)wd[1] << 32) | wd[0];
-      double w = partonic_w(a, (double)(v >> 11) * (1.0 / 9007199254740992.0));
-      if (MODE == 2) a.w_out[i] = w;
-      s1 += w; s2 += w * w; wm = fmax(wm, w);
+  const uint64_t nthr = (uint64_t)gridDim.x * CP_THREADS;
+  const uint64_t t = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x;
+  if (MODE == 1) {
+    // the reference's thread i makes draws k = 0 .. kper-1 from counter seed + i 0x100000001B3 + k
+    // (cuPythia/03_fused_resident_me/fused_gg2gg.cu:43-50); the n kper pairs are split into
+    // equal contiguous shares, so every thread here does the same number of draws
+    const uint64_t total = a.n * a.kper, q = total / nthr, rem = total % nthr;
+    const uint64_t w0 = q * t + (t < rem ? t : rem), cnt = q + (t < rem ? 1 : 0);
+    uint64_t i = w0 / a.kper, k = w0 - i * a.kper;
+    uint64_t ctr = a.seed + i * 0x100000001B3ULL + k;
+    for (uint64_t w = 0; w < cnt; ++w) {
+      const double v = f(cp_u01(cp_splitmix64(ctr)));
+      s1 += v; s2 += v * v; wm = fmax(wm, v);
+      if (++k == a.kper) { k = 0; ++i; ctr = a.seed + i * 0x100000001B3ULL; }
+      else ++ctr;
+    }
+  } else {
+    for (uint64_t i = t; i < a.n; i += nthr) {
+      const double v = f(cp_philox_u01_d(a.seed, a.p0 + i));
+      if (MODE == 2) { a.w_out[i] = v * a.scale; continue; }
+      s1 += v; s2 += v * v; wm = fmax(wm, v);
     }
   }
   if (MODE == 2) return;
@@ -570,14 +595,19 @@ __global__ void __launch_bounds__(CP_THREADS) k_partonic(const PartonicArgs a)
     double b1 = 0, b2 = 0, bm = 0;
     for (int k = 0; k < CP_WARPS; ++k) { b1 += sRed[k][0]; b2 += sRed[k][1]; bm = fmax(bm, sRed[k][2]); }
     double* slot = a.slots + 4 * (size_t)blockIdx.x;
-    slot[0] = b1; slot[1] = b2; slot[2] = bm; slot[3] = 0.0;
+    slot[0] = b1 * a.scale; slot[1] = b2 * (a.scale * a.scale); slot[2] = bm * a.scale; slot[3] = 0.0;
   }
 }
 
 static int partonic_run(cp_handle* h, int mode, PartonicArgs a, uint64_t npoints, cp_result* out)
 {
   if (!(a.s > 0) || !(a.cMax > 0) || !(a.cMax < 1)) return cp_fail(h, CP_ERR_INVALID, "partonic: bad kinematics");
-  int blocks = h->num_sms * 4;
+  // one wave of resident blocks: the per-thread shares are equal, so nothing waits on a tail
+  int per_sm = 0;
+  const cudaError_t oe = mode == 0 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_partonic<0>, CP_THREADS, 0)
+                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_partonic<1>, CP_THREADS, 0);
+  if (oe != cudaSuccess || per_sm < 1) per_sm = 4;
+  const int blocks = h->num_sms * per_sm;
   int rc = cp_ensure_slots(h, (size_t)blocks * 4);
   if (rc) return rc;
   a.slots = h->d_slots;
@@ -615,6 +645,7 @@ extern "C" int cp_partonic_splitmix(cp_handle* h, double sqrt_shat, double alpha
                                     cp_result* out)
 {
   CP_CHECK_HANDLE(h);
+  if (kper && nthr > UINT64_MAX / kper) return cp_fail(h, CP_ERR_INVALID, "too many draws");
   if (nthr * kper < 2) return cp_fail(h, CP_ERR_INVALID, "too few draws");
   double s = sqrt_shat * sqrt_shat;
   PartonicArgs a{s, alphas, cmax, (2.0 * cmax) * (s / 2.0) * conv, seed, 0, nthr, kper, nullptr, nullptr};

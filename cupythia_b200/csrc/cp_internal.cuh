@@ -116,11 +116,11 @@ struct cp_handle {
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
   unsigned long long* d_counter = nullptr; // accepted-event counter
-  // production staging for pdfbuf_cap points (K1 -> K2): PDFs and record tails per point, accepted
-  // counts per 32-point block, totals and output offsets per 1024-point range; per-chunk sums
+  // production staging for pdfbuf_cap points (K1 -> K2): PDFs and record tails per point, accept
+  // masks per 32-point block, totals and output offsets per 1024-point range; per-chunk sums
   float4* d_pdfbuf = nullptr;
   uint4* d_tails = nullptr;
-  uint8_t* d_bcount = nullptr;
+  unsigned* d_bmask = nullptr;
   unsigned* d_rsum = nullptr;
   unsigned long long* d_roff = nullptr;
   uint64_t pdfbuf_cap = 0;

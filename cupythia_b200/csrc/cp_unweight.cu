@@ -3,15 +3,16 @@
 // K1 draws, maps and evaluates each point exactly like the VEGAS pass and accepts it when
 // u * w_max < w (cuPythia/07_unweighting_lhe/unweight_lhe.cu:54; overweight events w > w_max
 // are kept with weight w / w_max, as Pythia keeps them, pythia8317/src/ProcessContainer.cc:
-// 383-385).  Per 32-point block (one warp's points) it stores the number accepted and adds it to
-// its 1024-point range's total (an integer atomic: exact in any order), and packs the accepted
-// points' record tails and 16 PDF values, in point order, at the front of the block's staging
-// slots.  A one-block scan of the range totals gives each range's output offset, so the records
+// 383-385).  Per 32-point block (one warp's points) it stores the warp's accept mask and adds
+// the number accepted to its 1024-point range's total (an integer atomic: exact in any order),
+// and packs the accepted points' event weights, mapped coordinates and 16 PDF values, in point
+// order, at the front of the block's staging slots.  A one-block scan of the range totals gives each range's output offset, so the records
 // come out in point order, exactly as the reference's library compaction orders them
 // (cub::DeviceSelect::Flagged, cuPythia/10_cub_compaction/cub_compaction.cu:76-80,
 // cuPythia/pipeline/generate.cu:97-104), without any block waiting on another.  K2 takes one
-// range per warp, spreads its accepted points over the lanes (every lane busy), recomputes the
-// points' kinematics and brackets (the PDFs come from K1), picks process, flavours and colour
+// range per warp, spreads its accepted points over the lanes (every lane busy), takes each one's
+// point index from its block's mask, recomputes the points' kinematics and brackets from the
+// staged coordinates (the PDFs come from K1 too), picks process, flavours and colour
 // flow, and writes the 64-byte records as four 16-byte stores (and, on request, the 7-point
 // scale-variation ratios).  Keeping the record builder out of K1 keeps K1's code small and its
 // lanes converged.  Staging grows with the points of a pass, so passes run in chunks of at most
@@ -36,15 +37,15 @@ struct UnwLaunch {
   const double* wmax;          // device threshold
   CpEventRec* out;
   float4* pdf;                 // staging per point: fa[8], fb[8] of the accepted points (K1 -> K2)
-  uint4* tails;                // staging per point: the record's last 16 bytes, or null (no records)
-  uint8_t* bcount;             // accepted points per 32-point block
+  uint4* tails;                // staging per point: event weight and x[3] (bits), or null (no records)
+  unsigned* bmask;             // accept mask of each 32-point block (bit = lane = point - 32 block)
   unsigned* rsum;              // accepted points per 1024-point range (zeroed before K1)
   const unsigned long long* roff;   // output index of the first record of each range
   uint64_t nblk, nrange;
   float* scalew;               // per record: 6 scale-variation ratios, or null
   uint64_t capacity;
   double* slots;
-  const float4* flow;          // flow output (v, ln J) per in-call point, or null
+  const float4* flow;          // flow output (v, ln J) per in-call point, or null (K1 only)
 };
 
 static_assert(sizeof(CpEventRec) == 64, "event record must be 64 bytes");
@@ -118,10 +119,11 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
     bool accept = false;
     float w = 0.f;
     CpPoint pt;
+    CpMapped m{};
     if (p < L.n) {
       uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
-      CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
+      m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
       w = cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt) * m.jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
       cp_kahan(s1, c1, w);
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
     // the warp's 32 points are one block: p0 is a multiple of 32 (stride and block slices are)
     const uint64_t p0 = p - (uint64_t)lane;
     if (L.tails && lane == 0 && p0 < L.n) {
-      L.bcount[p0 >> 5] = (uint8_t)__popc(ball);
+      L.bmask[p0 >> 5] = ball;
       if (ball) atomicAdd(&L.rsum[p0 >> 10], (unsigned)__popc(ball));   // integer sum: order-free
     }
     if (accept) {
@@ -143,8 +145,10 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
       cp_kahan(se, ce, ew);
       if (L.tails) {
         const uint64_t q = p0 + (uint64_t)__popc(ball & ((1u << lane) - 1u));
-        // weight, pt_hat, process, point: the last 16 bytes of the record
-        L.tails[q] = make_uint4(__float_as_uint(ew), 0u, 0u, (uint32_t)p);
+        // the event weight and the point's coordinates after the map (and flow): the record
+        // builder starts from them, so it needs neither the map nor the flow output
+        L.tails[q] = make_uint4(__float_as_uint(ew), __float_as_uint(m.x[0]), __float_as_uint(m.x[1]),
+                                __float_as_uint(m.x[2]));
         // the PDFs of the point, so that the record builder need not evaluate CTEQ5L again
         float4* f = L.pdf + 4 * q;
         f[0] = make_float4(pt.fa[0], pt.fa[1], pt.fa[2], pt.fa[3]);
@@ -220,9 +224,7 @@ __global__ void __launch_bounds__(1024) k_unw_scan(const unsigned* __restrict__ 
 template <bool SCALEW>
 __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const CpHadParams P, const UnwLaunch L)
 {
-  __shared__ float2 sEdge[3][CP_MAX_BINS];
   __shared__ CpCteqPoly sCteq[8];
-  cp_stage_edges(sEdge, L.edges, L.nb);
   cp_stage_cteq(sCteq, L.cteq);
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -231,7 +233,8 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
     const uint64_t R = U >> 2;
     const int quarter = (int)(U & 3);
     const uint64_t blk = R * CP_UNW_RANGE + lane;
-    const unsigned c = blk < L.nblk ? (unsigned)L.bcount[blk] : 0u;
+    const unsigned mk = blk < L.nblk ? L.bmask[blk] : 0u;
+    const unsigned c = __popc(mk);
     unsigned incl = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -251,15 +254,22 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
       for (int st = 16; st > 0; st >>= 1)
         if (__shfl_sync(0xffffffffu, incl, b + st - 1) <= j) b += st;
       const unsigned ex = __shfl_sync(0xffffffffu, excl, b);
+      const unsigned mb = __shfl_sync(0xffffffffu, mk, b);
       const uint64_t k = base + j;   // output record
       if (j >= total || k >= L.capacity) continue;
-      const uint64_t q = (R * CP_UNW_RANGE + b) * 32 + (j - ex);   // staging slot
+      // the entry is the block's accepted point of rank r; its lane is the position of the
+      // r-th set bit of the block's mask: the largest x with fewer than r + 1 set bits below x
+      const unsigned r = j - ex;
+      int x = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1)
+        if ((unsigned)__popc(mb & ((1u << (x + st)) - 1u)) <= r) x += st;
+      const uint64_t blkq = (R * CP_UNW_RANGE + b) * 32;
+      const uint64_t q = blkq + r;   // staging slot
       const uint4 tail = L.tails[q];
-      const uint64_t point = L.point0 + tail.w;
-      uint32_t wd[4], w2[4];
-      cp_point_words(L.seed, point, L.iter, 0, wd);
+      const uint64_t point = L.point0 + blkq + (uint64_t)x;
+      uint32_t w2[4];
       cp_point_words(L.seed, point, L.iter, 1, w2);
-      CpMapped m = cp_map_any(sEdge, L.nb, wd, L.flow, tail.w);
       float pdf[16];
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
@@ -267,7 +277,7 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
         pdf[4 * f] = v.x; pdf[4 * f + 1] = v.y; pdf[4 * f + 2] = v.z; pdf[4 * f + 3] = v.w;
       }
       CpPoint pt;
-      cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt, pdf);
+      cp_had_eval(P, sCteq, __uint_as_float(tail.y), __uint_as_float(tail.z), __uint_as_float(tail.w), pt, pdf);
       CpEventRec ev;
       cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
                     cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
@@ -315,21 +325,21 @@ static int build_blocks(cp_handle* h, bool scalew)
   return h->num_sms * c;
 }
 
-// Staging of a production chunk of n points: record tails and PDFs per point, accepted counts
-// per 32-point block, totals and output offsets per 1024-point range.
+// Staging of a production chunk of n points: record tails and PDFs per point, accept masks per
+// 32-point block, totals and output offsets per 1024-point range.
 static int unw_staging(cp_handle* h, uint64_t n)
 {
   if (n <= h->pdfbuf_cap) return CP_OK;
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
-  void* old[] = {h->d_pdfbuf, h->d_tails, h->d_bcount, h->d_roff, h->d_rsum};
+  void* old[] = {h->d_pdfbuf, h->d_tails, h->d_bmask, h->d_roff, h->d_rsum};
   for (void* b : old)
     if (b) CP_CUDA(h, cudaFree(b));
-  h->d_pdfbuf = nullptr; h->d_tails = nullptr; h->d_bcount = nullptr; h->d_roff = nullptr; h->d_rsum = nullptr;
+  h->d_pdfbuf = nullptr; h->d_tails = nullptr; h->d_bmask = nullptr; h->d_roff = nullptr; h->d_rsum = nullptr;
   h->pdfbuf_cap = 0;
   const uint64_t nblk = (n + 31) / 32, nrange = (nblk + CP_UNW_RANGE - 1) / CP_UNW_RANGE;
   CP_CUDA(h, cudaMalloc(&h->d_pdfbuf, sizeof(float4) * 4 * n));
   CP_CUDA(h, cudaMalloc(&h->d_tails, sizeof(uint4) * n));
-  CP_CUDA(h, cudaMalloc(&h->d_bcount, nblk));
+  CP_CUDA(h, cudaMalloc(&h->d_bmask, sizeof(unsigned) * nblk));
   CP_CUDA(h, cudaMalloc(&h->d_roff, sizeof(unsigned long long) * nrange));
   CP_CUDA(h, cudaMalloc(&h->d_rsum, sizeof(unsigned) * nrange));
   h->pdfbuf_cap = n;
@@ -388,14 +398,14 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;
   L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.slots = h->d_slots;
-  L.pdf = nullptr; L.tails = nullptr; L.bcount = nullptr; L.roff = nullptr; L.rsum = nullptr;
+  L.pdf = nullptr; L.tails = nullptr; L.bmask = nullptr; L.roff = nullptr; L.rsum = nullptr;
   L.nblk = (n + 31) / 32;
   L.nrange = (L.nblk + CP_UNW_RANGE - 1) / CP_UNW_RANGE;
   L.scalew = scalew;
   if (capacity) {
     rc = unw_staging(h, n);
     if (rc) return rc;
-    L.pdf = h->d_pdfbuf; L.tails = h->d_tails; L.bcount = h->d_bcount; L.roff = h->d_roff; L.rsum = h->d_rsum;
+    L.pdf = h->d_pdfbuf; L.tails = h->d_tails; L.bmask = h->d_bmask; L.roff = h->d_roff; L.rsum = h->d_rsum;
     CP_CUDA(h, cudaMemsetAsync(h->d_rsum, 0, sizeof(unsigned) * L.nrange, h->stream));
   }
   L.flow = nullptr;
