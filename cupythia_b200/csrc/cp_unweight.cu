@@ -95,9 +95,9 @@ __device__ __forceinline__ void cp_stage_edges(float2 (*sEdge)[CP_MAX_BINS], con
   }
 }
 
-// K1: weight, accept; per 32-point block the accepted count (also added to its range's total),
-// and each accepted point's record tail (event weight, in-call point index) and PDFs packed at
-// the front of the block's staging slots in point order; K2 fills in the rest of the record.
+// K1: weight, accept; per 32-point block the accept mask (its popcount added to its range's
+// total), and each accepted point's event weight, coordinates and PDFs packed at the front of the
+// block's staging slots in point order; K2 builds the record from them.
 __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const CpHadParams P, const UnwLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
@@ -215,9 +215,10 @@ __global__ void __launch_bounds__(1024) k_unw_scan(const unsigned* __restrict__ 
 }
 
 // K2: work units of a quarter range (8 blocks, 256 points: 65,536 per 2^24-point chunk, so the
-// warps' shares differ by about 1%).  A warp loads its range's 32 block counts, scans them with
-// shuffles and spreads the accepted points of its quarter over the lanes in point order; each
-// lane re-evaluates its point's kinematics (the PDFs come from K1's staging), picks process,
+// warps' shares differ by about 1%).  A warp loads its range's 32 block masks, scans their
+// popcounts with shuffles and spreads the accepted points of its quarter over the lanes in point
+// order; each lane takes its point index from its block's mask, re-evaluates the point's
+// kinematics from the staged coordinates (the PDFs come from K1's staging too), picks process,
 // flavours and colour flow, builds the lab-frame kinematics and stores the full 64-byte record
 // at its output index.
 // 4 resident blocks per SM without scale weights (64 registers), 2 with them
