@@ -49,6 +49,7 @@
 #define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
 #define CP_TC_SMEM (CP_TC_S_MISC + 256 + 1024)  // mbarriers, TMEM address, abort flags, final barriers; 1024-byte base alignment slack
 #define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
+#define CP_TC_A3 32                             // slot's TMEM column of the layer-3 A operand
 #define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
 
 static_assert(CP_TC_S_H % 1024 == 0, "activation buffers must stay aligned");
@@ -175,11 +176,13 @@ __device__ __forceinline__ void cp_tc_issue_l2(uint32_t d, uint64_t a, uint64_t 
     cp_tc_mma(d, a + j * (4096 >> 4), b64 + bw + ((CP_TC_B2 + j * 2048) >> 4), CP_TC_IDESC64, j > 0 ? 1u : 0u);
   cp_tc_mma(d, ones, b64 + bw + (CP_TC_B2B >> 4), CP_TC_IDESC64, 1u);
 }
-__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint64_t a, uint64_t ones, uint64_t b16, uint32_t bw)
+// layer 3 reads its A operand (the layer-2 activations, BF16 pairs) from the slot's TMEM columns
+// 32..63, where the ep2 epilogue stored them, and accumulates into columns 0..15
+__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint64_t ones, uint64_t b16, uint32_t bw)
 {
 #pragma unroll
   for (int j = 0; j < 4; ++j)
-    cp_tc_mma(d, a + j * (4096 >> 4), b16 + bw + ((CP_TC_B3 + j * 512) >> 4), CP_TC_IDESC16, j > 0 ? 1u : 0u);
+    cp_tc_mma_ts(d, d + CP_TC_A3 + 8 * j, b16 + bw + ((CP_TC_B3 + j * 512) >> 4), CP_TC_IDESC16, j > 0 ? 1u : 0u);
   cp_tc_mma(d, ones, b16 + bw + (CP_TC_B3B >> 4), CP_TC_IDESC16, 1u);
 }
 
@@ -188,6 +191,14 @@ __device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint64_t a, uint64_t 
 __device__ __forceinline__ void cp_tc_publish(uint32_t pub)
 {
   cp_fence_proxy_async();
+  cp_tc_fence_before();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) cp_mbar_arrive(pub);
+}
+
+// the same for a step whose only writes went to TMEM (tcgen05.st, completed by cp_tc_wait_st)
+__device__ __forceinline__ void cp_tc_publish_tmem(uint32_t pub)
+{
   cp_tc_fence_before();
   __syncwarp();
   if ((threadIdx.x & 31) == 0) cp_mbar_arrive(pub);
@@ -220,6 +231,25 @@ __device__ __forceinline__ void cp_tc_hidden_out(uint32_t taddr, uint32_t hbuf, 
                 cp_relu_bf2(v[8 * kb + 2], v[8 * kb + 3]), cp_relu_bf2(v[8 * kb + 4], v[8 * kb + 5]),
                 cp_relu_bf2(v[8 * kb + 6], v[8 * kb + 7]));
   }
+}
+
+// TMEM [row][0:64] -> ReLU -> BF16 pairs -> TMEM [row][32:64], the A operand of layer 3 (hidden
+// unit k in column 32 + k / 2).  Half 1 (columns 32..63) is loaded first and lands in columns
+// 48..63, then half 0 (0..31) in 32..47: every column is loaded before it is stored over.
+// Nothing is stored when the MMAs were not seen to complete.
+__device__ __forceinline__ void cp_tc_hidden_to_tmem(uint32_t taddr, bool ok)
+{
+  if (!ok) return;
+#pragma unroll
+  for (int half = 1; half >= 0; --half) {
+    float v[32];
+    cp_tc_ld32(taddr + half * 32, v);
+    uint32_t w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = cp_relu_bf2(v[2 * i], v[2 * i + 1]);
+    cp_tc_st16(taddr + CP_TC_A3 + 16 * half, w);
+  }
+  cp_tc_wait_st();
 }
 
 __global__ void __launch_bounds__(CP_TC_THREADS, 1)
@@ -308,7 +338,7 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
             cp_tc_issue_l2(tc, ad, adones, b64, bw);
             lay = 2;
           } else {
-            cp_tc_issue_l3(tc, ad, adones, b16, bw);
+            cp_tc_issue_l3(tc, adones, b16, bw);
             lay = 0;
             bw = bw == (CP_FLOW_NC - 1) * (CP_TC_PER >> 4) ? 0u : bw + (CP_TC_PER >> 4);
           }
@@ -380,10 +410,10 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
           cp_tc_publish(pb[s]);
         }
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {           // ep2: layer-2 output -> layer 3
+        for (int s = 0; s < 2; ++s) {           // ep2: layer-2 output -> layer 3 (A in TMEM)
           const bool ok = cp_tc_wait(mb[s], ph[s], abort);
-          cp_tc_hidden_out(tc[s] + lane_base, hb[s], row, ok);
-          cp_tc_publish(pb[s]);
+          cp_tc_hidden_to_tmem(tc[s] + lane_base, ok);
+          cp_tc_publish_tmem(pb[s]);
         }
 #pragma unroll
         for (int s = 0; s < 2; ++s) {           // ep3: coupling update, next coupling's layer 1

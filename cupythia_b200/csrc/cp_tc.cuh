@@ -54,6 +54,17 @@ __device__ __forceinline__ void cp_tc_mma(uint32_t d_tmem, uint64_t a_desc, uint
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+// D[tmem] (+)= A[tmem] * B[smem]^T, issued by one thread.  A in tensor memory: row r in lane r,
+// BF16 element k of the row in the low (k even) or high (k odd) half of column k / 2.
+__device__ __forceinline__ void cp_tc_mma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 // the mbarrier receives one arrival when every tcgen05 operation this thread issued has completed
 __device__ __forceinline__ void cp_tc_commit(uint32_t mbar)
 {
@@ -91,6 +102,19 @@ __device__ __forceinline__ void cp_tc_ld4(uint32_t taddr, float (&v)[4])
 #pragma unroll
   for (int j = 0; j < 4; ++j) v[j] = __uint_as_float(r[j]);
 }
+
+// 16 consecutive 32-bit columns of this thread's TMEM lane from registers (not waited for)
+__device__ __forceinline__ void cp_tc_st16(uint32_t taddr, const uint32_t (&r)[16])
+{
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};\n" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+// every tcgen05.st of this thread has completed
+__device__ __forceinline__ void cp_tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // relu, round to BF16 and pack: low half from lo, high half from hi
 __device__ __forceinline__ uint32_t cp_relu_bf2(float lo, float hi)
