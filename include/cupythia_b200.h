@@ -257,7 +257,12 @@ int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, uint64_t ch
  * words 0,1); sigma = <w>, w = dsigma/dtHat (2 cMax)(s/2) conv. */
 int cp_partonic_integrate(cp_handle* h, double sqrt_shat, double alphas, double cmax,
                           double conv, uint64_t seed, uint64_t n_points, cp_result* out_host);
-/* Same integrand on the reference's SplitMix64 per-thread streams (n_threads x k_per draws). */
+/* Same integrand on the reference's SplitMix64 per-thread streams (n_threads x k_per draws:
+ * reference thread i draws from counter seed + i 0x100000001B3 + k).  The draws are shared out
+ * in equal contiguous parts, so the sums are those of the reference's stage in another order;
+ * the matrix element is evaluated in its closed form (9/2)(3 - tu/s^2 - su/t^2 - st/u^2), within
+ * 1.1e-15 relative of Pythia's bracket form.  Fails with CP_ERR_INVALID when n_threads k_per
+ * overflows 64 bits or is below 2. */
 int cp_partonic_splitmix(cp_handle* h, double sqrt_shat, double alphas, double cmax,
                          double conv, uint64_t seed, uint64_t n_threads, uint64_t k_per,
                          cp_result* out_host);

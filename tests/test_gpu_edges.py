@@ -159,3 +159,47 @@ def test_host_generation_capacity_and_staging_reuse():
     a = cp.events_view(rec_f)
     b = cp.events_view(host_f[:st3["n_accepted"]])
     assert a.tobytes() == b.tobytes()
+
+
+def test_pass_across_staging_chunks_is_one_pass():
+    """A production pass of 2^24 + 4099 points runs as two staging chunks (the second ragged): its
+    records are the accepted points of the whole pass in strictly increasing point order, their
+    count is the recount u w_max < w, and the host-delivery call with chunks that divide neither
+    the pass nor 2^24 delivers the same bytes; with the flow as proposal (one forward pass for the
+    whole call, read chunk by chunk) the two calls agree as well."""
+    import torch
+
+    import cupythia_b200 as cp
+    n = (1 << 24) + 4099
+    with cp.Integrator() as it:
+        it.integrate(4, 1 << 20, alpha=1.5)
+        it.iteration(1 << 20, 60, alpha=0.0)
+        wq = it.weight_quantile(0.999)
+        rec, st = it.unweight(n, iteration=61)
+        w = it.point_weights(0, n, 61).cpu().numpy()
+        u = (it.philox_words(it.cfg.seed, 0, n, 61, 0)[:, 3] >> 8).astype(np.float32) * np.float32(1.0 / 16777216.0)
+        ev = cp.events_view(rec)
+        pts = ev["point"].astype(np.int64)
+        assert np.all(np.diff(pts) > 0) and pts.max() < n
+        assert len(pts) == st["n_accepted"]
+        assert (pts >= 1 << 24).any()                     # the second chunk delivered records
+        expect = np.nonzero(u * np.float32(wq) < w)[0]
+        assert len(np.setxor1d(expect, pts)) <= 2
+        host = torch.empty((st["n_accepted"] + 8, 64), dtype=torch.uint8, pin_memory=True)
+        st2 = it.generate_host(n, host, iteration=61, chunk=3 * (1 << 22) + 1)
+        assert st2["n_accepted"] == st["n_accepted"]
+        assert cp.events_view(host[:st2["n_accepted"]]).tobytes() == ev.tobytes()
+        it.flow_init(7)
+        it.flow_train(10, 65536, lr=8e-3)
+        it.flow_enable(True)
+        it.iteration(1 << 20, 62, alpha=0.0)
+        it.weight_quantile(0.999)
+        rec_f, st_f = it.unweight(n, iteration=63)
+        host_f = torch.empty((st_f["n_accepted"] + 8, 64), dtype=torch.uint8, pin_memory=True)
+        st3 = it.generate_host(n, host_f, iteration=63, chunk=5000011)
+        it.flow_enable(False)
+    a = cp.events_view(rec_f)
+    pf = a["point"].astype(np.int64)
+    assert np.all(np.diff(pf) > 0) and (pf >= 1 << 24).any()
+    assert st3["n_accepted"] == st_f["n_accepted"]
+    assert cp.events_view(host_f[:st3["n_accepted"]]).tobytes() == a.tobytes()
