@@ -396,7 +396,7 @@ def run_ours(a):
     }
     if rank == 0:
         if world == 1:      # the host-core baseline is timed at N = 1 only
-            line["cpu_baseline"] = cpu_baseline(a.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline(a.cpu_seconds, line["plain_vegas"]["eta"])
         print(json.dumps(line), flush=True)
     it.close()
     if pg is not None:
@@ -411,13 +411,43 @@ def pythia_gen(n_events, threads):
     return json.loads(out.strip().split("\n")[-1])
 
 
-def cpu_baseline(seconds):
-    """Stock Pythia 8.317 (ProcessLevel, same settings) on all host cores, bounded sample."""
+def oracle_rate(seconds, threads, eta):
+    """The FP64 C restatement of the integrand (oracle/cp_oracle.c, cpo_had_accumulate: Philox
+    draw, map, tau-y-z phase space, CTEQ5L, alpha_s, the five processes' channel sum) on all host
+    cores over a bounded sample; the unweighted rate it implies at the GPU arm's plain-VEGAS eta."""
+    import ctypes as C
+
+    import numpy as np
+
+    import oracle
+    L = oracle.lib()
+    cfg = oracle.had_cfg()
+    edges = oracle.vegas_uniform(50)
+    hist = np.zeros(3 * 50)
+    sums = (C.c_double * 2)()
+
+    def run(n):
+        t0 = time.perf_counter()
+        L.cpo_had_accumulate(C.byref(cfg), oracle.dptr(edges), 50, 42, 0, 0, n, sums, oracle.dptr(hist), threads)
+        return time.perf_counter() - t0
+    probe = 1 << 16
+    n = max(int(probe / run(probe) * seconds), probe)
+    rate = n / run(n)
+    return {"weighted_points_per_s": rate, "unweighted_events_per_s_at_plain_eta": rate * eta,
+            "cores": threads, "kind": "port",
+            "sample": f"{n} points of the FP64 restatement on a uniform 3x50 grid (the cost per point "
+                      f"does not depend on the grid), eta {eta:.3f} of the plain-VEGAS form"}
+
+
+def cpu_baseline(seconds, eta_plain):
+    """Stock Pythia 8.317 (ProcessLevel, same settings) on all host cores, bounded sample; beside
+    it the FP64 restatement of the integrand (the oracle) on the same cores."""
     import oracle
     threads = os.cpu_count() or 1
     if not os.path.exists(oracle.PYTHIA_REF):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "oracle/_ref/pythia_ref missing (reference not built)"}
+                "sample": "oracle/_ref/pythia_ref missing (reference not built)",
+                "port": oracle_rate(seconds / 5, threads, eta_plain)}
     probe = pythia_gen(20000 * threads, threads)
     rate = probe["accepted"] / probe["seconds"]
     n = max(int(rate * seconds), 20000 * threads)
@@ -426,7 +456,8 @@ def cpu_baseline(seconds):
             "kind": "reference",
             "sample": f"{r['accepted']} unweighted events ({r['tried']} tried) of stock Pythia 8.317 "
                       f"ProcessLevel, {threads} threads x 1 Pythia instance, sigma_gen "
-                      f"{r['sigma_mb']:.5g} +- {r['sigma_err_mb']:.2g} mb"}
+                      f"{r['sigma_mb']:.5g} +- {r['sigma_err_mb']:.2g} mb",
+            "port": oracle_rate(seconds / 5, threads, eta_plain)}
 
 
 def run_reference(a):
