@@ -145,9 +145,9 @@ CP_HD T cp_alphas_t(const CpHadParams& P, const CpHadParamsT<T>& Q, const T& Q2i
 }
 
 template <class T>
-CP_HD T cp_poly_t(const float c[3], const T& t)
+CP_HD T cp_poly_t(const CpCteqPoly& c, int f, const T& t)
 {
-  return (c[2] * t + c[1]) * t + c[0];
+  return (c.co[2][f] * t + c.co[1][f]) * t + c.co[0][f];
 }
 
 template <class T>
@@ -160,9 +160,9 @@ CP_HD T cp_cteq_answer_t(const CpCteqPoly& c, const T& sb1, const T& invQ, const
   T y = -lnx;
   T u = lnx + 11.512925465f;
   T x1L = cp_log_t(omx);
-  T A = cp_poly_t(c.A, sb1), B = cp_poly_t(c.B, sb1), af1 = cp_poly_t(c.af1, sb1);
-  T af2 = cp_poly_t(c.af2, sb1), p = cp_poly_t(c.p, sb1), af5 = cp_poly_t(c.af5, sb1);
-  T af6 = cp_poly_t(c.af6, sb1), af7 = cp_poly_t(c.af7, sb1), af8 = cp_poly_t(c.af8, sb1);
+  T A = cp_poly_t(c, CP_CQ_A, sb1), B = cp_poly_t(c, CP_CQ_B, sb1), af1 = cp_poly_t(c, CP_CQ_AF1, sb1);
+  T af2 = cp_poly_t(c, CP_CQ_AF2, sb1), p = cp_poly_t(c, CP_CQ_P, sb1), af5 = cp_poly_t(c, CP_CQ_AF5, sb1);
+  T af6 = cp_poly_t(c, CP_CQ_AF6, sb1), af7 = cp_poly_t(c, CP_CQ_AF7, sb1), af8 = cp_poly_t(c, CP_CQ_AF8, sb1);
   T ym1 = cp_expm1_t(p * cp_log_t(y));
   T U = af8 * u + 1.f;
   T part3 = x * omx * (af5 + af6 * omx + af7 * x * omx);

@@ -42,18 +42,24 @@
 // ------------------------------------------------------------------------------------------
 // Uniform parameters of the hadronic integrand (built on the host in FP64, stored in FP32).
 // ------------------------------------------------------------------------------------------
-// 144 bytes, 16-byte aligned: the kernels read one record as nine 128-bit shared-memory loads
+// the nine polynomials of a parametrisation, in the order of CpCteqPoly::co
+enum { CP_CQ_A, CP_CQ_B, CP_CQ_AF1, CP_CQ_AF2, CP_CQ_P, CP_CQ_AF5, CP_CQ_AF6, CP_CQ_AF7, CP_CQ_AF8, CP_CQ_N };
+
+// 160 bytes, 16-byte aligned: the kernels read one record as ten 128-bit shared-memory loads
 struct alignas(16) CpCteqPoly {
-  // per parametrisation i: polynomial coefficients in sb1 = ln ln(Q/alpha_i) - 1.2
-  float A[3], B[3], af1[3], af2[3], p[3], af5[3], af6[3], af7[3], af8[3];
+  // per parametrisation i: co[k][f] = coefficient of sb1^k in polynomial f (CP_CQ_*), sb1 =
+  // ln ln(Q/alpha_i) - 1.2.  The pairs (A, B), (af1, af2), (p, af5), (af6, af7) sit side by side
+  // at even offsets (co[k][9] pads each power to 10 floats), so one two-lane FMA evaluates a pair.
+  float co[3][10];
   float lnAlpha;  // ln(alpha_i)
   float qlim;     // max(Qmin_i, alpha_i)
   float qmin;     // Qmin_i
   float ut1;      // ut1_i
   float eut2;     // exp(ut2_i)
   int   useX1L;   // ut2_i < -100: part4 uses ln(1 - x) twice
-  int   pad[3];
+  int   pad[4];
 };
+static_assert(sizeof(CpCteqPoly) == 160, "coefficient record layout");
 
 struct CpHadParams {
   CpCteqPoly cteq[8];
@@ -77,7 +83,11 @@ CP_HD float cp_logf(float x) { return logf(x); }
 CP_HD float cp_expm1f(float x) { return expm1f(x); }
 CP_HD float cp_sqrtf(float x) { return sqrtf(x); }
 CP_HD float cp_fmaf(float a, float b, float c) { return fmaf(a, b, c); }
-CP_HD float cp_poly(const float c[3], float t) { return cp_fmaf(cp_fmaf(c[2], t, c[1]), t, c[0]); }
+// polynomial f of a coefficient record at t (Horner, FMA)
+CP_HD float cp_cq_poly(const CpCteqPoly& c, int f, float t)
+{
+  return cp_fmaf(cp_fmaf(c.co[2][f], t, c.co[1][f]), t, c.co[0][f]);
+}
 
 // ------------------------------------------------------------------------------------------
 // alpha_s(Q2) at first order with threshold matching (StandardModel.cc:189-215).
@@ -178,15 +188,20 @@ CP_HD CpCteqQ cp_cteq_coef(const CpCteqPoly& c, float lnQ, float Q, float invQ, 
 {
   CpCteqQ q;
   float sb1 = cp_logf(lnQ - c.lnAlpha) - 1.2f;
-  q.A = cp_poly(c.A, sb1);
-  q.B = cp_poly(c.B, sb1);
-  q.af1 = cp_poly(c.af1, sb1);
-  q.af2 = cp_poly(c.af2, sb1);
-  q.p = cp_poly(c.p, sb1);
-  q.af5 = cp_poly(c.af5, sb1);
-  q.af6 = cp_poly(c.af6, sb1);
-  q.af7 = cp_poly(c.af7, sb1);
-  q.af8 = cp_poly(c.af8, sb1);
+  // four pairs in two-lane FMAs (each lane rounded as the scalar FMA), af8 alone
+  const CpF2 t = cp_f2s(sb1);
+  CpF2 v[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const CpF2 c0 = cp_f2(c.co[0][2 * j], c.co[0][2 * j + 1]), c1 = cp_f2(c.co[1][2 * j], c.co[1][2 * j + 1]);
+    const CpF2 c2 = cp_f2(c.co[2][2 * j], c.co[2][2 * j + 1]);
+    v[j] = cp_fma2(cp_fma2(c2, t, c1), t, c0);
+  }
+  q.A = v[0].x; q.B = v[0].y;
+  q.af1 = v[1].x; q.af2 = v[1].y;
+  q.p = v[2].x; q.af5 = v[2].y;
+  q.af6 = v[3].x; q.af7 = v[3].y;
+  q.af8 = cp_cq_poly(c, CP_CQ_AF8, sb1);
   q.qfac = hq ? ((Q > c.qlim) ? (1.f - c.qmin * invQ) : 0.f) : 1.f;
   return q;
 }

@@ -85,15 +85,17 @@ static inline int cp_build_had_params(const CpHadConfig& c, CpHadParams& P)
   for (int i = 0; i < 8; ++i) {
     CpCteqPoly& q = P.cteq[i];
     for (int k = 0; k < 3; ++k) {
-      q.A[k] = (float)(AM[i][0][k] + AM[i][1][k]);
-      q.B[k] = (float)(AM[i][3][k] - AM[i][0][k]);
-      q.af1[k] = (float)AM[i][1][k];
-      q.af2[k] = (float)AM[i][2][k];
-      q.p[k] = (float)((k == 0 ? 1.0 : 0.0) + 0.01 * AM[i][4][k]);
-      q.af5[k] = (float)AM[i][5][k];
-      q.af6[k] = (float)AM[i][6][k];
-      q.af7[k] = (float)AM[i][7][k];
-      q.af8[k] = (float)AM[i][8][k];
+      float* co = q.co[k];
+      co[CP_CQ_A] = (float)(AM[i][0][k] + AM[i][1][k]);
+      co[CP_CQ_B] = (float)(AM[i][3][k] - AM[i][0][k]);
+      co[CP_CQ_AF1] = (float)AM[i][1][k];
+      co[CP_CQ_AF2] = (float)AM[i][2][k];
+      co[CP_CQ_P] = (float)((k == 0 ? 1.0 : 0.0) + 0.01 * AM[i][4][k]);
+      co[CP_CQ_AF5] = (float)AM[i][5][k];
+      co[CP_CQ_AF6] = (float)AM[i][6][k];
+      co[CP_CQ_AF7] = (float)AM[i][7][k];
+      co[CP_CQ_AF8] = (float)AM[i][8][k];
+      co[CP_CQ_N] = 0.f;
     }
     q.lnAlpha = (float)log(ALPHA[i]);
     q.qlim = (float)(QMIN[i] > ALPHA[i] ? QMIN[i] : ALPHA[i]);

@@ -471,7 +471,7 @@ extern "C" int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* h
 // ------------------------------------------------------------------------------------------
 #define CP_NOALLOC_MAX_BLOCKS 512
 #define CP_NOALLOC_SLOT_DOUBLES (CP_NOALLOC_MAX_BLOCKS * (CP_SLOT_HEAD + 3 * CP_MAX_BINS))
-#define CP_NOALLOC_CTEQ_DOUBLES 160   // 8 CpCteqPoly records (1056 bytes), rounded up
+#define CP_NOALLOC_CTEQ_DOUBLES 160   // 8 CpCteqPoly records (1280 bytes)
 #define CP_NOALLOC_DOUBLES (CP_NOALLOC_CTEQ_DOUBLES + CP_QBINS + CP_NOALLOC_SLOT_DOUBLES)
 
 static __device__ __align__(256) double cp_noalloc_scratch[CP_NOALLOC_DOUBLES];
