@@ -83,6 +83,16 @@ CP_HD float cp_logf(float x) { return logf(x); }
 CP_HD float cp_expm1f(float x) { return expm1f(x); }
 CP_HD float cp_sqrtf(float x) { return sqrtf(x); }
 CP_HD float cp_fmaf(float a, float b, float c) { return fmaf(a, b, c); }
+// a / b for a sub-ulp correction term a: the quotient's last bits do not reach the result, so
+// the device takes the fast division (about 2 ulp) instead of the IEEE one
+CP_HD float cp_div_correction(float a, float b)
+{
+#if defined(__CUDA_ARCH__)
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
 // polynomial f of a coefficient record at t (Horner, FMA)
 CP_HD float cp_cq_poly(const CpCteqPoly& c, int f, float t)
 {
@@ -161,7 +171,7 @@ CP_HD CpBeamX cp_beam_x(float lnx, float lnxLo)
   omx = cp_fmaf(-x, lnxLo, omx);
   if (omx < 1e-10f) { omx = 1e-10f; x = 1.f - 1e-10f; lnx = -1e-10f; lnxLo = 0.f; }
   float y = -lnx;                        // y = -ln x, correction -lnxLo
-  b.lny = cp_logf(y) - lnxLo / y;
+  b.lny = cp_logf(y) - cp_div_correction(lnxLo, y);
   // u = ln(x / 1e-5) = ln x + ln 1e5 as a (hi, lo) pair
   const float LN1E5_HI = 11.512925148f, LN1E5_LO = 3.1696e-07f;
   cp_twosum(lnx, LN1E5_HI, b.uh, b.ul);
