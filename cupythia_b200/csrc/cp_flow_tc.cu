@@ -1,8 +1,9 @@
 // cp_flow_tc.cu -- the flow forward (sampling) pass on the 5th-generation tensor cores.
 //
 // Same map as k_flow_fwd (Philox words -> VEGAS map -> logit -> 4 affine couplings -> sigmoid),
-// with every dense layer as tcgen05.mma over 128-point tiles: A (activations) and B (weights) in
-// shared memory, the FP32 accumulator in TMEM.
+// with every dense layer as tcgen05.mma over 128-point tiles: B (weights) in shared memory, the
+// FP32 accumulator in TMEM, A (activations) in shared memory for layers 1 and 2 and in TMEM for
+// layer 3 (stored over the spent layer-2 accumulator).
 //
 // Launch: one persistent CTA per SM (the shared-memory footprint admits one): 4 epilogue
 // warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two
@@ -11,7 +12,8 @@
 // does nothing but poll its warpgroup's two publish barriers and issue each slot's next layer,
 // so no epilogue warp ever waits on MMA issue.  Per coupling and slot the epilogue has three steps
 //   ep1: wait for layer 1, TMEM -> ReLU -> BF16 -> activation buffer, publish (layer 2 follows)
-//   ep2: the same for layer 2 (layer 3 follows)
+//   ep2: wait for layer 2, TMEM -> ReLU -> BF16 pairs -> TMEM columns 32..63, publish (layer 3,
+//        A from TMEM, accumulates into columns 0..15)
 //   ep3: wait for layer 3, read the 4 output columns, update the point, write the next
 //        coupling's layer-1 input, publish (its layer 1 follows)
 // and the steps of the two slots alternate, so one slot's MMAs run while the other slot's
