@@ -95,6 +95,28 @@ def test_simpson_and_partonic_mc(orc):
     assert abs(m - simp) < 4 * err
 
 
+def test_gg2gg_closed_form_matches_the_bracket_form(orc):
+    """The partonic kernel evaluates gg -> gg as (9/2)(3 - tu/s^2 - su/t^2 - st/u^2) with one
+    reciprocal of t u; with u = -s - t rounded as the reference rounds it, that form agrees with
+    the oracle's bracket form (Sigma2gg2gg::sigmaKin, the reference's gg2gg_sigma) to 2e-15 over
+    |cos theta| < 0.9, at the ends of the range included."""
+    L = orc.lib()
+    s, aS, cmax, conv = 1e4, 0.118, 0.9, 0.3893793721
+    u01 = np.concatenate([np.random.default_rng(5).random(20000), [0.0, 1e-12, 0.5, 1.0 - 2 ** -53]])
+    is_ = 1.0 / s
+    pre = np.pi * is_ * is_ * (aS * aS) * 0.5 * 4.5
+    c = (2.0 * u01 - 1.0) * cmax
+    t = -0.5 * s * (1.0 - c)
+    u = -s - t
+    tu = t * u
+    itu = 1.0 / tu
+    it, iu = u * itu, t * itu
+    closed = pre * (3.0 - tu * (is_ * is_) - (s * u) * (it * it) - (s * t) * (iu * iu))
+    closed *= (2.0 * cmax) * (s / 2.0) * conv
+    ref = np.array([L.cpo_partonic_weight(100.0, aS, cmax, conv, float(v)) for v in u01])
+    assert np.max(np.abs(closed / ref - 1)) < 2e-15
+
+
 def test_oracle_vegas_matches_pythia_sigma_gen(orc, golden):
     """FP64 oracle VEGAS (3 x 50 bins) against stock Pythia's sigmaGen for the dijet config."""
     L = orc.lib()
