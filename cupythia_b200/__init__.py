@@ -266,6 +266,19 @@ class Integrator:
         p = np.ascontiguousarray(np.asarray(p, np.float32))
         self._check(self.lib.cp_flow_set_params(self.h, p.ctypes.data_as(C.c_void_p), p.size))
 
+    def flow_state(self):
+        """Training checkpoint: (FP32 master parameters + Adam moments, updates taken)."""
+        n = self.lib.cp_flow_state_size()
+        out = np.zeros(n, np.float32)
+        k = C.c_int64()
+        self._check(self.lib.cp_flow_get_state(self.h, out.ctypes.data_as(C.c_void_p), n, C.byref(k)))
+        return out, k.value
+
+    def flow_restore(self, state, updates):
+        """Resumes training from a flow_state() checkpoint."""
+        state = np.ascontiguousarray(np.asarray(state, np.float32))
+        self._check(self.lib.cp_flow_set_state(self.h, state.ctypes.data_as(C.c_void_p), state.size, int(updates)))
+
     def flow_sample(self, point0, n, iteration=0, stream=0):
         torch = _torch()
         out = torch.empty((n, 4), dtype=torch.float32, device=self.device)
@@ -278,6 +291,10 @@ class Integrator:
     def flow_kernel(self, which):
         """Forward kernel: "tcgen05" (TMEM accumulators, default) or "mma" (warp-level mma.sync)."""
         self._check(self.lib.cp_flow_select_kernel(self.h, {"tcgen05": 0, "mma": 1}[which]))
+
+    def flow_objective(self, p=2.0):
+        """Training objective <w^p>/<w>^p (p = 2: the weight variance)."""
+        self._check(self.lib.cp_flow_set_objective(self.h, float(p)))
 
     def flow_train(self, steps, batch=65536, lr=1e-3):
         loss = np.zeros(steps)

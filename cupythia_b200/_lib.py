@@ -138,6 +138,9 @@ SIGNATURES = {
     "cp_flow_init": [_P, _u64],
     "cp_flow_get_params": [_P, _P, _i],
     "cp_flow_set_params": [_P, _P, _i],
+    "cp_flow_state_size": [],
+    "cp_flow_get_state": [_P, _P, _i, C.POINTER(_i64)],
+    "cp_flow_set_state": [_P, _P, _i, _i64],
     "cp_flow_sample": [_P, _u64, _u64, _u32, _u32, _P],
     "cp_flow_enable": [_P, _i],
     "cp_flow_select_kernel": [_P, _i],
@@ -145,6 +148,7 @@ SIGNATURES = {
     "cp_colour_tags": [C.c_uint16, C.c_uint16, _P, _P],
     "cp_write_lhef": [C.POINTER(cp_config), _P, _u64, _d, _d, C.c_char_p],
     "cp_flow_train": [_P, _i, _u64, _d, _P],
+    "cp_flow_set_objective": [_P, _d],
     "cp_flow_loss_grad": [_P, _u64, _u32, _P, _P],
     "cp_set_kernel_timing": [_P, _i],
     "cp_kernel_times": [_P, _P, _P, _i],

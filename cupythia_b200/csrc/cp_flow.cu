@@ -205,6 +205,44 @@ extern "C" int cp_flow_set_params(cp_handle* h, const float* in, int n)
   return CP_OK;
 }
 
+// Full training state: master parameters, Adam's first and second moments (the gradient slot
+// between them is zero between steps and is not part of it) and the number of updates taken.
+extern "C" int cp_flow_state_size(void) { return 3 * CP_FLOW_NPARAM; }
+
+extern "C" int cp_flow_get_state(cp_handle* h, float* out, int n, int64_t* updates)
+{
+  CP_CHECK_HANDLE(h);
+  if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised");
+  if (!out || !updates || n != 3 * CP_FLOW_NPARAM)
+    return cp_fail(h, CP_ERR_INVALID, "cp_flow_get_state: need cp_flow_state_size() floats and an update count");
+  const size_t P = sizeof(float) * CP_FLOW_NPARAM;
+  CP_CUDA(h, cudaMemcpyAsync(out, h->d_flow, P, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaMemcpyAsync(out + CP_FLOW_NPARAM, h->d_flow + 2 * CP_FLOW_NPARAM, 2 * P, cudaMemcpyDeviceToHost,
+                             h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  *updates = (int64_t)h->flow_t;
+  return CP_OK;
+}
+
+extern "C" int cp_flow_set_state(cp_handle* h, const float* in, int n, int64_t updates)
+{
+  CP_CHECK_HANDLE(h);
+  if (!in || n != 3 * CP_FLOW_NPARAM || updates < 0 || updates > 0xFFFFFFFFll)
+    return cp_fail(h, CP_ERR_INVALID, "cp_flow_set_state: need cp_flow_state_size() floats and 0 <= updates < 2^32");
+  int rc = cp_flow_ensure(h);
+  if (rc) return rc;
+  const size_t P = sizeof(float) * CP_FLOW_NPARAM;
+  CP_CUDA(h, cudaMemcpyAsync(h->d_flow, in, P, cudaMemcpyHostToDevice, h->stream));
+  CP_CUDA(h, cudaMemsetAsync(h->d_flow + CP_FLOW_NPARAM, 0, P, h->stream));
+  CP_CUDA(h, cudaMemcpyAsync(h->d_flow + 2 * CP_FLOW_NPARAM, in + CP_FLOW_NPARAM, 2 * P, cudaMemcpyHostToDevice,
+                             h->stream));
+  rc = cp_flow_repack(h);
+  if (rc) return rc;
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->flow_t = (long)updates;
+  return CP_OK;
+}
+
 extern "C" int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float* out_dev)
 {
   CP_CHECK_HANDLE(h);

@@ -1,7 +1,8 @@
 // cp_flow_train.cu -- training of the learned proposal on weights the integrator generates.
 //
 // Objective: the relative second moment of the weights, L = <w^2> / <w>^2 (= 1 + Var[w]/sigma^2),
-// minimised over the flow parameters theta at fixed VEGAS grid.  With w = f(x(x_v; theta)) J,
+// minimised over the flow parameters theta at fixed VEGAS grid (cp_flow_set_objective selects
+// the relative p-th moment <w^p>/<w>^p instead, which weighs the tail of the weights more).  With w = f(x(x_v; theta)) J,
 // x_v the VEGAS-mapped point (fixed by the random numbers), f the integrand and J the VEGAS
 // Jacobian times |dx/dx_v|, the pathwise gradient is
 //   dL/dtheta = 2/(B sigma^2) sum_points w^2 (d ln f/dx . dx/dtheta + d ln J/dtheta),
@@ -160,7 +161,7 @@ __device__ __forceinline__ void cp_store_rowfrag(uint16_t* base, int ld, uint64_
 __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g, uint64_t n,
                                                   double n_batch, const float* __restrict__ zs, const float4* __restrict__ vj,
                                                   const float4* __restrict__ wg, const double* __restrict__ sums,
-                                                  FlowTrainBufs out)
+                                                  FlowTrainBufs out, float loss_p)
 {
   extern __shared__ uint2 sPk[];   // all CP_FLOW_P_PER fragments of the 4 couplings, then biases
   float* sBias = reinterpret_cast<float*>(sPk + CP_FLOW_NC * CP_FLOW_P_PER);
@@ -171,6 +172,8 @@ __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g
   // the batch's moments and size (all ranks' points when the batch is sharded)
   const double sig = sums[0] / n_batch;
   const float cnorm = (float)(2.0 / (n_batch * sig * sig));
+  // objective <w^p>/<w>^p: dL/d ln w of a point = p (w / sigma)^p / B (p = 2: 2 w^2 / (B sigma^2))
+  const float cnorm_p = (float)(loss_p / n_batch), inv_sig = (float)(1.0 / sig);
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
   const uint64_t rounds = (n + 32 * warps - 1) / (32 * warps);
   for (uint64_t r = 0; r < rounds; ++r) {
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g
     float dz[3] = {0.f, 0.f, 0.f}, cJ = 0.f;
     if (active) {
       const float4 f = vj[p], g = wg[p];
-      cJ = cnorm * g.x * g.x;
+      cJ = loss_p == 2.f ? cnorm * g.x * g.x : cnorm_p * powf(g.x * inv_sig, loss_p);
       const float v[3] = {f.x, f.y, f.z}, gv[3] = {g.y, g.z, g.w};
       // sigmoid: dv/dz = v (1 - v); d ln(v (1 - v))/dz = 1 - 2 v
       for (int d = 0; d < 3; ++d) dz[d] = cJ * gv[d] * v[d] * (1.f - v[d]) + cJ * (1.f - 2.f * v[d]);
@@ -587,7 +590,7 @@ static int flow_phase_gradient(cp_handle* h, const FlowTrainBufs& t, uint64_t co
   k_flow_batch_loss<<<1, 1, 0, h->stream>>>(moments, (double)n_batch, t.sums, loss_dev);
   CP_LAUNCH_CHECK(h, "k_flow_batch_loss");
   k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, count, (double)n_batch, t.zs,
-                                                          t.vj, t.wg, t.sums, t);
+                                                          t.vj, t.wg, t.sums, t, (float)h->flow_loss_p);
   CP_LAUNCH_CHECK(h, "k_flow_bwd");
   float* G = h->d_flow + CP_FLOW_NPARAM;
   // at most CP_WG_MAXBLK blocks per coupling and layer; chunks are whole multiples of the staged
@@ -628,6 +631,14 @@ static int flow_phase_update(cp_handle* h, double lr)
 // Trains the flow for n_steps batches of `batch` points on the current VEGAS grid; loss_host
 // (n_steps doubles, may be NULL) receives <w^2>/<w>^2 of each batch before its update.  Step s
 // draws its batch at counter iteration flow_t (the number of updates so far), points 0..batch-1.
+extern "C" int cp_flow_set_objective(cp_handle* h, double p)
+{
+  CP_CHECK_HANDLE(h);
+  if (!(p >= 2.0 && p <= 8.0)) return cp_fail(h, CP_ERR_INVALID, "cp_flow_set_objective: p must be in [2, 8]");
+  h->flow_loss_p = p;
+  return CP_OK;
+}
+
 extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host)
 {
   CP_CHECK_HANDLE(h);

@@ -453,21 +453,24 @@ extern "C" int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* h
 // ------------------------------------------------------------------------------------------
 // Allocation-free VEGAS pass.
 //
-// For callers that must not allocate device memory: code running inside a CUDA graph that is
-// being captured, under a caller-owned memory pool or a fixed memory budget, or embedded in a
-// host framework that owns every device allocation (a Pythia plugin sharing the GPU with its
-// host program).  This entry point creates no handle and calls no cudaMalloc / cudaFree: its
-// scratch (the per-block partial sums, the weight histogram and the CTEQ5L coefficient
+// For callers that must not allocate device memory: a host program that owns every device
+// allocation (a caching allocator or memory pool whose accounting a cudaMalloc behind its back
+// would break), a process held to a fixed device-memory budget, or a plugin such as a Pythia
+// SigmaProcess running inside someone else's event loop, which cannot create and keep a handle
+// with its own buffers.  This entry point creates no handle and calls no cudaMalloc / cudaFree:
+// its scratch (the per-block partial sums, the weight histogram and the CTEQ5L coefficient
 // records) lives in the file-scope array below, which every GPU that loads this library keeps
-// until the process exits.
+// until the process exits.  The first call on a device looks up the array's address and the
+// launch shape (later calls only re-check the address); make that first call before any stream
+// capture.
 //
 // Limits: the partial sums hold at most CP_NOALLOC_MAX_BLOCKS blocks of CP_SLOT_HEAD + 3 *
 // CP_MAX_BINS doubles, so n_bins above CP_MAX_BINS is rejected; the grid is capped at
 // CP_NOALLOC_MAX_BLOCKS blocks (296 are used on a B200).  Total: 1,623,296 bytes per device.
-// Every call shares the array and it keeps the last call's contents; the weight histogram is
-// cleared at the start of each call and every partial-sum slot is rewritten.  Calls that overlap
-// on the GPU (different streams, or several host threads) race on the array and must not be
-// issued; calls in one stream are ordered and safe.
+// Every call shares the array and it keeps the last call's contents; each call rewrites the
+// coefficient records, clears the weight histogram and rewrites every partial-sum slot it
+// reads.  Calls that overlap on the GPU (different streams, or several host threads) race on the
+// array and must not be issued; calls in one stream are ordered and safe.
 // ------------------------------------------------------------------------------------------
 #define CP_NOALLOC_MAX_BLOCKS 512
 #define CP_NOALLOC_SLOT_DOUBLES (CP_NOALLOC_MAX_BLOCKS * (CP_SLOT_HEAD + 3 * CP_MAX_BINS))
@@ -477,11 +480,21 @@ extern "C" int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* h
 static __device__ __align__(256) double cp_noalloc_scratch[CP_NOALLOC_DOUBLES];
 static_assert(sizeof(CpCteqPoly) * 8 <= CP_NOALLOC_CTEQ_DOUBLES * sizeof(double), "CTEQ records fit");
 
+// Per-call set-up of the shared array, on the caller's stream: the CTEQ5L coefficient records
+// (taken from the kernel parameters, so no host copy is involved) and a cleared weight histogram.
+__global__ void k_noalloc_setup(const CpHadParams P, double* base)
+{
+  uint32_t* cteq = reinterpret_cast<uint32_t*>(base);
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(P.cteq);
+  for (int k = threadIdx.x; k < (int)(8 * sizeof(CpCteqPoly) / 4); k += blockDim.x) cteq[k] = src[k];
+  unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base + CP_NOALLOC_CTEQ_DOUBLES);
+  for (int k = threadIdx.x; k < CP_QBINS; k += blockDim.x) qhist[k] = 0ull;
+}
+
 namespace {
 struct NoallocDevice {
   double* scratch = nullptr;   // device address of cp_noalloc_scratch on this device
   int blocks = 0;
-  int ready = 0;
 };
 const int CP_NOALLOC_MAX_DEVICES = 64;
 NoallocDevice g_noalloc[CP_NOALLOC_MAX_DEVICES];
@@ -505,43 +518,48 @@ extern "C" int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, ui
   if (prev != cfg->device && cudaSetDevice(cfg->device) != cudaSuccess) return CP_ERR_CUDA;
   cudaStream_t stream = (cudaStream_t)cuda_stream;
   int rc = CP_OK;
-  NoallocDevice& D = g_noalloc[cfg->device];
+  NoallocDevice D;
   {
-    // once per device, with that device current: the array's device address, the launch shape
-    // and the (configuration-independent) CTEQ5L coefficient records
+    // With the device current: the array's device address (looked up on every call, so a
+    // reloaded module after a device reset is picked up) and, when it is new, the launch shape.
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!D.ready) {
-      void* ptr = nullptr;
+    NoallocDevice& G = g_noalloc[cfg->device];
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, cp_noalloc_scratch) != cudaSuccess || !ptr) {
+      rc = CP_ERR_CUDA;
+    } else if (ptr != G.scratch) {
       int nsm = 0, per_sm = 0;
-      if (cudaGetSymbolAddress(&ptr, cp_noalloc_scratch) != cudaSuccess || !ptr ||
-          cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess ||
-          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_had_accum<false>, CP_THREADS, 0) != cudaSuccess ||
-          cudaMemcpy(ptr, P.cteq, sizeof(CpCteqPoly) * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+      if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess ||
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_had_accum<false>, CP_THREADS, 0) != cudaSuccess) {
         rc = CP_ERR_CUDA;
       } else {
-        D.scratch = (double*)ptr;
-        int blocks = nsm * (per_sm > 0 ? per_sm : 1);
-        D.blocks = blocks < CP_NOALLOC_MAX_BLOCKS ? blocks : CP_NOALLOC_MAX_BLOCKS;
-        D.ready = 1;
+        const int blocks = nsm * (per_sm > 0 ? per_sm : 1);
+        G.blocks = blocks < CP_NOALLOC_MAX_BLOCKS ? blocks : CP_NOALLOC_MAX_BLOCKS;
+        G.scratch = (double*)ptr;
       }
     }
+    D = G;
   }
   if (rc == CP_OK) {
     double* base = D.scratch;
     unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base + CP_NOALLOC_CTEQ_DOUBLES);
     double* slots = base + CP_NOALLOC_CTEQ_DOUBLES + CP_QBINS;
-    const int nb = cfg->n_bins, width = CP_SLOT_HEAD + 3 * nb;
+    int nb = cfg->n_bins, width = CP_SLOT_HEAD + 3 * nb, max_col = 2;
     HadLaunch L;
     L.seed = cfg->seed; L.point0 = 0; L.n = n_points; L.iter = iter; L.stream = 0;
     L.nb = nb; L.edges = edges_dev; L.cteq = reinterpret_cast<const CpCteqPoly*>(base);
     L.slots = slots; L.w_out = nullptr; L.x_out = nullptr; L.qhist = qhist; L.flow = nullptr;
-    if (cudaMemsetAsync(qhist, 0, sizeof(unsigned long long) * CP_QBINS, stream) != cudaSuccess) {
+    // Each launch's own return code is checked; an error the caller left pending from earlier,
+    // unrelated work is neither reported as this call's nor cleared.
+    void* a_setup[] = {&P, &base};
+    void* a_accum[] = {&P, &L};
+    void* a_reduce[] = {&slots, &D.blocks, &width, &sums_dev, &max_col};
+    if (cudaLaunchKernel((const void*)k_noalloc_setup, dim3(1), dim3(256), a_setup, 0, stream) != cudaSuccess ||
+        cudaLaunchKernel((const void*)k_had_accum<false>, dim3(D.blocks), dim3(CP_THREADS), a_accum, 0, stream) !=
+            cudaSuccess ||
+        cudaLaunchKernel((const void*)k_reduce_slots<0>, dim3((width + 7) / 8), dim3(8 * 32), a_reduce, 0, stream) !=
+            cudaSuccess)
       rc = CP_ERR_CUDA;
-    } else {
-      k_had_accum<false><<<D.blocks, CP_THREADS, 0, stream>>>(P, L);
-      k_reduce_slots<0><<<(width + 7) / 8, 8 * 32, 0, stream>>>(slots, D.blocks, width, sums_dev);
-      if (cudaGetLastError() != cudaSuccess) rc = CP_ERR_CUDA;
-    }
   }
   if (prev != cfg->device) cudaSetDevice(prev);
   return rc;

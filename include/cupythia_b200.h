@@ -203,16 +203,19 @@ int cp_weight_at(cp_handle* h, const float* x_dev, int64_t n, float* w_dev);
 int cp_last_histogram(cp_handle* h, double* out_host);
 
 /* One VEGAS pass (the body of cp_vegas_iteration, without refinement) that allocates nothing.
- * No counterpart in the reference.  For callers that cannot call cudaMalloc: code inside a CUDA
- * graph being captured, under a caller-owned memory pool or fixed memory budget, or embedded in
- * a host program that owns every device allocation.  No handle is created; the scratch (block
- * partial sums for up to 512 blocks, the weight histogram, the CTEQ5L records: 1,623,296 bytes)
- * is a file-scope device array that every GPU loading this library keeps until exit.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc: a host program that
+ * owns every device allocation (a caching allocator or pool whose accounting an allocation
+ * behind its back would break), a process held to a fixed device-memory budget, or a plugin (a
+ * Pythia SigmaProcess) running inside another program's event loop without a handle of its own.
+ * No handle is created; the scratch (block partial sums for up to 512 blocks, the weight
+ * histogram, the CTEQ5L records: 1,623,296 bytes) is a file-scope device array that every GPU
+ * loading this library keeps until exit.
  * Inputs: cfg (host), the grid edges_dev (3 x (n_bins + 1) doubles).  Output: sums_dev (4 + 3
  * n_bins doubles, the layout of cp_last_histogram).  n_bins > CP_MAX_BINS is rejected
- * (CP_ERR_INVALID).  The first call on a device sets up (symbol address, coefficient copy) and
- * should come before any stream capture.  The array keeps the last call's contents and the
- * weight histogram is cleared per call; calls that overlap on the GPU race on it. */
+ * (CP_ERR_INVALID).  The first call on a device looks up the array's device address and the
+ * launch shape and should come before any stream capture; later calls re-check the address.
+ * Each call rewrites the coefficient records and clears the weight histogram on the stream; the
+ * array keeps the last call's contents, and calls that overlap on the GPU race on it. */
 int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, uint32_t iter,
                           const double* edges_dev, double* sums_dev, void* cuda_stream);
 
@@ -305,6 +308,15 @@ int cp_flow_num_params(void);
 int cp_flow_init(cp_handle* h, uint64_t seed);
 int cp_flow_get_params(cp_handle* h, float* params_host, int n);
 int cp_flow_set_params(cp_handle* h, const float* params_host, int n);
+/* Checkpoint and resume of training (no reference counterpart: the reference keeps no trained
+ * state and regenerates events from their counters, cuPythia/05_reproducible_events/
+ * repro_events.cu:3-10): the FP32 master parameters, then Adam's first and second moments
+ * (cp_flow_state_size() = 3 x cp_flow_num_params() floats), and the number of updates taken,
+ * which is also the counter iteration of the next training batch.  Restoring the state saved
+ * after k updates and training m more reproduces k + m uninterrupted updates bit for bit. */
+int cp_flow_state_size(void);
+int cp_flow_get_state(cp_handle* h, float* state_host, int n, int64_t* updates_host);
+int cp_flow_set_state(cp_handle* h, const float* state_host, int n, int64_t updates);
 /* Flow samples of points [point0, point0+n), counter (iter, stream): out (dev, 16-byte aligned)
  * holds (v0, v1, v2, ln|dv/du|) per point. */
 int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float* out_dev);
@@ -323,6 +335,11 @@ int cp_flow_enable(cp_handle* h, int on);
  * through the current flow and VEGAS grid, minimising <w^2>/<w>^2; loss_host (n_steps doubles,
  * may be NULL) receives each batch's value before its update. */
 int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host);
+/* Training objective of cp_flow_train and the data-parallel steps: the relative p-th moment of
+ * the weights <w^p>/<w>^p, 2 <= p <= 8 (default 2: <w^2>/<w>^2 = 1 + Var[w]/sigma^2, the weight
+ * variance).  A larger p weighs the tail of the weights, which sets the unweighting efficiency at
+ * a high-quantile w_max.  The reported batch loss stays <w^2>/<w>^2. */
+int cp_flow_set_objective(cp_handle* h, double p);
 /* The training gradient of one batch (counter iteration iter, stream 2) without an update. */
 int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, float* grad_host, double* loss_host);
 /* Data-parallel training (no reference counterpart): one step of cp_flow_train in three calls,

@@ -7,8 +7,11 @@
 #                                 pipeline/physics.cuh) compiled as plain C++ (oracle/ref_cupythia.cc)
 #   oracle/_ref/xmldoc/, tunes/   copies of Pythia's settings database and tune files, read at init
 #
-# Usage: make -f oracle/ref.mk -j8 REF=/root/reference
-REF     ?= /root/reference
+# Usage: make -f oracle/ref.mk -j8 REF=<reference root>   (or CUPYTHIA_REFERENCE in the environment)
+REF     ?= $(CUPYTHIA_REFERENCE)
+ifeq ($(strip $(REF)),)
+$(error set REF=<reference root> or CUPYTHIA_REFERENCE)
+endif
 PY8     := $(REF)/pythia8317
 OUT     := oracle/_ref
 CXX     ?= g++

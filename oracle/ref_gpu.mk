@@ -13,8 +13,11 @@
 # The reference builds them with `nvcc -O3 [-std=c++17] -arch=sm_120`; here the same flags with
 # the B200's architecture.
 #
-# Usage: make -f oracle/ref_gpu.mk -j8 REF=/root/reference
-REF   ?= /root/reference
+# Usage: make -f oracle/ref_gpu.mk -j8 REF=<reference root>   (or CUPYTHIA_REFERENCE in the environment)
+REF   ?= $(CUPYTHIA_REFERENCE)
+ifeq ($(strip $(REF)),)
+$(error set REF=<reference root> or CUPYTHIA_REFERENCE)
+endif
 CUP   := $(REF)/cuPythia
 OUT   := oracle/_ref/gpu
 NVCC  ?= nvcc

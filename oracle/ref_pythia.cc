@@ -8,7 +8,8 @@
 //                                       "x1 x2 sH tH"                (SigmaProcess.cc:423-480,846-925)
 //   gen    <nAccepted> <seed> <threads> [pTmin] [aSmZ]
 //                                       ProcessLevel-only HardQCD generation, one Pythia per thread,
-//                                       prints tried/accepted/s and sigmaGen +- sigmaErr
+//                                       prints tried/accepted, the seconds of generation alone
+//                                       (after every thread's init), the init seconds, sigmaGen +- sigmaErr
 //   lhef   <file> [shower]              reads a Les Houches Event File back (Beams:frameType = 4);
 //                                       with shower = 1 also showers (MPI off) and hadronizes every
 //                                       event, which needs a valid colour flow; prints counts and
@@ -19,6 +20,8 @@
 #include "Pythia8/Pythia.h"
 #include "Pythia8/SigmaQCD.h"
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -114,14 +117,32 @@ static int cmd_sigma(const char* path)
 
 struct GenResult { long tried = 0, accepted = 0; double sigma = 0, err = 0; };
 
+// Every worker constructs and initialises its own Pythia (including the sigma_max scan of
+// PhaseSpace::setupSampling), then waits until all workers are ready; the clock runs only around
+// the Pythia::next() loops, so the timed region is event generation alone, as on the GPU side
+// (where adaptation and training are outside the timed region too).  The initialisation time is
+// reported separately ("init_seconds", the slowest worker's).
 static int cmd_gen(long nAcc, int seed, int threads, double pTmin, double aSmZ)
 {
   std::vector<GenResult> res(threads);
-  std::vector<double> initT(threads);
+  std::vector<double> initT(threads, 0.0);
+  std::mutex mu;
+  std::condition_variable cv;
+  int ready = 0;
+  bool go = false;
   auto worker = [&](int t) {
+    const auto i0 = std::chrono::steady_clock::now();
     Pythia p(xmlDir(), false);
     configure(p, pTmin, aSmZ, true, seed + t);
-    if (!p.init()) return;
+    const bool ok = p.init();
+    initT[t] = std::chrono::duration<double>(std::chrono::steady_clock::now() - i0).count();
+    {
+      std::unique_lock<std::mutex> lock(mu);
+      ++ready;
+      cv.notify_all();
+      cv.wait(lock, [&] { return go; });
+    }
+    if (!ok) return;
     long per = nAcc / threads + (t < nAcc % threads ? 1 : 0);
     for (long i = 0; i < per; ++i) p.next();
     res[t].tried = p.info.nTried();
@@ -129,22 +150,31 @@ static int cmd_gen(long nAcc, int seed, int threads, double pTmin, double aSmZ)
     res[t].sigma = p.info.sigmaGen();
     res[t].err = p.info.sigmaErr();
   };
-  auto t0 = std::chrono::steady_clock::now();
   std::vector<std::thread> th;
   for (int t = 0; t < threads; ++t) th.emplace_back(worker, t);
+  std::chrono::steady_clock::time_point t0;
+  {
+    std::unique_lock<std::mutex> lock(mu);
+    cv.wait(lock, [&] { return ready == threads; });
+    t0 = std::chrono::steady_clock::now();
+    go = true;
+  }
+  cv.notify_all();
   for (auto& x : th) x.join();
   double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   long tried = 0, acc = 0;
-  double wsum = 0, w2 = 0;
-  for (auto& r : res) {
+  double wsum = 0, w2 = 0, initMax = 0;
+  for (int t = 0; t < threads; ++t) {
+    const GenResult& r = res[t];
     tried += r.tried;
     acc += r.accepted;
     if (r.err > 0) { wsum += r.sigma / (r.err * r.err); w2 += 1.0 / (r.err * r.err); }
+    if (initT[t] > initMax) initMax = initT[t];
   }
   double sig = w2 > 0 ? wsum / w2 : 0, err = w2 > 0 ? 1.0 / sqrt(w2) : 0;
-  printf("{\"tried\": %ld, \"accepted\": %ld, \"seconds\": %.6f, \"threads\": %d, "
+  printf("{\"tried\": %ld, \"accepted\": %ld, \"seconds\": %.6f, \"init_seconds\": %.6f, \"threads\": %d, "
          "\"sigma_mb\": %.8g, \"sigma_err_mb\": %.8g}\n",
-         tried, acc, sec, threads, sig, err);
+         tried, acc, sec, initMax, threads, sig, err);
   return 0;
 }
 

@@ -195,6 +195,35 @@ def test_training_is_reproducible():
     assert np.array_equal(runs[0][0], runs[1][0])
 
 
+def test_training_resumes_from_a_checkpoint_bit_for_bit():
+    """A training interrupted after k updates, checkpointed (parameters, Adam moments, update
+    count), restored into a fresh handle on the same grid and trained for m more updates ends
+    with the parameters and losses of k + m uninterrupted updates, bit for bit."""
+    import cupythia_b200 as cp
+    k, m = 12, 9
+    with cp.Integrator() as it:
+        it.integrate(3, 1 << 20, alpha=1.5)
+        grid = it.grid
+        it.flow_init(7)
+        loss_all = np.asarray(it.flow_train(k + m, 65536, lr=8e-3)).copy()
+        p_all = it.flow_params.copy()
+    with cp.Integrator() as it:
+        it.grid = grid
+        it.flow_init(7)
+        loss_a = np.asarray(it.flow_train(k, 65536, lr=8e-3)).copy()
+        state, updates = it.flow_state()
+    assert updates == k and state.size == 3 * p_all.size
+    with cp.Integrator() as it:
+        it.grid = grid
+        it.flow_restore(state, updates)
+        assert np.array_equal(it.flow_params, state[:p_all.size])
+        loss_b = np.asarray(it.flow_train(m, 65536, lr=8e-3)).copy()
+        again, n_up = it.flow_state()
+        assert n_up == k + m
+        assert np.array_equal(np.concatenate([loss_a, loss_b]), loss_all)
+        assert np.array_equal(it.flow_params, p_all)
+
+
 def test_expired_tensor_core_wait_is_reported_and_recoverable(integ):
     """Failure detection without a GPU fault: the test hook stops MMA issue, so the epilogue's
     bounded waits expire (about 1 s); the call must return CP_ERR_TIMEOUT (4), and the next call

@@ -1,8 +1,8 @@
 """The allocation-free VEGAS pass (cp_vegas_pass_noalloc) against the handle's pass.
 
-Some callers cannot allocate device memory (code inside a CUDA graph under capture, a host
-program that owns every device allocation under a fixed budget); cp_vegas_pass_noalloc serves
-them from a file-scope device array.  Its sums and histograms must equal those of
+Some callers cannot allocate device memory (a host program that owns every device allocation, a
+process under a fixed memory budget, a plugin inside another program's event loop);
+cp_vegas_pass_noalloc serves them from a file-scope device array.  Its sums and histograms must equal those of
 cp_vegas_iteration on the same grid and counter iteration, on consecutive calls (the array keeps
 the previous call's contents, so a second call checks that nothing leaks between calls).
 Collected last on purpose: a run that stops at the first failure has run everything else first.
