@@ -161,7 +161,14 @@ def measured_peaks():
 # --------------------------------------------------------------------------- our arm
 # algorithmic work per point of the two dominant kernels
 UNW_CHUNK = 1 << 24               # points per production chunk of the library (accept/scan/build launches)
-FP32_FLOP_PER_POINT = 3278.0      # k_unw_accept: FADD + FMUL + 2 FFMA per point (ncu SASS counters, profiles/)
+# k_unw_accept, algorithmic: the integrand's operations per point counted on its least-arithmetic
+# FP64 restatement (oracle/cp_opcount.cc, pinned by tests/test_opcount.py): 364 add + 422 mul + 9
+# div FP32 ops, 35 exp + 26 log + 2 sqrt + 9 reciprocals on the MUFU
+ALG_FP32_OPS_PER_POINT = 795
+ALG_MUFU_OPS_PER_POINT = 72
+# k_unw_accept, executed: FADD + FMUL + 2 FFMA per point from the ncu SASS counters (profiles/),
+# i.e. the algorithm plus the FP32 precision bookkeeping (compensated sums, (hi, lo) logarithms)
+EXEC_FLOP_PER_POINT = 3278.0
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
 # launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points
@@ -339,13 +346,28 @@ def run_ours(a):
     fp32_peak, mufu_peak = it.measure_peaks()
     acc_ms, acc_n = kt_f["accept"]
     flow_ms, flow_n = kt_f["flow_forward"]
-    roof_acc = FP32_FLOP_PER_POINT * n / (acc_ms / acc_n / 1e3) / 1e12
+    pts_per_s = n / (acc_ms / acc_n / 1e3)
+    # the integrand's bound (SIMT FP32 and MUFU co-limited): algorithmic FP32 operations per second
+    # against the FP32 issue peak (one operation per lane and cycle = half the FMA-chain TFLOP/s,
+    # which counts an FMA as two), and MUFU operations against the measured MUFU peak; the larger
+    # fraction is the roofline
+    fp32_op_peak = fp32_peak / 2.0
+    ops_acc = ALG_FP32_OPS_PER_POINT * pts_per_s / 1e12
+    mufu_acc = ALG_MUFU_OPS_PER_POINT * pts_per_s / 1e12
     roof_flow = FLOW_FLOP_PER_POINT * n / (flow_ms / flow_n / 1e3) / 1e12
     bf16_peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
-    r_acc = {"bound": "fp32", "kernel": "k_unw_accept", "achieved": roof_acc, "peak": fp32_peak,
-             "unit": "TFLOP/s", "frac": roof_acc / fp32_peak,
-             "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks)",
-             "flop_per_point": FP32_FLOP_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_unw_accept"] * n,
+    r_acc = {"bound": "fp32", "kernel": "k_unw_accept", "achieved": ops_acc, "peak": fp32_op_peak,
+             "unit": "TFLOP/s", "frac": max(ops_acc / fp32_op_peak, mufu_acc / mufu_peak),
+             "basis": "algorithmic FP32 operations per point (add + mul + div = %d, oracle/cp_opcount.cc) "
+                      "per second against the FP32 issue peak (one op per lane-cycle); frac = max of that "
+                      "and the MUFU fraction" % ALG_FP32_OPS_PER_POINT,
+             "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks), "
+                            "%.1f TFLOP/s at 2 per FMA" % fp32_peak,
+             "fp32_frac": ops_acc / fp32_op_peak, "mufu_frac": mufu_acc / mufu_peak,
+             "mufu_achieved_tops": mufu_acc, "mufu_ops_per_point": ALG_MUFU_OPS_PER_POINT,
+             "executed_flop_per_point": EXEC_FLOP_PER_POINT,
+             "executed_frac": EXEC_FLOP_PER_POINT * pts_per_s / 1e12 / fp32_peak,
+             "flop_per_point": ALG_FP32_OPS_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_unw_accept"] * n,
              "ms_per_launch": acc_ms / acc_n}
     r_flow = {"bound": "tensor", "kernel": "k_flow_fwd_tc", "achieved": roof_flow, "peak": bf16_peak,
               "unit": "TFLOP/s", "frac": roof_flow / bf16_peak,

@@ -108,6 +108,7 @@ SIGNATURES = {
     "cp_splitmix_uniforms": [_P, _u64, _u64, _u64, _P],
     "cp_event_keys": [_P, _u64, _u64, _u64, _P],
     "cp_set2kin_batch": [_P, _P, _P, _P, _P, _i64],
+    "cp_set2kin_batch_f64": [_P, _P, _P, _P, _P, _i64],
     "cp_sigma_kin_batch": [_P, _i, _P],
     "cp_sigma_hat_batch": [_P, _i, _i, _i, _P],
     "cp_sigma_pdf_batch": [_P, _i, _P],
@@ -146,6 +147,7 @@ SIGNATURES = {
     "cp_flow_select_kernel": [_P, _i],
     "cp_flow_test_stall": [_P, _i],
     "cp_colour_tags": [C.c_uint16, C.c_uint16, _P, _P],
+    "cp_set_id_col_acol": [_i, _i, _i, _d, _d, _i, _d, _d, _d, _P, _P, _P],
     "cp_write_lhef": [C.POINTER(cp_config), _P, _u64, _d, _d, C.c_char_p],
     "cp_flow_train": [_P, _i, _u64, _d, _P],
     "cp_flow_set_objective": [_P, _d],

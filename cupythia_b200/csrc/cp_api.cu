@@ -50,7 +50,7 @@ int cp_ensure_iters(cp_handle* h, int n)
 static int ensure_kin(cp_handle* h, int64_t n)
 {
   if (n <= h->kin_cap) return CP_OK;
-  float** bufs[7] = {&h->d_x1, &h->d_x2, &h->d_sH, &h->d_tH, &h->d_as, &h->d_q2r, &h->d_q2f};
+  float** bufs[8] = {&h->d_x1, &h->d_x2, &h->d_sH, &h->d_tH, &h->d_uH, &h->d_as, &h->d_q2r, &h->d_q2f};
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   for (auto b : bufs) {
     if (*b) CP_CUDA(h, cudaFree(*b));
@@ -152,7 +152,7 @@ extern "C" int cp_destroy(cp_handle* h)
   if (h->gen_copy) cudaStreamDestroy(h->gen_copy);
   if (h->h_gen_cnt) cudaFreeHost(h->h_gen_cnt);
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
-                  h->d_tH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq, h->d_flow, h->d_flow_pk,
+                  h->d_tH, h->d_uH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq, h->d_flow, h->d_flow_pk,
                   h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_pdfbuf,
                   h->d_gen_stage, h->d_gen_red, h->d_gen_cnt, h->d_ftrain, h->d_tails, h->d_bmask,
                   h->d_rsum, h->d_roff, h->d_unw_red};
@@ -313,13 +313,38 @@ extern "C" int cp_event_keys(cp_handle* h, uint64_t base, uint64_t e0, uint64_t 
 // SigmaProcess surface
 // ------------------------------------------------------------------------------------------
 __global__ void k_set2kin(const CpHadParams P, int64_t n, const float* __restrict__ sH,
-                          const float* __restrict__ tH, float* as, float* q2r, float* q2f)
+                          const float* __restrict__ tH, float* uH, float* as, float* q2r, float* q2f)
 {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     float s = sH[i], t = tH[i], u = -(s + t);
     float pT2 = t * u / s;
     float qr = P.kR * pT2, qf = P.kF * pT2;
+    uH[i] = u;
+    q2r[i] = qr;
+    q2f[i] = qf;
+    as[i] = cp_alphas(P, qr);
+  }
+}
+
+// The same from FP64 kinematics (what Pythia's set2Kin receives): uHat = -(sHat + tHat) and
+// pT^2 = tHat uHat / sHat are formed in FP64 and only then rounded, so a small |uHat| (a large
+// sHat near the pT cut, where the FP32 sum of sHat and tHat would cancel) keeps its precision.
+__global__ void k_set2kin_f64(const CpHadParams P, int64_t n, const double* __restrict__ x1d,
+                              const double* __restrict__ x2d, const double* __restrict__ sHd,
+                              const double* __restrict__ tHd, float* x1, float* x2, float* sH, float* tH,
+                              float* uH, float* as, float* q2r, float* q2f)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double s = sHd[i], t = tHd[i], u = -(s + t);
+    const float pT2 = (float)(t * u / s);
+    const float qr = P.kR * pT2, qf = P.kF * pT2;
+    x1[i] = (float)x1d[i];
+    x2[i] = (float)x2d[i];
+    sH[i] = (float)s;
+    tH[i] = (float)t;
+    uH[i] = (float)u;
     q2r[i] = qr;
     q2f[i] = qf;
     as[i] = cp_alphas(P, qr);
@@ -330,15 +355,15 @@ __global__ void k_set2kin(const CpHadParams P, int64_t n, const float* __restric
 __global__ void k_sigma(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n, int which, int code,
                         int id1, int id2, int mask, const float* __restrict__ x1,
                         const float* __restrict__ x2, const float* __restrict__ sH,
-                        const float* __restrict__ tH, const float* __restrict__ as,
-                        const float* __restrict__ q2f, float* out)
+                        const float* __restrict__ tH, const float* __restrict__ uH,
+                        const float* __restrict__ as, const float* __restrict__ q2f, float* out)
 {
   __shared__ CpCteqPoly cteq[8];
   cp_stage_cteq(cteq, cteq_g);
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    float s = sH[i], t = tH[i], u = -(s + t);
+    float s = sH[i], t = tH[i], u = uH[i];
     float tp = t / s, up = u / s;
     CpBrackets b;
     cp_brackets(P, tp, up, b);
@@ -373,7 +398,8 @@ __global__ void k_sigma(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n
 __global__ void k_pick_state(const CpHadParams P, const CpCteqPoly* cteq_g, int64_t n, int k,
                              const float* __restrict__ x1, const float* __restrict__ x2,
                              const float* __restrict__ sH, const float* __restrict__ tH,
-                             const float* __restrict__ q2f, const float4* __restrict__ r,
+                             const float* __restrict__ uH, const float* __restrict__ q2f,
+                             const float4* __restrict__ r,
                              short4* __restrict__ ids, uint16_t* __restrict__ colour)
 {
   __shared__ CpCteqPoly cteq[8];
@@ -381,7 +407,7 @@ __global__ void k_pick_state(const CpHadParams P, const CpCteqPoly* cteq_g, int6
   __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    const float s = sH[i], t = tH[i], u = -(s + t);
+    const float s = sH[i], t = tH[i], u = uH[i];
     const float tp = t / s, up = u / s;
     CpPoint pt;
     cp_brackets(P, tp, up, pt.b);
@@ -427,8 +453,25 @@ extern "C" int cp_set2kin_batch(cp_handle* h, const float* x1, const float* x2, 
   CP_CUDA(h, cudaMemcpyAsync(h->d_x2, x2, bytes, cudaMemcpyDeviceToDevice, h->stream));
   CP_CUDA(h, cudaMemcpyAsync(h->d_sH, sH, bytes, cudaMemcpyDeviceToDevice, h->stream));
   CP_CUDA(h, cudaMemcpyAsync(h->d_tH, tH, bytes, cudaMemcpyDeviceToDevice, h->stream));
-  k_set2kin<<<grid_for(h, n), 256, 0, h->stream>>>(h->P, n, h->d_sH, h->d_tH, h->d_as, h->d_q2r, h->d_q2f);
+  k_set2kin<<<grid_for(h, n), 256, 0, h->stream>>>(h->P, n, h->d_sH, h->d_tH, h->d_uH, h->d_as, h->d_q2r, h->d_q2f);
   CP_LAUNCH_CHECK(h, "k_set2kin");
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  return CP_OK;
+}
+
+extern "C" int cp_set2kin_batch_f64(cp_handle* h, const double* x1, const double* x2, const double* sH,
+                                    const double* tH, int64_t n)
+{
+  CP_CHECK_HANDLE(h);
+  if (n < 0 || (n > 0 && (!x1 || !x2 || !sH || !tH)))
+    return cp_fail(h, CP_ERR_INVALID, "cp_set2kin_batch_f64: bad arguments");
+  int rc = ensure_kin(h, n > 0 ? n : 1);
+  if (rc) return rc;
+  h->kin_n = n;
+  if (!n) return CP_OK;
+  k_set2kin_f64<<<grid_for(h, n), 256, 0, h->stream>>>(h->P, n, x1, x2, sH, tH, h->d_x1, h->d_x2, h->d_sH, h->d_tH,
+                                                       h->d_uH, h->d_as, h->d_q2r, h->d_q2f);
+  CP_LAUNCH_CHECK(h, "k_set2kin_f64");
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return CP_OK;
 }
@@ -438,8 +481,8 @@ static int sigma_launch(cp_handle* h, int which, int code, int id1, int id2, int
   if (h->kin_n == 0) return CP_OK;
   if (!out) return cp_fail(h, CP_ERR_INVALID, "null output");
   k_sigma<<<grid_for(h, h->kin_n), 256, 0, h->stream>>>(h->P, h->d_cteq, h->kin_n, which, code, id1, id2, mask,
-                                                         h->d_x1, h->d_x2, h->d_sH, h->d_tH, h->d_as,
-                                                         h->d_q2f, out);
+                                                         h->d_x1, h->d_x2, h->d_sH, h->d_tH, h->d_uH,
+                                                         h->d_as, h->d_q2f, out);
   CP_LAUNCH_CHECK(h, "k_sigma");
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return CP_OK;
@@ -477,7 +520,7 @@ extern "C" int cp_pick_state_batch(cp_handle* h, int code, const float* r_dev, i
   if (!r_dev || !ids_dev || !colour_dev || ((uintptr_t)r_dev & 15) || ((uintptr_t)ids_dev & 7))
     return cp_fail(h, CP_ERR_INVALID, "cp_pick_state_batch: r (16-byte aligned) and ids (8-byte aligned) required");
   k_pick_state<<<grid_for(h, h->kin_n), 256, 0, h->stream>>>(h->P, h->d_cteq, h->kin_n, code - 111, h->d_x1, h->d_x2,
-                                                             h->d_sH, h->d_tH, h->d_q2f,
+                                                             h->d_sH, h->d_tH, h->d_uH, h->d_q2f,
                                                              reinterpret_cast<const float4*>(r_dev),
                                                              reinterpret_cast<short4*>(ids_dev), colour_dev);
   CP_LAUNCH_CHECK(h, "k_pick_state");

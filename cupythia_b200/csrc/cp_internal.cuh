@@ -108,6 +108,7 @@ struct cp_handle {
   int64_t kin_n = 0, kin_cap = 0;
   float *d_x1 = nullptr, *d_x2 = nullptr, *d_sH = nullptr, *d_tH = nullptr;
   float *d_as = nullptr, *d_q2r = nullptr, *d_q2f = nullptr;
+  float* d_uH = nullptr;          // uHat, formed at the input precision (FP64 for cp_set2kin_batch_f64)
   // launch shapes (resident blocks per SM on this handle's device; -1 until first use)
   int had_blocks = 0;
   int adj_per_sm = -1, flow_per_sm = -1, unw_per_sm = -1;

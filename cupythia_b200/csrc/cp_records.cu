@@ -20,6 +20,37 @@ extern "C" int cp_colour_tags(uint16_t process, uint16_t colour, int col[4], int
   return cp_colour_expand(process, colour, col, acol) ? CP_OK : CP_ERR_INVALID;
 }
 
+// One event's Sigma2*::setIdColAcol on the host, with the record builder's code (cp_colour_flow,
+// cp_colour_expand) at FP32: the outgoing flavours and the colour tags of process `code` for the
+// incoming pair (id1, id2) at tHat/sHat = t_over_s, uHat/sHat = u_over_s.
+extern "C" int cp_set_id_col_acol(int code, int id1, int id2, double t_over_s, double u_over_s, int n_quark_new,
+                                  double r_flavour, double r_colour, double r_swap, int ids_out[4], int col[4],
+                                  int acol[4])
+{
+  if (code < 111 || code > 115 || !ids_out || !col || !acol || !(t_over_s < 0.0) || !(u_over_s < 0.0) ||
+      n_quark_new < 1 || n_quark_new > 5)
+    return CP_ERR_INVALID;
+  const bool gin1 = id1 == 21, gin2 = id2 == 21;
+  const bool q1 = id1 != 0 && id1 >= -5 && id1 <= 5, q2 = id2 != 0 && id2 >= -5 && id2 <= 5;
+  const bool ok = (code == 111 || code == 112) ? (gin1 && gin2)
+                  : code == 113                ? ((q1 && gin2) || (gin1 && q2))
+                  : code == 114                ? (q1 && q2)
+                                               : (q1 && q2 && id2 == -id1);
+  if (!ok) return CP_ERR_INVALID;
+  int id[4] = {id1, id2, id1, id2};
+  if (code == 111 || code == 115) { id[2] = 21; id[3] = 21; }
+  if (code == 112) {
+    int qn = 1 + (int)((float)n_quark_new * (float)r_flavour);
+    if (qn > n_quark_new) qn = n_quark_new;
+    id[2] = qn;
+    id[3] = -qn;
+  }
+  const uint32_t flow = cp_colour_flow(code, id, (float)t_over_s, (float)u_over_s, (float)r_colour, (float)r_swap);
+  if (!cp_colour_expand((uint16_t)code, (uint16_t)flow, col, acol)) return CP_ERR_INVALID;
+  for (int k = 0; k < 4; ++k) ids_out[k] = id[k];
+  return CP_OK;
+}
+
 // LHEF tag of a colour index (0 = none)
 static inline int lhef_tag(int c) { return c ? 500 + c : 0; }
 

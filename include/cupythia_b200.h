@@ -139,6 +139,11 @@ int cp_event_keys(cp_handle* h, uint64_t base, uint64_t e0, uint64_t n, uint64_t
  * uHat, pT^2, Q2Ren, Q2Fac and alpha_s.  Inputs are dev SoA arrays of n points. */
 int cp_set2kin_batch(cp_handle* h, const float* x1, const float* x2, const float* sH,
                      const float* tH, int64_t n);
+/* The same from FP64 device arrays, the precision of Pythia's set2Kin arguments: uHat and pT^2
+ * are formed in FP64 before the batch is rounded to FP32, so points at large sHat near the pT
+ * cut (|uHat| << sHat, where an FP32 sHat + tHat cancels) keep FP32 relative precision. */
+int cp_set2kin_batch_f64(cp_handle* h, const double* x1, const double* x2, const double* sH,
+                         const double* tH, int64_t n);
 /* Batched sigmaKin + sigmaHat of the flavour-independent processes 111, 112, 113, 115
  * (pythia8317/src/SigmaQCD.cc:115-325): dsigmaHat/dtHat in GeV^-4, one value per point. */
 int cp_sigma_kin_batch(cp_handle* h, int process_code, float* out_dev);
@@ -395,6 +400,16 @@ int cp_records_to_device_events(cp_handle* h, const cp_event* records_dev, uint6
  * its process code and encoded colour flow, as the process's setIdColAcol sets them
  * (pythia8317/src/SigmaQCD.cc:135-342, setColAcol + swapColAcol / swapCol1234). */
 int cp_colour_tags(uint16_t process, uint16_t colour, int col[4], int acol[4]);
+/* Host-only (no GPU needed).  One event's Sigma2*::setIdColAcol (pythia8317/src/SigmaQCD.cc:
+ * 135-148, 195-205, 232-244, 292-304, 331-342) for process `code` 111..115 with incoming
+ * (id1, id2): the outgoing flavours (g g -> q qbar: 1 + int(n_quark_new r_flavour), the new
+ * flavour its sigmaKin draws) and the colour tags (1..4, 0 = none) of the topology drawn with
+ * r_colour in proportion to its kinematic term at tHat/sHat, uHat/sHat, g g -> g g oriented by
+ * r_swap, then the swaps for antiquarks and a leading gluon.  The same code as the record
+ * builder's colour flow; the Pythia adapter's setIdColAcol calls it with Pythia's own draws.
+ * CP_ERR_INVALID for a pair the process does not accept. */
+int cp_set_id_col_acol(int code, int id1, int id2, double t_over_s, double u_over_s, int n_quark_new,
+                       double r_flavour, double r_colour, double r_swap, int ids_out[4], int col[4], int acol[4]);
 /* Writes n host records as a Les Houches Event File 3.0 (the reference's LHE writers:
  * cuPythia/pipeline/lhe_writer.cu:46-70, cuPythia/07_unweighting_lhe/unweight_lhe.cu:74-102):
  * beams and PDF set from cfg, one <init> line per process present with XSECUP = sigma x its

@@ -42,6 +42,8 @@ _SIG = {
     "cpo_had_default": (None, [C.c_void_p]),
     "cpo_had_sigma_pdf": (None, [C.c_void_p, _D, _D, _D, _D, C.c_int, _PD]),
     "cpo_had_weight_x": (_D, [C.c_void_p, _PD, _PD]),
+    "cpo_opcount_weight": (_D, [C.c_void_p, _PD]),
+    "cpo_opcount_counts": (None, [C.c_void_p, C.c_void_p, C.c_int64, _PD]),
     "cpo_had_weight_x_batch": (None, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int]),
     "cpo_vegas_map": (_D, [_PD, C.c_int, C.POINTER(_U32), _PD, C.POINTER(C.c_int)]),
     "cpo_had_point_weight": (_D, [C.c_void_p, _PD, C.c_int, _U64, _U32, _U64, C.POINTER(C.c_int), _PD]),
@@ -58,6 +60,10 @@ _SIG = {
     "cpo_pick_state": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int),
                                  C.POINTER(C.c_int)]),
     "cpo_pick_record": (C.c_int, [C.c_void_p, _PD, _D, _D, _D, _D, _D, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "cpo_pick_state_margin": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), _PD]),
+    "cpo_pick_record_margin": (C.c_int, [C.c_void_p, _PD, _D, _D, _D, _D, _D, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), _PD]),
     "cpo_flow_forward": (None, [C.c_void_p, _PD, _PD, _PD]),
     "cpo_flow_set_rounding": (None, [C.c_int]),
     "cpo_flow_backward_batch": (None, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
@@ -132,19 +138,24 @@ def cupythia_ref():
     return L
 
 
-def pick_record(cfg, x, r0, r1, r3, rc, rs):
-    """(code, ids[4], colour) of the oracle's record picks at the point x (cpo_pick_record)."""
+def pick_record(cfg, x, r0, r1, r3, rc, rs, with_margin=False):
+    """(code, ids[4], colour) of the oracle's record picks at the point x (cpo_pick_record); with
+    with_margin also the draws' smallest relative distance from a selection boundary."""
     ids = (C.c_int * 4)()
     col = C.c_int()
+    m = C.c_double()
     xx = np.ascontiguousarray(np.asarray(x, np.float64))
-    code = lib().cpo_pick_record(C.byref(cfg), dptr(xx), r0, r1, r3, rc, rs, ids, C.byref(col))
-    return code, list(ids), col.value
+    code = lib().cpo_pick_record_margin(C.byref(cfg), dptr(xx), r0, r1, r3, rc, rs, ids, C.byref(col), C.byref(m))
+    return (code, list(ids), col.value, m.value) if with_margin else (code, list(ids), col.value)
 
 
-def pick_state(cfg, code, x1, x2, sH, tH, r1, r3, rc, rs):
-    """(code or 0, ids[4], colour) of the oracle's pickInState + setIdColAcol at given kinematics."""
+def pick_state(cfg, code, x1, x2, sH, tH, r1, r3, rc, rs, with_margin=False):
+    """(code or 0, ids[4], colour) of the oracle's pickInState + setIdColAcol at given kinematics;
+    with with_margin also the draws' smallest relative distance from a selection boundary."""
     ids = (C.c_int * 4)()
     col = C.c_int()
-    got = lib().cpo_pick_state(C.byref(cfg), code, x1, x2, sH, tH, r1, r3, rc, rs, ids, C.byref(col))
-    return got, list(ids), col.value
+    m = C.c_double()
+    got = lib().cpo_pick_state_margin(C.byref(cfg), code, x1, x2, sH, tH, r1, r3, rc, rs, ids, C.byref(col),
+                                      C.byref(m))
+    return (got, list(ids), col.value, m.value) if with_margin else (got, list(ids), col.value)
 

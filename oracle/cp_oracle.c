@@ -126,6 +126,17 @@ static const double CTEQ5L_AM[8][9][3] = {
    {-0.1327377E+02, 0.1201754E+02, -0.6277844E+01}, {0.0, 0.0, 0.0},
    {0.0, 0.0, 0.0}}};
 
+/* read-only view of the tables above (the operation-count restatement, cp_opcount.cc) */
+void cpo_cteq5l_table(const double** am, const double** qmin, const double** alpha, const double** ut1,
+                      const double** ut2)
+{
+  *am = &CTEQ5L_AM[0][0][0];
+  *qmin = CTEQ5L_QMIN;
+  *alpha = CTEQ5L_ALPHA;
+  *ut1 = CTEQ5L_UT1;
+  *ut2 = CTEQ5L_UT2;
+}
+
 /* ======================= the integrand, twice ======================= */
 #define REAL double
 #define FN(n) n##_r
@@ -316,8 +327,16 @@ static void pick_lists(const cpo_had_cfg* c, double x1, double x2, double sH, do
 /* pickInState of process k with r1 (the first pair whose running sum of pair terms reaches
  * r1 x the process total; the last pair if rounding leaves none), the new flavour of
  * Sigma2gg2qqbar::sigmaKin (SigmaQCD.cc:173) from r3, and setIdColAcol's colour flow from rc, rs. */
+/* The smallest distance of a draw from a selection boundary of this pick, relative to the
+ * quantity it selects from (the process or pair total, the topology sum, the flavour count):
+ * a pick whose margin is above the FP32 rounding of those sums is decided the same way in FP32. */
+static void margin_upd(double* m, double v)
+{
+  if (m && v < *m) *m = v;
+}
+
 static int pick_finish(const cpo_had_cfg* c, int k, const cpo_pairs* L, double r1, double r3, double rc,
-                       double rs, int id[4], int* colour)
+                       double rs, int id[4], int* colour, double* margin)
 {
   const int (*pa)[128] = (const int (*)[128])L->pa, (*pb)[128] = (const int (*)[128])L->pb;
   const int* np = L->np;
@@ -331,6 +350,13 @@ static int pick_finish(const cpo_had_cfg* c, int k, const cpo_pairs* L, double r
     u -= ps[k][i];
     if (u <= 0.0) break;
   }
+  if (margin) {
+    double cum = 0.0;
+    for (int j = 0; j < np[k] - 1; ++j) {
+      cum += ps[k][j];
+      margin_upd(margin, fabs(r1 * tot[k] - cum) / tot[k]);
+    }
+  }
   const int a = pa[k][i], b = pb[k][i];
   id[0] = a; id[1] = b;
   if (k == 0 || k == 4) { id[2] = 21; id[3] = 21; }
@@ -338,6 +364,8 @@ static int pick_finish(const cpo_had_cfg* c, int k, const cpo_pairs* L, double r
     int qn = 1 + (int)(c->nQuarkNew * r3);
     if (qn > c->nQuarkNew) qn = c->nQuarkNew;
     id[2] = qn; id[3] = -qn;
+    const double v = c->nQuarkNew * r3;
+    for (int j = 1; j < c->nQuarkNew; ++j) margin_upd(margin, fabs(v - j) / c->nQuarkNew);
   } else { id[2] = a; id[3] = b; }
   /* colour flow */
   const double sH2 = sH * sH, tH2 = tH * tH, uH2 = uH * uH;
@@ -349,50 +377,64 @@ static int pick_finish(const cpo_had_cfg* c, int k, const cpo_pairs* L, double r
     const double r = (sTS + sUS + sTU) * rc;
     topo = r < sTS ? 0 : (r < sTS + sUS ? 1 : 2);
     swapCA = rs > 0.5;
+    margin_upd(margin, fabs(r - sTS) / (sTS + sUS + sTU));
+    margin_upd(margin, fabs(r - sTS - sUS) / (sTS + sUS + sTU));
+    margin_upd(margin, fabs(rs - 0.5));
   } else if (k == 1) {
     const double sTS = (1. / 6.) * uH / tH - (3. / 8.) * uH2 / sH2;
     const double sUS = (1. / 6.) * tH / uH - (3. / 8.) * tH2 / sH2;
     topo = (sTS + sUS) * rc < sTS ? 0 : 1;
+    margin_upd(margin, fabs((sTS + sUS) * rc - sTS) / fabs(sTS + sUS));
   } else if (k == 2) {
     const double sTS = uH2 / tH2 - (4. / 9.) * uH / sH;
     const double sTU = sH2 / tH2 - (4. / 9.) * sH / uH;
     topo = (sTS + sTU) * rc < sTS ? 0 : 1;
+    margin_upd(margin, fabs((sTS + sTU) * rc - sTS) / fabs(sTS + sTU));
     swap12 = id[0] == 21;
     swapCA = id[0] < 0 || id[1] < 0;
   } else if (k == 3) {
     const double sT = (4. / 9.) * (sH2 + uH2) / tH2, sU = (4. / 9.) * (sH2 + tH2) / uH2;
     topo = id[0] * id[1] > 0 ? 0 : 1;
     if (id[1] == id[0] && (sT + sU) * rc > sT) topo = 2;
+    if (id[1] == id[0]) margin_upd(margin, fabs((sT + sU) * rc - sT) / (sT + sU));
     swapCA = id[0] < 0;
   } else {
     const double sTS = (32. / 27.) * uH / tH - (8. / 3.) * uH2 / sH2;
     const double sUS = (32. / 27.) * tH / uH - (8. / 3.) * tH2 / sH2;
     topo = (sTS + sUS) * rc < sTS ? 0 : 1;
+    margin_upd(margin, fabs((sTS + sUS) * rc - sTS) / fabs(sTS + sUS));
     swapCA = id[0] < 0;
   }
   *colour = topo | (swapCA << 2) | (swap12 << 3);
   return 111 + k;
 }
 
-int cpo_pick_state(const cpo_had_cfg* c, int code, double x1, double x2, double sH, double tH, double r1,
-                   double r3, double rc, double rs, int id[4], int* colour)
+int cpo_pick_state_margin(const cpo_had_cfg* c, int code, double x1, double x2, double sH, double tH, double r1,
+                          double r3, double rc, double rs, int id[4], int* colour, double* margin)
 {
+  if (margin) *margin = 1.0;
   if (code < 111 || code > 115) return 0;
   cpo_pairs L;
   pick_lists(c, x1, x2, sH, tH, &L);
-  return pick_finish(c, code - 111, &L, r1, r3, rc, rs, id, colour);
+  return pick_finish(c, code - 111, &L, r1, r3, rc, rs, id, colour, margin);
 }
 
-int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3, double rc,
-                    double rs, int id[4], int* colour)
+int cpo_pick_state(const cpo_had_cfg* c, int code, double x1, double x2, double sH, double tH, double r1,
+                   double r3, double rc, double rs, int id[4], int* colour)
 {
+  return cpo_pick_state_margin(c, code, x1, x2, sH, tH, r1, r3, rc, rs, id, colour, NULL);
+}
+
+int cpo_pick_record_margin(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3, double rc,
+                           double rs, int id[4], int* colour, double* margin)
+{
+  if (margin) *margin = 1.0;
   double tyz[3];
   if (!(weight_x_r(c, c->aSmZ, c->kR, c->pTmin, x, tyz) > 0.0)) return 0;
   const double s = c->sqrtS * c->sqrtS;
   const double tau = tyz[0], y = tyz[1], z = tyz[2];
-  const double sH = tau * s, tH = -0.5 * sH * (1.0 - z), uH = -0.5 * sH * (1.0 + z);
+  const double sH = tau * s, tH = -0.5 * sH * (1.0 - z);
   const double x1 = sqrt(tau) * exp(y), x2 = sqrt(tau) * exp(-y);
-  (void)uH;
   cpo_pairs L;
   pick_lists(c, x1, x2, sH, tH, &L);
   const double* tot = L.tot;
@@ -402,7 +444,20 @@ int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r
   int k = 0;
   while (k < 4 && (t >= tot[k] || tot[k] <= 0.0)) { t -= tot[k]; ++k; }
   if (tot[k] <= 0.0) { k = 0; while (k < 4 && !(tot[k] > 0.0)) ++k; }
-  return pick_finish(c, k, &L, r1, r3, rc, rs, id, colour);
+  if (margin) {
+    double cum = 0.0;
+    for (int j = 0; j < 4; ++j) {
+      cum += tot[j];
+      margin_upd(margin, fabs(r0 * all - cum) / all);
+    }
+  }
+  return pick_finish(c, k, &L, r1, r3, rc, rs, id, colour, margin);
+}
+
+int cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3, double rc,
+                    double rs, int id[4], int* colour)
+{
+  return cpo_pick_record_margin(c, x, r0, r1, r3, rc, rs, id, colour, NULL);
 }
 
 double cpo_vegas_map(const double* edges, int nb, const uint32_t w[3], double x[3], int bins[3])

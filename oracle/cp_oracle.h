@@ -81,6 +81,16 @@ typedef struct {
 
 void cpo_had_default(cpo_had_cfg* c);
 
+/* ---------------- operation count (cp_opcount.cc) ---------------- */
+/* CTEQ5L coefficient tables: AM [8][9][3], QMIN, ALPHA, UT1, UT2 [8] */
+void   cpo_cteq5l_table(const double** am, const double** qmin, const double** alpha, const double** ut1,
+                        const double** ut2);
+/* the weight of cpo_had_weight_x in the counted (least-arithmetic) form, FP64 */
+double cpo_opcount_weight(const cpo_had_cfg* c, const double x[3]);
+/* mean add, mul, div, exp, log, sqrt per point over n points x (3n doubles), VEGAS map included;
+ * out[6] = largest relative difference of the counted form from cpo_had_weight_x */
+void   cpo_opcount_counts(const cpo_had_cfg* c, const double* x, int64_t n, double out[7]);
+
 /* SigmaProcess surface for one phase-space point (Pythia set2Kin + sigmaKin + sigmaPDF).
  * out[0] = sigmaPDF summed over the selected processes (mb), per Pythia's pair loop.
  * out[1] = alpha_s(muR^2), out[2] = Q2Ren, out[3] = Q2Fac, out[4] = uH, out[5] = pT2. */
@@ -98,6 +108,12 @@ int    cpo_pick_state(const cpo_had_cfg* c, int code, double x1, double x2, doub
                       double r3, double rc, double rs, int id[4], int* colour);
 int    cpo_pick_record(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3,
                        double rc, double rs, int id[4], int* colour);
+/* the same two picks with *margin = the smallest distance of any draw from a selection
+ * boundary, relative to what it selects from (1 when nothing is selected) */
+int    cpo_pick_state_margin(const cpo_had_cfg* c, int code, double x1, double x2, double sH, double tH,
+                             double r1, double r3, double rc, double rs, int id[4], int* colour, double* margin);
+int    cpo_pick_record_margin(const cpo_had_cfg* c, const double x[3], double r0, double r1, double r3,
+                              double rc, double rs, int id[4], int* colour, double* margin);
 double cpo_had_weight_x(const cpo_had_cfg* c, const double x[3], double tyz[3]);
 
 /* VEGAS map of one point given the three 24-bit uniforms m_d = w_d >> 8:

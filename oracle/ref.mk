@@ -6,6 +6,9 @@
 #   oracle/_ref/libcupythia_ref.so cuPythia's host/device headers (common/rng.cuh,
 #                                 pipeline/physics.cuh) compiled as plain C++ (oracle/ref_cupythia.cc)
 #   oracle/_ref/xmldoc/, tunes/   copies of Pythia's settings database and tune files, read at init
+#   oracle/_ref/pythia_plugin_check (target `plugin`, after the CUDA library is built) the test
+#                                 program of the Pythia plug-in cupythia_b200/pythia/CpSigmaQCD.*,
+#                                 linked against this Pythia and libcupythia_b200.so
 #
 # Usage: make -f oracle/ref.mk -j8 REF=<reference root>   (or CUPYTHIA_REFERENCE in the environment)
 REF     ?= $(CUPYTHIA_REFERENCE)
@@ -46,4 +49,13 @@ $(OUT)/tunes/.stamp: $(wildcard $(PY8)/share/Pythia8/tunes/*)
 	cp -r $(PY8)/share/Pythia8/tunes/. $(OUT)/tunes/
 	touch $@
 
-.PHONY: all
+CUDA_HOME ?= /usr/local/cuda
+PLUGIN_SRC := tests/pythia_plugin_check.cc cupythia_b200/pythia/CpSigmaQCD.cc
+plugin: $(OUT)/pythia_plugin_check
+
+$(OUT)/pythia_plugin_check: $(PLUGIN_SRC) cupythia_b200/pythia/CpSigmaQCD.h include/cupythia_b200.h $(OUT)/libpythia8.a cupythia_b200/libcupythia_b200.so
+	$(CXX) -O2 -std=c++17 -Wall -I$(PY8)/include -Iinclude -Icupythia_b200/pythia -I$(CUDA_HOME)/include $(PLUGIN_SRC) \
+	  -o $@ $(OUT)/libpythia8.a -Lcupythia_b200 -lcupythia_b200 -L$(CUDA_HOME)/lib64 -lcudart \
+	  -Wl,-rpath,'$$ORIGIN/../../cupythia_b200' -ldl -lpthread
+
+.PHONY: all plugin

@@ -254,11 +254,19 @@ def test_edge_cases(integ):
     assert np.all(np.isfinite(w.cpu().numpy()))
 
 
+# a draw this close (relative) to a selection boundary can be decided either way by FP32 sums
+PICK_MARGIN = 1e-4
+# picks observed to differ from the FP64 oracle's per process code (3000 seeded points each)
+PICK_DIFFERS = {111: 3, 112: 3, 113: 3, 114: 3, 115: 3}
+
+
 def test_pick_in_state_and_set_id_col_acol_match_oracle():
     import oracle
     """The SigmaProcess surface's pickInState and setIdColAcol over a batch, per process, against
-    the oracle's restatement at the same FP32 kinematics and uniforms (<= 1 in 1000 may differ:
-    FP32 pair sums against FP64 ones at a boundary)."""
+    the oracle's restatement at the same FP32 kinematics and uniforms.  A pick may differ only
+    where a draw lies within FP32 rounding of a selection boundary (the oracle's margin below
+    PICK_MARGIN: FP32 pair sums and PDFs against FP64 ones), and no more picks differ than were
+    observed on the B200 (PICK_DIFFERS, deterministic kernels and draws)."""
     import ctypes as C
 
     import cupythia_b200 as cp
@@ -287,15 +295,20 @@ def test_pick_in_state_and_set_id_col_acol_match_oracle():
             assert np.array_equal(id1.cpu().numpy(), ids[:, 0]) and np.array_equal(id2.cpu().numpy(), ids[:, 1])
             ref = np.zeros(n, cp.EVENT_DTYPE)
             ref_ids = np.zeros((n, 4), int)
+            margin = np.zeros(n)
             for i in range(n):
-                got, rid, rcol = oracle.pick_state(cfg, sp.code(), *[float(v) for v in kin[i]], *[float(v) for v in r[i]])
+                got, rid, rcol, margin[i] = oracle.pick_state(cfg, sp.code(), *[float(v) for v in kin[i]],
+                                                              *[float(v) for v in r[i]], with_margin=True)
                 assert got == sp.code()
                 ref_ids[i] = rid
                 ref["colour"][i] = rcol
             ref["process"] = sp.code()
             rc_, ra_ = cp.colour_tags(ref)
             same = (ids == ref_ids).all(1) & (col == rc_).all(1) & (acol == ra_).all(1)
-            assert (~same).sum() <= n // 1000, (sp.name(), int((~same).sum()))
+            differ = int((~same).sum())
+            print(f"{sp.name()}: {differ} of {n} picks differ, margins {np.sort(margin[~same]).tolist()}")
+            assert np.all(margin[~same] < PICK_MARGIN), (sp.name(), margin[~same])
+            assert differ <= PICK_DIFFERS[sp.code()], (sp.name(), differ)
 
 
 def test_philox_words_match_curand(integ, tmp_path):

@@ -2,7 +2,9 @@
 new flavour and colour flow (pickInState + setIdColAcol restated in cpo_pick_record) at the
 kernel's own points and random numbers, and the LHE file of device records read back by Pythia.
 The kernel evaluates the pair sums in FP32 and the oracle in FP64, so a pick can differ when a
-random number falls within rounding of a boundary: at most 1 in 1000 records may differ."""
+random number falls within rounding of a boundary: every differing record must have a draw within
+RECORD_MARGIN (relative) of a selection boundary by the oracle's own sums, and no more records
+may differ than were observed on the B200 (RECORD_DIFFERS; kernels and draws are deterministic)."""
 import json
 import os
 import subprocess
@@ -15,6 +17,8 @@ import oracle
 pytestmark = pytest.mark.gpu
 
 N = 1 << 20
+RECORD_MARGIN = 1e-4
+RECORD_DIFFERS = 20
 
 
 @pytest.fixture(scope="module")
@@ -42,17 +46,21 @@ def test_record_picks_match_oracle(production):
     w1 = it.philox_words(it.cfg.seed, 0, N, 61, 1)[pts]
     cfg = oracle.had_cfg()
     bad = 0
+    bad_margins = []
     codes = np.zeros(len(sub), int)
     for i in range(len(sub)):
         w = [int(v) for v in w1[i]]
         rc = ((w[0] & 0xFF) | ((w[1] & 0xFF) << 8) | ((w[2] & 0xFF) << 16)) / 16777216.0
         rs = (w[3] & 0xFF) / 256.0
         r = [float(_u24(w1[i, 0])), float(_u24(w1[i, 1])), float(_u24(w1[i, 3])), rc, rs]
-        code, ids, colour = oracle.pick_record(cfg, x[i], *r)
+        code, ids, colour, margin = oracle.pick_record(cfg, x[i], *r, with_margin=True)
         codes[i] = code
         if (code, ids, colour) != (int(sub["process"][i]), sub["id"][i].tolist(), int(sub["colour"][i])):
             bad += 1
-    assert bad <= len(sub) // 1000, bad
+            bad_margins.append(margin)
+    print(f"records: {bad} of {len(sub)} differ from the oracle's picks, margins {sorted(bad_margins)}")
+    assert all(m < RECORD_MARGIN for m in bad_margins), bad_margins
+    assert bad <= RECORD_DIFFERS, bad
     assert set(np.unique(codes)) == {111, 112, 113, 114, 115}
 
 
