@@ -479,12 +479,18 @@ __global__ void k_flow_adam(float* __restrict__ P, float* __restrict__ G, float*
 }
 
 // batch moments of this handle's points from the integrand kernel's block slots, fixed order
+// (one warp: strided lane sums, then the xor tree; the same order on every run)
 __global__ void k_flow_moments(const double* slots, int nblk, double* moments)
 {
+  const int lane = threadIdx.x & 31;
   double a = 0.0, b = 0.0;
-  for (int k = 0; k < nblk; ++k) { a += slots[2 * k]; b += slots[2 * k + 1]; }
-  moments[0] = a;
-  moments[1] = b;
+  for (int k = lane; k < nblk; k += 32) { a += slots[2 * k]; b += slots[2 * k + 1]; }
+  a = cp_warp_sum_d(a);
+  b = cp_warp_sum_d(b);
+  if (lane == 0) {
+    moments[0] = a;
+    moments[1] = b;
+  }
 }
 
 // the batch's moments (summed over ranks) for the backward pass, and its loss <w^2> / <w>^2
@@ -577,7 +583,7 @@ static int flow_phase_moments(cp_handle* h, const FlowTrainBufs& t, uint64_t poi
   const float lnTauMin = (float)log(4.0 * h->cfg.pt_hat_min * h->cfg.pt_hat_min / (h->cfg.sqrt_s * h->cfg.sqrt_s));
   k_flow_igrad<<<gblk, 128, 0, h->stream>>>(h->P, h->d_cteq, count, lnTauMin, t.vj, t.wg, h->d_slots);
   CP_LAUNCH_CHECK(h, "k_flow_igrad");
-  k_flow_moments<<<1, 1, 0, h->stream>>>(h->d_slots, gblk, moments);
+  k_flow_moments<<<1, 32, 0, h->stream>>>(h->d_slots, gblk, moments);
   CP_LAUNCH_CHECK(h, "k_flow_moments");
   return CP_OK;
 }

@@ -114,13 +114,17 @@ class ShardedIntegrator:
         return adapt_gradient_loop(self.gradient_step, steps, n_points, lr, iteration0)
 
     # ---------------------------------------------------------------- flow training
-    def flow_train(self, steps, batch=65536, lr=1e-3):
+    def flow_train(self, steps, batch=65536, lr=1e-3, phases=False):
         """Integrator.flow_train data-parallel: each step's batch [0, batch) is shared out in
         contiguous ranges; two exchanges per step (the batch moments, 2 doubles, then the gradient,
         one float per parameter) and every rank takes the same Adam step.  One rank reproduces
-        Integrator.flow_train bit for bit."""
+        Integrator.flow_train bit for bit, and with one rank the backend's own training loop runs
+        unless phases is set."""
         if batch < self.world:
             raise ValueError("flow_train: fewer batch points than ranks")
+        if self.world == 1 and not phases and hasattr(self.b, "flow_train"):
+            # nothing to exchange: the handle's own loop, with no host round trip per step
+            return self.b.flow_train(steps, batch, lr)
         offset, count = shard(batch, self.rank, self.world)
         losses = np.zeros(steps)
         for s in range(steps):

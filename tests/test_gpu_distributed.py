@@ -97,7 +97,7 @@ def test_data_parallel_training_equals_flow_train():
         for it in (a, b):
             it.flow_init(7)
         la = a.flow_train(6, 65536, lr=8e-3)
-        lb = ShardedIntegrator(b).flow_train(6, 65536, lr=8e-3)
+        lb = ShardedIntegrator(b).flow_train(6, 65536, lr=8e-3, phases=True)
         assert np.array_equal(la, lb)
         assert np.array_equal(a.flow_params, b.flow_params)
         # the next step, whole batch vs two shards
