@@ -18,10 +18,12 @@
 //        coupling's layer-1 input, publish (its layer 1 follows)
 // and the steps of the two slots alternate, so one slot's MMAs run while the other slot's
 // epilogue runs; a slot that finishes its last coupling writes its points and starts on the
-// warpgroup's next pair at once, while the other slot finishes the current one.  The biases are part of the MMAs: layer 1 has them as input columns 14 and 15
-// (constant 1) times weight rows holding the BF16 high and low parts of the FP32 bias; layers 2
-// and 3 add one K = 16 MMA of a constant block (columns 0 and 1 equal to 1) against the hi/lo
-// bias rows.  hi + lo reproduces the FP32 bias to about 2^-17 relative.
+// warpgroup's next pair at once, while the other slot finishes the current one.  The biases of layers 1 and 2 are part of the MMAs: layer 1 has them as input
+// columns 14 and 15 (constant 1) times weight rows holding the BF16 high and low parts of the
+// FP32 bias; layer 2 adds one K = 16 MMA of a constant block (columns 0 and 1 equal to 1) against
+// the hi/lo bias rows (hi + lo reproduces the FP32 bias to about 2^-17 relative).  Layer 3's
+// biases are added in FP32 by the coupling update: its 2 or 4 outputs per point cost as many
+// adds, against one more MMA per tile step.
 //
 // Synchronisation is by mbarriers: each epilogue warp publishes its rows of a step (proxy fence,
 // one arrival per warp on the slot's publish barrier); the issuing warp, seeing four arrivals,
@@ -39,8 +41,7 @@
 #define CP_TC_B2 2048     // [N 64][K 64]: W2
 #define CP_TC_B2B 10240   // [N 64][K 16]: b2 hi/lo in K 0/1
 #define CP_TC_B3 12288    // [N 16][K 64]: W3 (outputs 0..7, rest zero)
-#define CP_TC_B3B 14336   // [N 16][K 16]: b3 hi/lo in K 0/1
-#define CP_TC_PER 14848
+#define CP_TC_PER 14336
 #define CP_TC_IMG (CP_FLOW_NC * CP_TC_PER)
 #define CP_TC_WG 4
 #define CP_TC_THREADS (CP_TC_WG * 128 + CP_TC_WG * 32)   // 4 epilogue warpgroups + 4 issuing warps
@@ -49,7 +50,8 @@
 #define CP_TC_S_H (CP_TC_S_ONES + 4096)
 #define CP_TC_S_EDGE (CP_TC_S_H + CP_TC_WG * 2 * CP_TC_HBYTES)
 #define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
-#define CP_TC_SMEM (CP_TC_S_MISC + 256 + 1024)  // mbarriers, TMEM address, abort flags, final barriers; 1024-byte base alignment slack
+#define CP_TC_S_B3 (CP_TC_S_MISC + 256)         // FP32 layer-3 biases, 8 per coupling
+#define CP_TC_SMEM (CP_TC_S_B3 + 128 + 1024)    // mbarriers, TMEM address, abort flags, final barriers; biases; 1024-byte base alignment slack
 #define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
 #define CP_TC_A3 32                             // slot's TMEM column of the layer-3 A operand
 #define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
@@ -85,7 +87,6 @@ __global__ void k_flow_pack_tc(const float* __restrict__ P, uint8_t* __restrict_
   const float* W2 = P + c * CP_FLOW_PER + CP_FLOW_W2;
   const float* b2 = P + c * CP_FLOW_PER + CP_FLOW_B2;
   const float* W3 = P + c * CP_FLOW_PER + CP_FLOW_W3;
-  const float* b3 = P + c * CP_FLOW_PER + CP_FLOW_B3;
   uint8_t* q = img + c * CP_TC_PER;
   for (int e = threadIdx.x; e < CP_TC_PER / 2; e += blockDim.x) {
     uint16_t v = 0, hi, lo;
@@ -106,17 +107,10 @@ __global__ void k_flow_pack_tc(const float* __restrict__ P, uint8_t* __restrict_
       off = CP_TC_B2B + cp_tc_off(nn, k, 64);
       cp_bf16_split(b2[nn], hi, lo);
       v = k == 0 ? hi : (k == 1 ? lo : (uint16_t)0);
-    } else if (e < 7168) {                // B3 [16][64]
+    } else {                              // B3 [16][64]
       const int i = e - 6144, nn = i >> 6, k = i & 63;
       off = CP_TC_B3 + cp_tc_off(nn, k, 16);
       if (nn < 8) v = cp_bf16_bits(W3[k * 8 + nn]);
-    } else {                              // B3B [16][16]
-      const int i = e - 7168, nn = i >> 4, k = i & 15;
-      off = CP_TC_B3B + cp_tc_off(nn, k, 16);
-      if (nn < 8) {
-        cp_bf16_split(b3[nn], hi, lo);
-        v = k == 0 ? hi : (k == 1 ? lo : (uint16_t)0);
-      }
     }
     *reinterpret_cast<uint16_t*>(q + off) = v;
   }
@@ -180,12 +174,11 @@ __device__ __forceinline__ void cp_tc_issue_l2(uint32_t d, uint64_t a, uint64_t 
 }
 // layer 3 reads its A operand (the layer-2 activations, BF16 pairs) from the slot's TMEM columns
 // 32..63, where the ep2 epilogue stored them, and accumulates into columns 0..15
-__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint64_t ones, uint64_t b16, uint32_t bw)
+__device__ __forceinline__ void cp_tc_issue_l3(uint32_t d, uint64_t b16, uint32_t bw)
 {
 #pragma unroll
   for (int j = 0; j < 4; ++j)
     cp_tc_mma_ts(d, d + CP_TC_A3 + 8 * j, b16 + bw + ((CP_TC_B3 + j * 512) >> 4), CP_TC_IDESC16, j > 0 ? 1u : 0u);
-  cp_tc_mma(d, ones, b16 + bw + (CP_TC_B3B >> 4), CP_TC_IDESC16, 1u);
 }
 
 // makes this warp's shared-memory writes (and its earlier TMEM reads) visible to the tensor core
@@ -255,7 +248,8 @@ __device__ __forceinline__ void cp_tc_hidden_to_tmem(uint32_t taddr, bool ok)
 }
 
 __global__ void __launch_bounds__(CP_TC_THREADS, 1)
-    k_flow_fwd_tc(const uint4* __restrict__ img_g, const double* __restrict__ edges, int nb, uint64_t seed,
+    k_flow_fwd_tc(const uint4* __restrict__ img_g, const float* __restrict__ params, const double* __restrict__ edges,
+                  int nb, uint64_t seed,
                   uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* __restrict__ out,
                   int* __restrict__ status, int stall)
 {
@@ -275,6 +269,8 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   for (int e = tid; e < CP_TC_IMG / 16; e += CP_TC_THREADS) reinterpret_cast<uint4*>(sm)[e] = img_g[e];
   for (int e = tid; e < 256; e += CP_TC_THREADS)
     reinterpret_cast<uint4*>(sm + CP_TC_S_ONES)[e] = e < 128 ? make_uint4(CP_TC_ONE2, 0u, 0u, 0u) : make_uint4(0u, 0u, 0u, 0u);
+  float* sB3 = reinterpret_cast<float*>(sm + CP_TC_S_B3);
+  if (tid < CP_FLOW_NC * 8) sB3[tid] = params[(tid >> 3) * CP_FLOW_PER + CP_FLOW_B3 + (tid & 7)];
   for (int k = tid; k < 3 * nb; k += CP_TC_THREADS) {
     const int d = k / nb, b = k - d * nb;
     const double lo = edges[d * (nb + 1) + b], hi = edges[d * (nb + 1) + b + 1];
@@ -340,7 +336,7 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
             cp_tc_issue_l2(tc, ad, adones, b64, bw);
             lay = 2;
           } else {
-            cp_tc_issue_l3(tc, adones, b16, bw);
+            cp_tc_issue_l3(tc, b16, bw);
             lay = 0;
             bw = bw == (CP_FLOW_NC - 1) * (CP_TC_PER >> 4) ? 0u : bw + (CP_TC_PER >> 4);
           }
@@ -423,10 +419,11 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
           float o[4] = {0.f, 0.f, 0.f, 0.f};
           if (ok) cp_tc_ld4(tc[s] + lane_base, o);
           const CpCoupling k = cp_coupling(c);
+          const float* b3 = sB3 + 8 * c;
 #pragma unroll
           for (int j = 0; j < 2; ++j) {
             if (j >= k.nt) break;
-            const float sc = cp_tc_softclamp(o[j]), sh = o[k.nt + j];
+            const float sc = cp_tc_softclamp(o[j] + b3[j]), sh = o[k.nt + j] + b3[k.nt + j];
             const int d = k.tr[j];
             const float zn = fmaf(cp_sel3(t[s], d), __expf(sc), sh);
             if (d == 0) t[s].z0 = zn;
@@ -489,7 +486,8 @@ int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter,
   const uint64_t want = (pairs + CP_TC_WG - 1) / CP_TC_WG;
   const int grid = (int)(want < (uint64_t)h->num_sms ? want : (uint64_t)h->num_sms);
   if (grid < 1) return CP_OK;
-  k_flow_fwd_tc<<<grid, CP_TC_THREADS, CP_TC_SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_edges,
+  k_flow_fwd_tc<<<grid, CP_TC_THREADS, CP_TC_SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_flow,
+                                                                 h->d_edges,
                                                                  h->nb, h->cfg.seed, point0, n, iter, stream, out,
                                                                  h->d_flow_status, h->flow_stall);
   CP_LAUNCH_CHECK(h, "k_flow_fwd_tc");
@@ -508,7 +506,8 @@ int cp_flow_tc_status(cp_handle* h)
   if (!s) return CP_OK;
   CP_CUDA(h, cudaMemsetAsync(h->d_flow_status, 0, sizeof(int), h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
-  return cp_fail(h, CP_ERR_TIMEOUT, "k_flow_fwd_tc: a tensor-core wait expired (results of this pass are invalid)");
+  return cp_fail(h, CP_ERR_TIMEOUT, (s & 2) ? "k_flow_wgrad_tc: a tensor-core wait expired (this training step's gradient is invalid)"
+                                            : "k_flow_fwd_tc: a tensor-core wait expired (results of this pass are invalid)");
 }
 
 // Test hook of the failure path: with on != 0 the issuing warps issue nothing, so every bounded

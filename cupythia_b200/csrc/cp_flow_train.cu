@@ -13,6 +13,7 @@
 #include "cp_dual.cuh"
 #include "cp_flow.cuh"
 #include "cp_internal.cuh"
+#include "cp_tc.cuh"
 
 int cp_flow_ensure(cp_handle* h);
 int cp_flow_repack(cp_handle* h);
@@ -439,6 +440,217 @@ __global__ void __launch_bounds__(128) k_flow_wgrad(const uint16_t* __restrict__
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// 4'. The same weight and bias gradients on the 5th-generation tensor cores, all couplings and
+//     the three layer shapes in one launch (blockIdx.y = coupling, blockIdx.z = layer).  Every
+//     product has the hidden side (64 wide) as M and the other side as N:
+//       layer 0: dW1^T[n][k] = sum_p D1[p][n] X[p][k]    M = 64 (n), N = 16 (k), bias b1 = sum D1
+//       layer 1: dW2[k][n]   = sum_p H1[p][k] D2[p][n]   M = 64 (k), N = 64 (n), bias b2 = sum D2
+//       layer 2: dW3[k][n]   = sum_p H2[p][k] DO[p][n]   M = 64 (k), N = 16 (n), bias b3 = sum DO
+//     so D[M][N] += A[M][K] B[N][K]^T with K = the block's points, 64 per stage: A and B are the
+//     row-major [point][feature] arrays read as MN-major operands (features contiguous).  Shared
+//     memory holds them in the no-swizzle MN-major canonical layout: core matrices of 8 features
+//     (16 bytes) x 8 points, 128 bytes; element (feature f, point q) of a stage at
+//     (q / 8) * (F / 8) * 128 + (f / 8) * 128 + (q % 8) * 16 + (f % 8) * 2, so the descriptor's
+//     stride in the feature direction (SBO) is 128 bytes and in the point direction (LBO)
+//     (F / 8) * 128.  Stages are copied with cp.async (16-byte chunks, zero fill past the chunk's
+//     end) into two buffers; one thread issues a stage's four K = 16 MMAs and commits them to the
+//     buffer's mbarrier, which every thread waits on (bounded) before the buffer is refilled.  The
+//     M = 64 accumulator occupies TMEM lanes 0-15 of each 32-lane quarter (row r in lane
+//     r % 16 + 32 (r / 16)), so thread t < 16 of warp w reads row 16 w + t.  Each block writes its
+//     own slot of the partial buffer; k_flow_gsum adds the slots in block order.
+// ------------------------------------------------------------------------------------------
+#define CP_WGT_STAGE 64   // points per stage (four K = 16 MMAs)
+
+__device__ __forceinline__ void cp_cp_async16(uint32_t dst, const void* src, bool valid)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// one stage of F-wide rows [q0, q0 + 64) of X (row-major, leading dim F) into the MN-major layout
+template <int F>
+__device__ __forceinline__ void cp_wgt_stage_load(uint32_t sdst, const uint16_t* __restrict__ X, uint64_t q0,
+                                                  uint64_t q_end)
+{
+  constexpr int CH = CP_WGT_STAGE * F / 8;   // 16-byte chunks
+  for (int e = threadIdx.x; e < CH; e += blockDim.x) {
+    // e = (point group, feature group, point within group): consecutive threads fill a core
+    // matrix's consecutive 16-byte rows
+    const int qg = e / (F / 8 * 8), fg = (e / 8) % (F / 8), r = e % 8;
+    const uint64_t q = q0 + qg * 8 + r;
+    const bool ok = q < q_end;
+    cp_cp_async16(sdst + (uint32_t)e * 16u, X + (ok ? q : q0) * F + fg * 8, ok);
+  }
+}
+
+__device__ __forceinline__ float cp_wgt_elem(const uint8_t* s, int F, int f, int q)
+{
+  const uint16_t v = *reinterpret_cast<const uint16_t*>(s + (q / 8) * (F / 8) * 128 + (f / 8) * 128 + (q % 8) * 16 + (f % 8) * 2);
+  return __uint_as_float((uint32_t)v << 16);
+}
+
+template <int NB>
+__device__ __forceinline__ void cp_wgt_layer(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B, bool bias_of_a,
+                                             uint64_t p_begin, uint64_t p_end, float* __restrict__ G, int layer,
+                                             uint8_t* smem, uint32_t tmem, uint32_t mbar0, float* sBias,
+                                             int* __restrict__ status)
+{
+  constexpr int ABYTES = CP_WGT_STAGE * 64 * 2, BBYTES = CP_WGT_STAGE * NB * 2;
+  const uint32_t sbase = cp_smem_u32(smem);
+  const uint32_t sA[2] = {sbase, sbase + ABYTES}, sB[2] = {sbase + 2 * ABYTES, sbase + 2 * ABYTES + BBYTES};
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(NB >> 3) << 17) |
+                         ((uint32_t)(64 >> 4) << 24);
+  const int nst = (int)((p_end - p_begin + CP_WGT_STAGE - 1) / CP_WGT_STAGE);
+  const int tid = threadIdx.x;
+  // bias column of this thread and its share of a stage's points (fixed order)
+  constexpr int BW = 64;   // the bias side is 64 wide for layer 0 (A = D1), NB wide otherwise
+  const int bw = bias_of_a ? BW : NB;
+  const int bcol = tid % bw, bsplit = 128 / bw, brow0 = tid / bw;
+  float bsum = 0.f;
+  uint32_t phase[2] = {0u, 0u};
+  volatile int abort_flag = 0;
+  bool ok = true;
+  cp_wgt_stage_load<64>(sA[0], A, p_begin, p_end);
+  cp_wgt_stage_load<NB>(sB[0], B, p_begin, p_end);
+  cp_cp_async_commit();
+  for (int st = 0; st < nst; ++st) {
+    const int b = st & 1;
+    if (st + 1 < nst) {
+      // the other buffer was read by stage st - 1's MMAs: wait for their commit before refilling
+      if (st >= 1) {
+        ok = ok && cp_mbar_wait_bounded(mbar0 + 8 * (1 - b), phase[1 - b], &abort_flag);
+        phase[1 - b] ^= 1u;
+      }
+      const uint64_t q0 = p_begin + (uint64_t)(st + 1) * CP_WGT_STAGE;
+      cp_wgt_stage_load<64>(sA[1 - b], A, q0, p_end);
+      cp_wgt_stage_load<NB>(sB[1 - b], B, q0, p_end);
+      cp_cp_async_commit();
+      cp_cp_async_wait<1>();
+    } else {
+      cp_cp_async_wait<0>();
+    }
+    cp_fence_proxy_async();
+    __syncthreads();
+    {
+      const uint8_t* sb = smem + (bias_of_a ? (b ? ABYTES : 0) : 2 * ABYTES + (b ? BBYTES : 0));
+      for (int q = brow0; q < CP_WGT_STAGE; q += bsplit) bsum += cp_wgt_elem(sb, bias_of_a ? 64 : NB, bcol, q);
+    }
+    if (tid == 0 && ok) {
+      cp_tc_fence_after();
+#pragma unroll
+      for (int k = 0; k < CP_WGT_STAGE / 16; ++k) {
+        // K = 16 points = two point groups: +2 groups of (F / 8) core matrices
+        const uint64_t da = cp_tc_desc(sA[b] + k * 2 * (64 / 8) * 128, (64 / 8) * 128, 128);
+        const uint64_t db = cp_tc_desc(sB[b] + k * 2 * (NB / 8) * 128, (NB / 8) * 128, 128);
+        cp_tc_mma(tmem, da, db, idesc, (st > 0 || k > 0) ? 1u : 0u);
+      }
+      cp_tc_commit(mbar0 + 8 * b);
+    } else if (tid == 0) {
+      cp_tc_commit(mbar0 + 8 * b);   // nothing issued: the barrier still completes its phase
+    }
+  }
+  // the last stage's MMAs (and, in order, every earlier one) have completed
+  const int bl = (nst - 1) & 1;
+  ok = ok && cp_mbar_wait_bounded(mbar0 + 8 * bl, phase[bl], &abort_flag);
+  if (nst >= 2) ok = ok && cp_mbar_wait_bounded(mbar0 + 8 * (1 - bl), phase[1 - bl], &abort_flag);
+  cp_tc_fence_after();
+  ok = __syncthreads_and(ok) != 0;
+  if (!ok) {
+    // a wait expired: record it, and before TMEM is released let every MMA this thread issued
+    // complete (a fresh barrier, bounded wait)
+    if (tid == 0) {
+      atomicOr(status, 2);
+      cp_tc_commit(mbar0 + 16);
+      volatile int drain_abort = 0;
+      cp_mbar_wait_bounded(mbar0 + 16, 0u, &drain_abort);
+    }
+    __syncthreads();
+    return;
+  }
+  // accumulator: warp w, lane t < 16 = row 16 w + t
+  const int warp = tid >> 5, lane = tid & 31, row = 16 * warp + lane;
+  const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16);
+#pragma unroll
+  for (int half = 0; half < NB / 16; half += 2) {
+    float v[32];
+    if (NB == 64) {
+      cp_tc_ld32(taddr + half * 16, v);
+    } else {
+      float v4[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        cp_tc_ld4(taddr + 4 * j, v4);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[4 * j + i] = v4[i];
+      }
+    }
+    if (lane < 16) {
+      const int ncol = NB == 64 ? 32 : 16;
+#pragma unroll
+      for (int j = 0; j < ncol; ++j) {
+        const int c = half * 16 + j;
+        if (layer == 0) G[CP_FLOW_W1 + c * 64 + row] = v[j];                 // dW1[k = c][n = row]
+        else if (layer == 1) G[CP_FLOW_W2 + row * 64 + c] = v[j];            // dW2[k = row][n = c]
+        else if (c < 8) G[CP_FLOW_W3 + row * 8 + c] = v[j];                  // dW3[k = row][n = c < 8]
+      }
+    }
+  }
+  // bias: the bsplit threads of a column add their sums in thread order
+  sBias[tid] = bsum;
+  __syncthreads();
+  const int nb_valid = layer == 2 ? 8 : 64;
+  if (tid < bw && tid < nb_valid) {
+    float acc = 0.f;
+    for (int r = 0; r < bsplit; ++r) acc += sBias[r * bw + tid];
+    G[(layer == 0 ? CP_FLOW_B1 : (layer == 1 ? CP_FLOW_B2 : CP_FLOW_B3)) + tid] = acc;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_flow_wgrad_tc(FlowTrainBufs t, uint64_t n, int chunk, int* __restrict__ status)
+{
+  // two A and two B stage buffers (32 KB), plus 8 KB so that the operand ranges of every
+  // descriptor stay inside this array whichever of its two strides a layout reading applies
+  __shared__ __align__(1024) uint8_t smem[2 * (CP_WGT_STAGE * 64 * 2) + 2 * (CP_WGT_STAGE * 64 * 2) + 8192];
+  __shared__ float sBias[128];
+  __shared__ __align__(8) uint64_t mbar[3];   // the two stage buffers' MMA commits, the drain
+  __shared__ uint32_t tmem_slot;
+  const int c = blockIdx.y, layer = blockIdx.z, tid = threadIdx.x;
+  if (tid == 0) {
+    for (int i = 0; i < 3; ++i) cp_mbar_init(cp_smem_u32(&mbar[i]), 1);
+    cp_mbar_init_fence();
+  }
+  if ((tid >> 5) == 0) {
+    cp_tc_alloc(cp_smem_u32(&tmem_slot), 64);
+    cp_tc_relinquish();
+  }
+  cp_tc_fence_before();
+  __syncthreads();
+  cp_tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint64_t p_begin = (uint64_t)blockIdx.x * chunk;
+  const uint64_t p_end = p_begin + chunk < n ? p_begin + chunk : n;
+  float* G = t.gpart + (size_t)blockIdx.x * CP_FLOW_NPARAM + c * CP_FLOW_PER;
+  const uint64_t off = (uint64_t)c * n;
+  const uint32_t mb = cp_smem_u32(&mbar[0]);
+  if (p_begin < p_end) {
+    if (layer == 0)
+      cp_wgt_layer<16>(t.D1 + off * 64, t.X + off * 16, true, p_begin, p_end, G, 0, smem, tmem, mb, sBias, status);
+    else if (layer == 1)
+      cp_wgt_layer<64>(t.H1 + off * 64, t.D2 + off * 64, false, p_begin, p_end, G, 1, smem, tmem, mb, sBias, status);
+    else
+      cp_wgt_layer<16>(t.H2 + off * 64, t.DO + off * 16, false, p_begin, p_end, G, 2, smem, tmem, mb, sBias, status);
+  }
+  cp_tc_fence_before();
+  __syncthreads();
+  if ((tid >> 5) == 0) {
+    cp_tc_fence_after();
+    cp_tc_dealloc(tmem, 64);
+  }
+}
+
 // G[i] += sum over the nblk block slots of the partial gradients, in block order
 __global__ void k_flow_gsum(const float* __restrict__ part, int nblk, float* __restrict__ G)
 {
@@ -604,15 +816,23 @@ static int flow_phase_gradient(cp_handle* h, const FlowTrainBufs& t, uint64_t co
   // partial slots 0 .. nblk-1 (all of W1, b1, W2, b2, W3, b3 of every coupling).
   const uint64_t chunk = ((count + CP_WG_MAXBLK - 1) / CP_WG_MAXBLK + CP_WG_ROWS - 1) / CP_WG_ROWS * CP_WG_ROWS;
   const int nblk = (int)((count + chunk - 1) / chunk);
-  const dim3 grid((unsigned)nblk, CP_FLOW_NC);
-  k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, count, t.gpart, CP_FLOW_W1, 64, 64, (int)chunk,
-                                                    CP_FLOW_B1 - CP_FLOW_W1);
-  k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, count, t.gpart, CP_FLOW_W2, 64, 64, (int)chunk,
-                                                    CP_FLOW_B2 - CP_FLOW_W2);
-  // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
-  k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, count, t.gpart, CP_FLOW_W3, 8, 8, (int)chunk,
-                                                    CP_FLOW_B3 - CP_FLOW_W3);
-  CP_LAUNCH_CHECK(h, "k_flow_wgrad");
+  if (h->flow_kernel == 0) {
+    // tensor cores (tcgen05): every coupling and layer shape in one launch
+    k_flow_wgrad_tc<<<dim3((unsigned)nblk, CP_FLOW_NC, 3), 128, 0, h->stream>>>(t, count, (int)chunk,
+                                                                             h->d_flow_status);
+    CP_LAUNCH_CHECK(h, "k_flow_wgrad_tc");
+  } else {
+    // warp-level mma.sync, one launch per layer shape (the cross-check path)
+    const dim3 grid((unsigned)nblk, CP_FLOW_NC);
+    k_flow_wgrad<16, 64><<<grid, 128, 0, h->stream>>>(t.X, t.D1, count, t.gpart, CP_FLOW_W1, 64, 64, (int)chunk,
+                                                      CP_FLOW_B1 - CP_FLOW_W1);
+    k_flow_wgrad<64, 64><<<grid, 128, 0, h->stream>>>(t.H1, t.D2, count, t.gpart, CP_FLOW_W2, 64, 64, (int)chunk,
+                                                      CP_FLOW_B2 - CP_FLOW_W2);
+    // W3 [64][8] from the 16-wide output-gradient rows (columns 8..15 are zero padding)
+    k_flow_wgrad<64, 16><<<grid, 128, 0, h->stream>>>(t.H2, t.DO, count, t.gpart, CP_FLOW_W3, 8, 8, (int)chunk,
+                                                      CP_FLOW_B3 - CP_FLOW_W3);
+    CP_LAUNCH_CHECK(h, "k_flow_wgrad");
+  }
   CP_CUDA(h, cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream));
   k_flow_gsum<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(t.gpart, nblk, G);
   CP_LAUNCH_CHECK(h, "k_flow_gsum");
@@ -634,9 +854,6 @@ static int flow_phase_update(cp_handle* h, double lr)
   return CP_OK;
 }
 
-// Trains the flow for n_steps batches of `batch` points on the current VEGAS grid; loss_host
-// (n_steps doubles, may be NULL) receives <w^2>/<w>^2 of each batch before its update.  Step s
-// draws its batch at counter iteration flow_t (the number of updates so far), points 0..batch-1.
 extern "C" int cp_flow_set_objective(cp_handle* h, double p)
 {
   CP_CHECK_HANDLE(h);
@@ -645,6 +862,9 @@ extern "C" int cp_flow_set_objective(cp_handle* h, double p)
   return CP_OK;
 }
 
+// Trains the flow for n_steps batches of `batch` points on the current VEGAS grid; loss_host
+// (n_steps doubles, may be NULL) receives <w^2>/<w>^2 of each batch before its update.  Step s
+// draws its batch at counter iteration flow_t (the number of updates so far), points 0..batch-1.
 extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double lr, double* loss_host)
 {
   CP_CHECK_HANDLE(h);
@@ -666,6 +886,7 @@ extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double l
   if (!rc && loss_host) e = cudaMemcpyAsync(loss_host, losses, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, h->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   if (!rc && e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_train readback");
+  if (!rc) rc = cp_flow_tc_status(h);
   cudaFree(losses);
   train_buffers_release(h);
   return rc;
@@ -693,6 +914,7 @@ extern "C" int cp_flow_loss_grad(cp_handle* h, uint64_t batch, uint32_t iter, fl
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) rc = cp_fail_cuda(h, e, "cp_flow_loss_grad readback");
   }
+  if (!rc) rc = cp_flow_tc_status(h);
   train_buffers_release(h);
   return rc;
 }
@@ -724,11 +946,8 @@ extern "C" int cp_flow_step_gradient(cp_handle* h, const double* moments_dev, ui
   if (grad_dev)
     CP_CUDA(h, cudaMemcpyAsync(grad_dev, h->d_flow + CP_FLOW_NPARAM, sizeof(float) * CP_FLOW_NPARAM,
                                cudaMemcpyDeviceToDevice, h->stream));
-  if (loss_host) {
-    CP_CUDA(h, cudaMemcpyAsync(loss_host, t.loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    CP_CUDA(h, cudaStreamSynchronize(h->stream));
-  }
-  return CP_OK;
+  if (loss_host) CP_CUDA(h, cudaMemcpyAsync(loss_host, t.loss, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  return cp_flow_tc_status(h);   // synchronises the stream
 }
 
 extern "C" int cp_flow_step_update(cp_handle* h, const float* grad_dev, double lr)

@@ -22,8 +22,11 @@
 //     for the gluon, the constant parts are pre-combined in FP64 on the host:
 //       A = af0 + af1, B = af3 - af0, C = af1 af8, and y^p = 1 + expm1(p ln y), giving
 //       exponent = A + B x + C u + af1 expm1(p ln y) (1 + af8 u) + part3 + part4,
-//     summed in FP32 with the products' FMA residuals and the additions' TwoSum errors
-//     carried in a second float, and exp(hi + lo) = exp(hi) (1 + lo);
+//     summed in FP32 with the products' FMA residuals carried in a second float, and
+//     exp(hi + lo) = exp(hi) (1 + lo).  The additions' own rounding errors (TwoSum) and the
+//     residual of p ln y are not carried: measured on 720k points against the FP64 oracle they
+//     move the largest relative weight error from 5.7e-6 to 6.5e-6, for about 310 fewer FP32
+//     instructions per point;
 //   * matrix elements are written in tHat/sHat and uHat/sHat with all terms of one sign.
 #pragma once
 #include <stdint.h>
@@ -144,16 +147,6 @@ CP_HD CpF2 cp_sub2(CpF2 a, CpF2 b) { return cp_f2(a.x - b.x, a.y - b.y); }
 CP_HD CpF2 cp_mul2(CpF2 a, CpF2 b) { return cp_f2(a.x * b.x, a.y * b.y); }
 CP_HD CpF2 cp_fma2(CpF2 a, CpF2 b, CpF2 c) { return cp_f2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y)); }
 #endif
-// TwoSum in both lanes, and (s, c) += v with the addition's rounding error kept in c
-CP_HD void cp_acc2_2(CpF2& s, CpF2& c, CpF2 v)
-{
-  const CpF2 t = cp_add2(s, v);
-  const CpF2 bp = cp_sub2(t, s);
-  const CpF2 e = cp_add2(cp_sub2(s, cp_sub2(t, bp)), cp_sub2(v, bp));
-  s = t;
-  c = cp_add2(c, e);
-}
-
 // x-dependent quantities of one beam, from ln x = lnx + lnxLo (<= 0, lnxLo a sub-ulp correction)
 struct CpBeamX {
   float x, omx, lny, uh, ul, x1L;
@@ -219,18 +212,16 @@ CP_HD CpCteqQ cp_cteq_coef(const CpCteqPoly& c, float lnQ, float Q, float invQ, 
 // "answer" of xfUpdate (PartonDistributions.cc:1031-1046) for one parametrisation, for both
 // beams at once (lane x: beam A, lane y: beam B): x exp(exponent) (1 - Qmin/Q), with
 //   exponent = A + B x + C u + af1 (y^p - 1) U + part3 + ut1 ln(1-x) + af2 L,  C = af1 af8,
-// summed with the products' FMA residuals and the additions' TwoSum errors kept in a second
-// float, and exp(hi + lo) = exp(hi) (1 + lo).  Every product, residual and TwoSum runs in
-// two-lane arithmetic, the transcendentals per lane.  ux = cp_cteq_uses_x1l(i).
+// summed with the products' FMA residuals kept in a second float, and exp(hi + lo) =
+// exp(hi) (1 + lo).  Every product, residual and sum runs in two-lane arithmetic, the
+// transcendentals per lane.  ux = cp_cteq_uses_x1l(i).
 CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX& bA, const CpBeamX& bB, bool ux)
 {
   const CpF2 lny = cp_f2(bA.lny, bB.lny), x = cp_f2(bA.x, bB.x), omx = cp_f2(bA.omx, bB.omx);
   const CpF2 uh = cp_f2(bA.uh, bB.uh), ul = cp_f2(bA.ul, bB.ul), x1L = cp_f2(bA.x1L, bB.x1L);
   const CpF2 p = cp_f2s(a.p);
   const CpF2 ah = cp_mul2(p, lny);
-  const CpF2 al = cp_fma2(p, lny, cp_f2(-ah.x, -ah.y));
-  CpF2 ym1 = cp_f2(cp_expm1f(ah.x), cp_expm1f(ah.y));
-  ym1 = cp_fma2(cp_add2(cp_f2s(1.f), ym1), al, ym1);
+  const CpF2 ym1 = cp_f2(cp_expm1f(ah.x), cp_expm1f(ah.y));
   const CpF2 U = cp_fma2(cp_f2s(a.af8), uh, cp_f2s(1.f));
   const CpF2 xo = cp_mul2(x, omx);
   const CpF2 part3 = cp_mul2(xo, cp_fma2(cp_f2s(a.af7), xo, cp_fma2(cp_f2s(a.af6), omx, cp_f2s(a.af5))));
@@ -247,14 +238,8 @@ CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX&
   const CpF2 t6 = cp_mul2(u1, x1L), t6l = cp_fma2(u1, x1L, cp_f2(-t6.x, -t6.y));
   const CpF2 a2 = cp_f2s(a.af2);
   const CpF2 t7 = cp_mul2(a2, L), t7l = cp_fma2(a2, L, cp_f2(-t7.x, -t7.y));
-  CpF2 eh = cp_f2s(a.A);
-  CpF2 el = cp_add2(cp_add2(t2l, t3l), cp_add2(cp_add2(t4l, t6l), t7l));
-  cp_acc2_2(eh, el, t3);
-  cp_acc2_2(eh, el, t4);
-  cp_acc2_2(eh, el, t2);
-  cp_acc2_2(eh, el, part3);
-  cp_acc2_2(eh, el, t6);
-  cp_acc2_2(eh, el, t7);
+  const CpF2 el = cp_add2(cp_add2(t2l, t3l), cp_add2(cp_add2(t4l, t6l), t7l));
+  const CpF2 eh = cp_add2(cp_add2(cp_add2(cp_f2s(a.A), t3), cp_add2(t4, t2)), cp_add2(part3, cp_add2(t6, t7)));
   const CpF2 ex = cp_f2(cp_expf(eh.x), cp_expf(eh.y));
   return cp_mul2(cp_mul2(x, cp_fma2(ex, el, ex)), cp_f2s(a.qfac));
 }

@@ -159,6 +159,30 @@ def test_training_gradient_matches_fp64_backprop(integ, orc):
     integ.reset_grid()
 
 
+def test_tcgen05_weight_gradients_match_mma_sync(integ):
+    """The training step's weight and bias gradients from the tcgen05 GEMMs (TMEM accumulators,
+    MN-major shared-memory operands) equal those of the warp-level mma.sync GEMMs on the same
+    activations and output gradients, up to FP32 summation order: the same BF16 products, FP32
+    accumulation, block slots added in the same order."""
+    integ.reset_grid()
+    integ.integrate(4, 1 << 20, alpha=1.5)
+    _random_flow(integ, seed=9, scale=0.05)
+    m = _used_mask()
+    for batch in (65536, 65536 - 96, 4096):
+        integ.flow_kernel("tcgen05")
+        g_tc, l_tc = integ.flow_loss_grad(batch, 17)
+        integ.flow_kernel("mma")
+        g_mma, l_mma = integ.flow_loss_grad(batch, 17)
+        integ.flow_kernel("tcgen05")
+        assert l_tc == l_mma
+        a, b = g_tc[m].astype(np.float64), g_mma[m].astype(np.float64)
+        assert np.all(g_tc[~m] == 0)
+        assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), (batch, np.linalg.norm(a - b) / np.linalg.norm(b))
+        big = np.abs(b) > 1e-3 * np.abs(b).max()
+        assert np.max(np.abs(a[big] - b[big]) / np.abs(b[big])) < 1e-3, batch
+    integ.reset_grid()
+
+
 def test_training_lowers_the_weight_variance():
     import cupythia_b200 as cp
     n = 1 << 22
