@@ -39,7 +39,7 @@ __device__ __forceinline__ float cp_bf_hi(uint32_t v) { return __uint_as_float(v
 // ------------------------------------------------------------------------------------------
 // 1. forward, saving the input z of every coupling
 // ------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(CP_THREADS) k_flow_fwd_train(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g,
+__global__ void __launch_bounds__(CP_THREADS, 2) k_flow_fwd_train(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g,
                                                                const double* __restrict__ edges, int nb,
                                                                uint64_t seed, uint32_t iter, uint32_t stream, uint64_t point0,
                                                                uint64_t n, float* __restrict__ zs, float4* __restrict__ vj)
@@ -159,7 +159,8 @@ __device__ __forceinline__ void cp_store_rowfrag(uint16_t* base, int ld, uint64_
   }
 }
 
-__global__ void __launch_bounds__(128) k_flow_bwd(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g, uint64_t n,
+#define CP_BWD_THREADS 256   // 8 warps; the 92 KB of staged fragments admit two blocks per SM
+__global__ void __launch_bounds__(CP_BWD_THREADS, 2) k_flow_bwd(const uint2* __restrict__ pk_g, const float* __restrict__ bias_g, uint64_t n,
                                                   double n_batch, const float* __restrict__ zs, const float4* __restrict__ vj,
                                                   const float4* __restrict__ wg, const double* __restrict__ sums,
                                                   FlowTrainBufs out, float loss_p)
@@ -807,7 +808,7 @@ static int flow_phase_gradient(cp_handle* h, const FlowTrainBufs& t, uint64_t co
 {
   k_flow_batch_loss<<<1, 1, 0, h->stream>>>(moments, (double)n_batch, t.sums, loss_dev);
   CP_LAUNCH_CHECK(h, "k_flow_batch_loss");
-  k_flow_bwd<<<h->num_sms, 128, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, count, (double)n_batch, t.zs,
+  k_flow_bwd<<<h->num_sms * 2, CP_BWD_THREADS, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, count, (double)n_batch, t.zs,
                                                           t.vj, t.wg, t.sums, t, (float)h->flow_loss_p);
   CP_LAUNCH_CHECK(h, "k_flow_bwd");
   float* G = h->d_flow + CP_FLOW_NPARAM;

@@ -256,8 +256,8 @@ def test_edge_cases(integ):
 
 # a draw this close (relative) to a selection boundary can be decided either way by FP32 sums
 PICK_MARGIN = 1e-4
-# picks observed to differ from the FP64 oracle's per process code (3000 seeded points each)
-PICK_DIFFERS = {111: 3, 112: 3, 113: 3, 114: 3, 115: 3}
+# picks observed to differ from the FP64 oracle's per process code (3000 seeded points each, B200)
+PICK_DIFFERS = {111: 0, 112: 0, 113: 0, 114: 0, 115: 0}
 
 
 def test_pick_in_state_and_set_id_col_acol_match_oracle():

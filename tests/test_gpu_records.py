@@ -18,7 +18,7 @@ pytestmark = pytest.mark.gpu
 
 N = 1 << 20
 RECORD_MARGIN = 1e-4
-RECORD_DIFFERS = 20
+RECORD_DIFFERS = 0        # observed on the B200 for these 20,000 records
 
 
 @pytest.fixture(scope="module")
