@@ -228,6 +228,10 @@ class Integrator:
         batch variance (measured at the pre-step grid of each step) rises. Returns the history."""
         return adapt_gradient_loop(self.gradient_step, steps, n_points, lr, iteration0)
 
+    def gradient_objective(self, p=2.0):
+        """Moment order of the adjoint passes: <w^p>/<w>^p instead of the variance (p = 2)."""
+        self._check(self.lib.cp_vegas_gradient_objective(self.h, float(p)))
+
     def gradient_step(self, n_points, iteration=0, lr=0.5):
         g = cp_grad()
         self._check(self.lib.cp_vegas_gradient_step(self.h, n_points, iteration, lr, C.byref(g)))

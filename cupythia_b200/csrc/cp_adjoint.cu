@@ -11,6 +11,10 @@
 // accumulated per bin (lower- and upper-edge parts, plain and w-weighted) in deterministic
 // warp-private shared-memory histograms, then FP64 block slots, then the fixed-order reduction.
 // sigma = <w>, Var = <w^2> - <w>^2, d sigma = <dw>, d Var = 2 <w dw> - 2 <w> <dw>.
+// With a moment order p != 2 (cp_vegas_gradient_objective) the same pass gives the gradient of
+// the relative p-th moment R_p = <w^p> / <w>^p instead: w^(p-1) takes the place of w in the
+// weighted sums, and the record's var entry becomes (R_p - 1) sigma^2, so var / sigma^2 is
+// R_p - 1 (for p = 2 the relative variance, as before).
 #include <vector>
 #include "cp_dual.cuh"
 #include "cp_internal.cuh"
@@ -30,6 +34,7 @@ struct AdjLaunch {
   double* slots;            // gridDim.x * (CP_ADJ_HEAD + 12 nb)
   float lnTauMin, dlnTauMin_dpt;   // ln tauMin and its pT_hat_min derivative 2 / pTmin
   float lnL2[4], dlnL2_da[4];      // ln Lambda_nf^2 and d/d alpha_s(mZ) = 12 pi / (b0 alpha_s(mZ)^2)
+  float pm1;                       // moment order - 1 (1: the variance)
 };
 
 __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P, const AdjLaunch L)
@@ -73,7 +78,7 @@ __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P,
     const uint64_t p = r * stride + gtid;
     int bin[3] = {0, 0, 0};
     float dlo[3] = {0.f, 0.f, 0.f}, dhi[3] = {0.f, 0.f, 0.f};
-    float w = 0.f;
+    float w = 0.f, wq = 0.f;   // the weight and w^(p-1)
     if (p < L.n) {
       uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, L.stream, wd);
@@ -97,12 +102,13 @@ __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P,
         w = 0.f;
       } else {
         float dth[3] = {wb.d[3] * jv, wb.d[4] * jv, wb.d[5] * jv};
+        wq = L.pm1 == 1.f ? w : powf(w, L.pm1);
         cp_kahan(acc[0], cmp[0], w);
-        cp_kahan(acc[1], cmp[1], w * w);
+        cp_kahan(acc[1], cmp[1], w * wq);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           cp_kahan(acc[2 + k], cmp[2 + k], dth[k]);
-          cp_kahan(acc[5 + k], cmp[5 + k], w * dth[k]);
+          cp_kahan(acc[5 + k], cmp[5 + k], wq * dth[k]);
         }
         wmax = fmaxf(wmax, w);
 #pragma unroll
@@ -119,8 +125,8 @@ __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P,
       float* h = my + d * 4 * nb;
       cp_warp_hist_add(h, bin[d], dlo[d]);
       cp_warp_hist_add(h + nb, bin[d], dhi[d]);
-      cp_warp_hist_add(h + 2 * nb, bin[d], w * dlo[d]);
-      cp_warp_hist_add(h + 3 * nb, bin[d], w * dhi[d]);
+      cp_warp_hist_add(h + 2 * nb, bin[d], wq * dlo[d]);
+      cp_warp_hist_add(h + 3 * nb, bin[d], wq * dhi[d]);
     }
   }
   // block reduction of the head sums, FP64 across warps in fixed order
@@ -149,17 +155,23 @@ __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P,
 // grid: per dimension, G_b = dVar / d ln(Delta_b) of the bin widths (widening bin b shifts every
 // edge above it), ln Delta_b -= lr G_b / max_b |G_b|, renormalised to span [0, 1].  The step is
 // scale-free: the most sensitive bin changes its width by exp(+-lr).  One thread per dimension.
-__global__ void k_adjoint_finish(const double* red, int nb, double n, double* edges, double lr,
+__global__ void k_adjoint_finish(const double* red, int nb, double n, double* edges, double lr, double p,
                                  double* out)   // out: sigma, var, dsig[3], dvar[3], nbad, wmax, dsig_de[3(nb+1)], dvar_de[3(nb+1)]
 {
   const int d = threadIdx.x;
-  const double mean = red[0] / n, var = red[1] / n - mean * mean;
+  const double mean = red[0] / n;
+  // p = 2: Var and its gradient 2 <w dw> - 2 <w> <dw>; otherwise (R_p - 1) sigma^2 and the
+  // gradient of the p-th moment, p <w^(p-1) dw> - p (<w^p> / <w>) <dw>
+  const bool two = p == 2.0;
+  const double mp = red[1] / n;
+  const double var = two ? mp - mean * mean : (mp / pow(mean, p) - 1.0) * mean * mean;
+  const double cw = two ? 2.0 : p, cm = two ? 2.0 * mean : p * mp / mean;
   if (d == 0) {
     out[0] = mean;
     out[1] = var;
     for (int k = 0; k < 3; ++k) {
       out[2 + k] = red[2 + k] / n;
-      out[5 + k] = 2.0 * red[5 + k] / n - 2.0 * mean * red[2 + k] / n;
+      out[5 + k] = cw * red[5 + k] / n - cm * red[2 + k] / n;
     }
     out[8] = red[9];
     out[9] = red[8];
@@ -172,7 +184,7 @@ __global__ void k_adjoint_finish(const double* red, int nb, double n, double* ed
     double a = (k < nb ? h[k] : 0.0) + (k > 0 ? h[nb + k - 1] : 0.0);
     double aw = (k < nb ? h[2 * nb + k] : 0.0) + (k > 0 ? h[3 * nb + k - 1] : 0.0);
     gs[k] = a / n;
-    gv[k] = 2.0 * aw / n - 2.0 * mean * a / n;
+    gv[k] = cw * aw / n - cm * a / n;
   }
   if (!(lr > 0.0) || !(var > 0.0)) return;
   double* e = edges + d * (nb + 1);
@@ -220,6 +232,7 @@ static int adjoint_accumulate(cp_handle* h, uint64_t n, uint32_t iter, uint32_t 
   L.edges = h->d_edges; L.cteq = h->d_cteq; L.slots = h->d_slots;
   const double pt = h->cfg.pt_hat_min, s = h->cfg.sqrt_s * h->cfg.sqrt_s, a = h->cfg.alphas_mz;
   L.lnTauMin = (float)log(4.0 * pt * pt / s);
+  L.pm1 = (float)(h->adj_p - 1.0);
   L.dlnTauMin_dpt = (float)(2.0 / pt);
   const double b0[4] = {27.0, 25.0, 23.0, 21.0};
   for (int k = 0; k < 4; ++k) {
@@ -243,7 +256,7 @@ static int adjoint_finish(cp_handle* h, const double* sums, double n_total, doub
   const size_t out_n = 10 + 6 * (nb + 1);
   double* out = nullptr;
   CP_CUDA(h, cudaMallocAsync(reinterpret_cast<void**>(&out), sizeof(double) * out_n, h->stream));
-  k_adjoint_finish<<<1, 32, 0, h->stream>>>(sums, nb, n_total, h->d_edges, lr, out);
+  k_adjoint_finish<<<1, 32, 0, h->stream>>>(sums, nb, n_total, h->d_edges, lr, h->adj_p, out);
   cudaError_t e = cudaGetLastError();
   std::vector<double> host(out_n, 0.0);
   if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), out, sizeof(double) * out_n, cudaMemcpyDeviceToHost, h->stream);
@@ -275,6 +288,14 @@ static int adjoint_run(cp_handle* h, uint64_t n, uint32_t iter, uint32_t stream,
   if (!rc) rc = adjoint_finish(h, sums, (double)n, lr, g, dsig_de, dvar_de);
   cudaFreeAsync(sums, h->stream);
   return rc;
+}
+
+extern "C" int cp_vegas_gradient_objective(cp_handle* h, double p)
+{
+  CP_CHECK_HANDLE(h);
+  if (!(p >= 2.0 && p <= 8.0)) return cp_fail(h, CP_ERR_INVALID, "cp_vegas_gradient_objective: p must be in [2, 8]");
+  h->adj_p = p;
+  return CP_OK;
 }
 
 extern "C" int cp_adjoint_sums_size(cp_handle* h, int* n_doubles)

@@ -154,6 +154,7 @@ struct cp_handle {
   int flow_on = 0;
   long flow_t = 0;                         // optimiser updates so far (a step's batch iteration)
   double flow_loss_p = 2.0;                // training objective <w^p>/<w>^p
+  double adj_p = 2.0;                      // adjoint / variance-gradient objective: moment order
   // training buffers of the current step (per-point forward state and GEMM operands for
   // ftrain_count points), kept between the phases of a data-parallel step
   void* d_ftrain = nullptr;

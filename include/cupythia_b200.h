@@ -290,6 +290,12 @@ int cp_adjoint(cp_handle* h, uint64_t n_points, uint32_t iter, uint32_t stream, 
  * ln(bin width) -= lr * G / max|G|, G = dVar/dln(width), per dimension (the most sensitive bin
  * changes by exp(+-lr)); the alternative to the classic refinement of cp_vegas_iteration. */
 int cp_vegas_gradient_step(cp_handle* h, uint64_t n_points, uint32_t iter, double lr, cp_grad* out_host);
+/* Moment order p of the adjoint passes (2 <= p <= 8; default 2): cp_adjoint, the gradient steps
+ * and their data-parallel form differentiate the relative p-th moment <w^p>/<w>^p instead of the
+ * variance, and the record's var becomes (<w^p>/<w>^p - 1) sigma^2.  A p above 2 weighs the tail
+ * of the weights, which sets the unweighting efficiency at a high-quantile w_max; classic VEGAS
+ * refinement (a w^2 histogram) has no such choice.  No reference counterpart. */
+int cp_vegas_gradient_objective(cp_handle* h, double p);
 /* The same step data-parallel, with one exchange (the reference shards its passes by point range,
  * cuPythia/common/rng.cuh:5-19, and merges on the host; here the ranks sum device arrays):
  * cp_adjoint_accumulate writes the adjoint sums of this handle's points [offset, offset +

@@ -156,6 +156,40 @@ def test_edge_gradients_match_central_differences(adapted):
         assert abs(g["dvar_dedges"][d][k] - fd_v) < 5e-3 * scale_v, (d, k, g["dvar_dedges"][d][k], fd_v)
 
 
+def test_moment_objective_edge_gradients_match_central_differences(adapted):
+    """With moment order p = 4 the adjoint pass differentiates <w^4>: its edge gradient equals
+    the central difference of sigma^4 d(<w^4> / sigma^4) = d<w^4> - 4 (<w^4> / sigma) d sigma over
+    the same points (common random numbers), FP32-representable grid and power-of-two ulp steps as
+    for the variance."""
+    it = adapted
+    n = 1 << 22
+    grid = it.grid.astype(np.float32).astype(np.float64)
+    it.grid = grid
+    it.gradient_objective(4.0)
+    try:
+        g = it.adjoint(n, iteration=29)
+    finally:
+        it.gradient_objective(2.0)
+    w0 = it.point_weights(0, n, 29).double()
+    s0, m0 = w0.mean().item(), (w0 ** 4).mean().item()
+    assert abs(g["var"] / g["sigma"] ** 2 - (m0 / s0 ** 4 - 1)) < 1e-3 * (m0 / s0 ** 4)
+    for d, k in [(0, 10), (1, 25), (2, 40), (2, 49)]:
+        want = 1e-3 * min(grid[d][k] - grid[d][k - 1], grid[d][k + 1] - grid[d][k])
+        ulp = float(np.spacing(np.float32(grid[d][k])))
+        h = ulp * 2.0 ** max(0, int(np.floor(np.log2(want / ulp))))
+        est = []
+        for sgn in (+1, -1):
+            e = grid.copy()
+            e[d][k] += sgn * h
+            it.grid = e
+            w = it.point_weights(0, n, 29).double()
+            est.append((w.mean().item(), (w ** 4).mean().item()))
+        it.grid = grid
+        fd = ((est[0][1] - est[1][1]) - 4 * m0 / s0 * (est[0][0] - est[1][0])) / (2 * h)
+        scale = np.max(np.abs(g["dvar_dedges"][d]))
+        assert abs(g["dvar_dedges"][d][k] - fd) < 1e-2 * scale, (d, k, g["dvar_dedges"][d][k], fd)
+
+
 def test_variance_gradient_adaptation_vs_classic_vegas():
     import cupythia_b200 as cp
     n = 1 << 20
