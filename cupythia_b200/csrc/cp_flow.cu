@@ -128,11 +128,15 @@ int cp_flow_ensure(cp_handle* h)
   return cp_flow_tc_alloc(h);
 }
 
+// The warp-level fragments (used by training and the mma.sync forward) are repacked at once; the
+// tcgen05 forward's shared-memory image only when a sampling pass next needs it, so a training
+// run does not repack it after every update.
 int cp_flow_repack(cp_handle* h)
 {
   k_flow_pack<<<CP_FLOW_NC, 256, 0, h->stream>>>(h->d_flow, h->d_flow_pk, h->d_flow_bias);
   CP_LAUNCH_CHECK(h, "k_flow_pack");
-  return cp_flow_tc_repack(h);
+  h->flow_tc_stale = 1;
+  return CP_OK;
 }
 
 int cp_flow_buffer(cp_handle* h, uint64_t n)

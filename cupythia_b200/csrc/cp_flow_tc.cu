@@ -482,6 +482,11 @@ int cp_flow_tc_alloc(cp_handle* h)
 
 int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out)
 {
+  if (h->flow_tc_stale) {
+    const int rc = cp_flow_tc_repack(h);
+    if (rc) return rc;
+    h->flow_tc_stale = 0;
+  }
   const uint64_t pairs = (n + 255) / 256;
   const uint64_t want = (pairs + CP_TC_WG - 1) / CP_TC_WG;
   const int grid = (int)(want < (uint64_t)h->num_sms ? want : (uint64_t)h->num_sms);
