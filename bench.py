@@ -182,8 +182,8 @@ EXEC_FLOP_PER_POINT = 3278.0
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
 # launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points
-TRAFFIC_PER_POINT = {"k_unw_accept": (276745216 + 575733760) / 2 ** 24,
-                     "k_flow_fwd_tc": (108544 + 209209344) / 2 ** 24}
+TRAFFIC_PER_POINT = {"k_unw_accept": (276613120 + 655162880) / 2 ** 24,
+                     "k_flow_fwd_tc": (366592 + 209136896) / 2 ** 24}
 
 
 def production(it, n, records, k0, warmup, steps, pg, dev, stream, clocks=None):
