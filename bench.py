@@ -377,35 +377,60 @@ def run_ours(a):
     fp32_peak, mufu_peak = it.measure_peaks()
     acc_ms, acc_n = kt_f["accept"]
     flow_ms, flow_n = kt_f["flow_forward"]
-    pts_per_s = n / (acc_ms / acc_n / 1e3)
+    # the flow form's production kernel: the fused tcgen05 kernel (flow forward, integrand and
+    # accept step in one launch per chunk) unless the forward ran as its own launch
+    fused = use_flow and flow_n == 0
+    bf16_peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
     # the integrand's bound (SIMT FP32 and MUFU co-limited): algorithmic FP32 operations per second
     # against the FP32 issue peak (one operation per lane and cycle = half the FMA-chain TFLOP/s,
     # which counts an FMA as two), and MUFU operations against the measured MUFU peak; the larger
     # fraction is the roofline
     fp32_op_peak = fp32_peak / 2.0
-    ops_acc = ALG_FP32_OPS_PER_POINT * pts_per_s / 1e12
-    mufu_acc = ALG_MUFU_OPS_PER_POINT * pts_per_s / 1e12
-    roof_flow = FLOW_FLOP_PER_POINT * n / (flow_ms / flow_n / 1e3) / 1e12
-    bf16_peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
-    r_acc = {"bound": "fp32", "kernel": "k_unw_accept", "achieved": ops_acc, "peak": fp32_op_peak,
-             "unit": "TFLOP/s", "frac": max(ops_acc / fp32_op_peak, mufu_acc / mufu_peak),
+
+    chunks = (n + UNW_CHUNK - 1) // UNW_CHUNK    # launches of the accept kernel per pass
+
+    def integrand_roof(kernel, ms, launches, with_flow):
+        pts_per_s = n / (ms / max(1, launches) / 1e3)
+        ops = ALG_FP32_OPS_PER_POINT * pts_per_s / 1e12
+        mufu = ALG_MUFU_OPS_PER_POINT * pts_per_s / 1e12
+        traffic = TRAFFIC_PER_POINT.get(kernel)
+        r = {"bound": "fp32", "kernel": kernel, "achieved": ops, "peak": fp32_op_peak,
+             "unit": "TFLOP/s", "frac": max(ops / fp32_op_peak, mufu / mufu_peak),
              "basis": "algorithmic FP32 operations per point (add + mul + div = %d, oracle/cp_opcount.cc) "
                       "per second against the FP32 issue peak (one op per lane-cycle); frac = max of that "
                       "and the MUFU fraction" % ALG_FP32_OPS_PER_POINT,
              "peak_source": "measured: FMA-chain microbenchmark on this GPU (cp_measure_peaks), "
                             "%.1f TFLOP/s at 2 per FMA" % fp32_peak,
-             "fp32_frac": ops_acc / fp32_op_peak, "mufu_frac": mufu_acc / mufu_peak,
-             "mufu_achieved_tops": mufu_acc, "mufu_ops_per_point": ALG_MUFU_OPS_PER_POINT,
-             "executed_flop_per_point": EXEC_FLOP_PER_POINT,
-             "executed_frac": EXEC_FLOP_PER_POINT * pts_per_s / 1e12 / fp32_peak,
-             "flop_per_point": ALG_FP32_OPS_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_unw_accept"] * n,
-             "ms_per_launch": acc_ms / acc_n}
-    r_flow = {"bound": "tensor", "kernel": "k_flow_fwd_tc", "achieved": roof_flow, "peak": bf16_peak,
-              "unit": "TFLOP/s", "frac": roof_flow / bf16_peak,
-              "peak_source": "bf16 sustained, %s" % src,
-              "flop_per_point": FLOW_FLOP_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_flow_fwd_tc"] * n,
-              "ms_per_launch": flow_ms / flow_n}
-    roof, roof2 = (r_acc, r_flow) if acc_ms >= flow_ms else (r_flow, r_acc)
+             "fp32_frac": ops / fp32_op_peak, "mufu_frac": mufu / mufu_peak,
+             "mufu_achieved_tops": mufu, "mufu_ops_per_point": ALG_MUFU_OPS_PER_POINT,
+             "flop_per_point": ALG_FP32_OPS_PER_POINT, "traffic": traffic * n / chunks if traffic else None,
+             "ms_per_launch": ms / max(1, launches) / chunks, "points_per_launch": n / chunks}
+        if not with_flow:
+            # executed FP32 FLOPs of k_unw_accept from its SASS counters
+            r.update({"executed_flop_per_point": EXEC_FLOP_PER_POINT,
+                      "executed_frac": EXEC_FLOP_PER_POINT * pts_per_s / 1e12 / fp32_peak})
+        if with_flow:
+            # the same launch also runs the flow's dense layers on the tensor cores
+            tens = FLOW_FLOP_PER_POINT * pts_per_s / 1e12
+            r.update({"basis": r["basis"] + "; and the flow's BF16 MMA FLOPs (%d per point) against the "
+                      "sustained bf16 peak (%s), the largest of the three fractions" % (FLOW_FLOP_PER_POINT, src),
+                      "tensor_achieved_tflops": tens, "tensor_frac": tens / bf16_peak,
+                      "frac": max(r["frac"], tens / bf16_peak)})
+        return r
+
+    if fused:
+        roof = integrand_roof("k_flow_accept_tc", acc_ms, acc_n, True)
+        # the integrand alone: the plain VEGAS form's accept kernel
+        roof2 = integrand_roof("k_unw_accept", kt_p["accept"][0], kt_p["accept"][1], False)
+    else:
+        r_acc = integrand_roof("k_unw_accept", acc_ms, acc_n, False)
+        roof_flow = FLOW_FLOP_PER_POINT * n / (flow_ms / max(1, flow_n) / 1e3) / 1e12
+        r_flow = {"bound": "tensor", "kernel": "k_flow_fwd_tc", "achieved": roof_flow, "peak": bf16_peak,
+                  "unit": "TFLOP/s", "frac": roof_flow / bf16_peak,
+                  "peak_source": "bf16 sustained, %s" % src,
+                  "flop_per_point": FLOW_FLOP_PER_POINT, "traffic": TRAFFIC_PER_POINT["k_flow_fwd_tc"] * n,
+                  "ms_per_launch": flow_ms / max(1, flow_n), "points_per_launch": n}
+        roof, roof2 = (r_acc, r_flow) if acc_ms >= flow_ms else (r_flow, r_acc)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -449,9 +474,9 @@ def run_ours(a):
                 "d2h_bytes_per_step": int(d2h / e2e_steps),
                 "d2h_copy_gbs": d2h_gbs, "events_per_s_at_copy_rate": d2h_gbs * 1e9 / RECORD_BYTES,
                 "d2h_seconds_per_step": d2h / e2e_steps / (d2h_gbs * 1e9)},
-        # per step: the flow forward once, then per 2^24-point chunk the accept kernel, the slot
-        # reduction, the output-offset scan and the record builder
-        "gpu_launches": a.steps * ((1 if use_flow else 0) + 4 * ((n + UNW_CHUNK - 1) // UNW_CHUNK)),
+        # per step and 2^24-point chunk: the accept kernel (fused: flow forward + accept), the slot
+        # reduction, the output-offset scan and the record builder; unfused, the flow forward once
+        "gpu_launches": a.steps * ((1 if use_flow and not fused else 0) + 4 * ((n + UNW_CHUNK - 1) // UNW_CHUNK)),
         "roofline": roof, "roofline_secondary": roof2,
         "mufu_peak_tops": mufu_peak,
         "clocks": clk.summary(),

@@ -296,6 +296,12 @@ class Integrator:
         """Forward kernel: "tcgen05" (TMEM accumulators, default) or "mma" (warp-level mma.sync)."""
         self._check(self.lib.cp_flow_select_kernel(self.h, {"tcgen05": 0, "mma": 1}[which]))
 
+    def flow_fuse_production(self, on=True):
+        """Production passes in the flow form: flow forward, integrand and accept step in one
+        tcgen05 kernel (on), or the forward over the pass followed by the accept kernel (off, the
+        default and the faster of the two)."""
+        self._check(self.lib.cp_flow_fuse_production(self.h, 1 if on else 0))
+
     def flow_objective(self, p=2.0):
         """Training objective <w^p>/<w>^p (p = 2: the weight variance)."""
         self._check(self.lib.cp_flow_set_objective(self.h, float(p)))

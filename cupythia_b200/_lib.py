@@ -146,6 +146,7 @@ SIGNATURES = {
     "cp_flow_sample": [_P, _u64, _u64, _u32, _u32, _P],
     "cp_flow_enable": [_P, _i],
     "cp_flow_select_kernel": [_P, _i],
+    "cp_flow_fuse_production": [_P, _i],
     "cp_flow_test_stall": [_P, _i],
     "cp_colour_tags": [C.c_uint16, C.c_uint16, _P, _P],
     "cp_set_id_col_acol": [_i, _i, _i, _d, _d, _i, _d, _d, _d, _P, _P, _P],

@@ -269,6 +269,13 @@ extern "C" int cp_flow_select_kernel(cp_handle* h, int which)
   return CP_OK;
 }
 
+extern "C" int cp_flow_fuse_production(cp_handle* h, int on)
+{
+  CP_CHECK_HANDLE(h);
+  h->flow_fuse = on ? 1 : 0;
+  return CP_OK;
+}
+
 extern "C" int cp_flow_enable(cp_handle* h, int on)
 {
   CP_CHECK_HANDLE(h);

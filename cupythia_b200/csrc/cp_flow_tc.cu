@@ -5,6 +5,14 @@
 // FP32 accumulator in TMEM, A (activations) in shared memory for layers 1 and 2 and in TMEM for
 // layer 3 (stored over the spent layer-2 accumulator).
 //
+// A production form (k_flow_accept_tc, opt-in through cp_flow_fuse_production) instantiates the
+// same body and takes each finished tile on, from registers, through the integrand and the
+// accept step of the production pass (the code of k_unw_accept, shared through cp_unweight.cuh),
+// so no flow output is stored.  Its records equal the two-kernel path's byte for byte, but it is
+// the slower of the two: a warpgroup's slots idle while its warps run the integrand, and the
+// integrand's FMA-bound warps lengthen every flow step (2^27 points on B200: 24.6 ms with 4
+// warpgroups at 96 registers, 25.3 ms with 3 at 128, against 10.4 + 11.1 ms for the two kernels).
+//
 // Launch: one persistent CTA per SM (the shared-memory footprint admits one): 4 epilogue
 // warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two
 // 128-point tiles in flight ("slots") with 64 TMEM columns and a 16 KB activation buffer each;
@@ -35,6 +43,7 @@
 #include "cp_flow.cuh"
 #include "cp_internal.cuh"
 #include "cp_tc.cuh"
+#include "cp_unweight.cuh"
 
 // weight image of one coupling, bytes (K-major, no swizzle; see cp_tc.cuh)
 #define CP_TC_B1 0        // [N 64][K 16]: W1 rows 0..n_in-1, bias hi/lo in K 14/15
@@ -43,22 +52,32 @@
 #define CP_TC_B3 12288    // [N 16][K 64]: W3 (outputs 0..7, rest zero)
 #define CP_TC_PER 14336
 #define CP_TC_IMG (CP_FLOW_NC * CP_TC_PER)
-#define CP_TC_WG 4
-#define CP_TC_THREADS (CP_TC_WG * 128 + CP_TC_WG * 32)   // 4 epilogue warpgroups + 4 issuing warps
 #define CP_TC_HBYTES 16384                      // activation buffer of one slot: [128][64] bf16
-#define CP_TC_S_ONES CP_TC_IMG                  // [128][16] bf16 constant block
-#define CP_TC_S_H (CP_TC_S_ONES + 4096)
-#define CP_TC_S_EDGE (CP_TC_S_H + CP_TC_WG * 2 * CP_TC_HBYTES)
-#define CP_TC_S_MISC (CP_TC_S_EDGE + 3 * CP_MAX_BINS * 8)
-#define CP_TC_S_B3 (CP_TC_S_MISC + 256)         // FP32 layer-3 biases, 8 per coupling
-#define CP_TC_SMEM (CP_TC_S_B3 + 128 + 1024)    // mbarriers, TMEM address, abort flags, final barriers; biases; 1024-byte base alignment slack
-#define CP_TC_TMEM_COLS 512                     // 8 slots x 64 columns
+#define CP_TC_TMEM_COLS 512                     // up to 8 slots x 64 columns
 #define CP_TC_A3 32                             // slot's TMEM column of the layer-3 A operand
 #define CP_TC_ONE2 0x3F803F80u                  // two BF16 ones
+#define CP_TC_WG 4                              // sampling form: epilogue warpgroups per CTA
+#define CP_TC_WG_ACC 4                          // production form: 20 warps, 5 per SM sub-partition -> 96 registers
 
-static_assert(CP_TC_S_H % 1024 == 0, "activation buffers must stay aligned");
-static_assert(CP_TC_PER % 16 == 0 && CP_TC_SMEM < (1 << 18), "descriptor offsets are added to the 14-bit address field");
-static_assert(CP_TC_SMEM <= 227 * 1024, "shared memory budget");
+// Shared-memory layout of a CTA with NWG epilogue warpgroups, bytes from the 1024-aligned base.
+template <int NWG>
+struct CpTcLayout {
+  static constexpr int THREADS = NWG * 128 + NWG * 32;     // epilogue warpgroups + one issuing warp each
+  static constexpr int ONES = CP_TC_IMG;                   // [128][16] bf16 constant block
+  static constexpr int H = ONES + 4096;                    // activation buffers, two per warpgroup
+  static constexpr int EDGE = H + NWG * 2 * CP_TC_HBYTES;
+  static constexpr int MISC = EDGE + 3 * CP_MAX_BINS * 8;  // mbarriers, TMEM address, abort flags, final barriers
+  static constexpr int B3 = MISC + 256;                    // FP32 layer-3 biases, 8 per coupling
+  static constexpr int CTEQ = B3 + 128;                    // production form: CTEQ5L coefficient records
+  static constexpr int RED = CTEQ + 8 * (int)sizeof(CpCteqPoly);   // production form: per-warp sums
+  static constexpr int SMEM = RED + NWG * 4 * 7 * 8 + 1024;        // + 1024-byte base alignment slack
+  static_assert(H % 1024 == 0 && CTEQ % 16 == 0, "activation buffers and records must stay aligned");
+  static_assert(SMEM < (1 << 18), "descriptor offsets are added to the 14-bit address field");
+  static_assert(SMEM <= 227 * 1024, "shared memory budget");
+  static_assert(NWG <= 4 && 2 * NWG * 64 <= CP_TC_TMEM_COLS, "barrier area and TMEM columns");
+};
+
+static_assert(CP_TC_PER % 16 == 0, "coupling images are whole descriptor units");
 
 constexpr uint32_t CP_TC_IDESC64 = cp_tc_idesc_bf16(64);
 constexpr uint32_t CP_TC_IDESC16 = cp_tc_idesc_bf16(16);
@@ -247,42 +266,55 @@ __device__ __forceinline__ void cp_tc_hidden_to_tmem(uint32_t taddr, bool ok)
   cp_tc_wait_st();
 }
 
-__global__ void __launch_bounds__(CP_TC_THREADS, 1)
-    k_flow_fwd_tc(const uint4* __restrict__ img_g, const float* __restrict__ params, const double* __restrict__ edges,
-                  int nb, uint64_t seed,
-                  uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* __restrict__ out,
-                  int* __restrict__ status, int stall)
+// The kernel body.  Sampling form (ACCEPT false): each point's (v, ln J) goes to out.  Production
+// form (ACCEPT true, draws of stream 0): each point goes straight on, from registers, through the
+// integrand and the accept step of the production pass (cp_unw_point, the code of k_unw_accept),
+// after both slots of its pair have started their next pair, and each CTA leaves its sums in its
+// slot of L->slots; the record builder then runs unchanged.
+template <int NWG, bool ACCEPT>
+__device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g, const float* __restrict__ params,
+                                                const double* __restrict__ edges, int nb, uint64_t seed, uint64_t point0,
+                                                uint64_t n, uint32_t iter, uint32_t stream, float4* __restrict__ out,
+                                                int* __restrict__ status, int stall, const CpHadParams* P,
+                                                const UnwLaunch* L)
 {
+  using Lay = CpTcLayout<NWG>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   const uint32_t raw = cp_smem_u32(smem_raw);
   const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
   uint8_t* sm = smem_raw + pad;
   const uint32_t sbase = raw + pad;
-  float2* sEdge = reinterpret_cast<float2*>(sm + CP_TC_S_EDGE);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC);   // [0, 8) MMA done, [8, 16) publish
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + CP_TC_S_MISC + 128);
-  int* abort_flags = reinterpret_cast<int*>(sm + CP_TC_S_MISC + 144);
-  uint64_t* fin_bar = reinterpret_cast<uint64_t*>(sm + CP_TC_S_MISC + 160);   // [4] issuers' final commits
+  float2* sEdge = reinterpret_cast<float2*>(sm + Lay::EDGE);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + Lay::MISC);   // [0, 2 NWG) MMA done, [2 NWG, 4 NWG) publish
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + Lay::MISC + 128);
+  int* abort_flags = reinterpret_cast<int*>(sm + Lay::MISC + 144);
+  uint64_t* fin_bar = reinterpret_cast<uint64_t*>(sm + Lay::MISC + 160);   // [NWG] issuers' final commits
 
   const int tid = threadIdx.x, warp = tid >> 5, wg = warp >> 2, row = tid & 127;
 
-  for (int e = tid; e < CP_TC_IMG / 16; e += CP_TC_THREADS) reinterpret_cast<uint4*>(sm)[e] = img_g[e];
-  for (int e = tid; e < 256; e += CP_TC_THREADS)
-    reinterpret_cast<uint4*>(sm + CP_TC_S_ONES)[e] = e < 128 ? make_uint4(CP_TC_ONE2, 0u, 0u, 0u) : make_uint4(0u, 0u, 0u, 0u);
-  float* sB3 = reinterpret_cast<float*>(sm + CP_TC_S_B3);
+  for (int e = tid; e < CP_TC_IMG / 16; e += Lay::THREADS) reinterpret_cast<uint4*>(sm)[e] = img_g[e];
+  for (int e = tid; e < 256; e += Lay::THREADS)
+    reinterpret_cast<uint4*>(sm + Lay::ONES)[e] = e < 128 ? make_uint4(CP_TC_ONE2, 0u, 0u, 0u) : make_uint4(0u, 0u, 0u, 0u);
+  float* sB3 = reinterpret_cast<float*>(sm + Lay::B3);
   if (tid < CP_FLOW_NC * 8) sB3[tid] = params[(tid >> 3) * CP_FLOW_PER + CP_FLOW_B3 + (tid & 7)];
-  for (int k = tid; k < 3 * nb; k += CP_TC_THREADS) {
+  for (int k = tid; k < 3 * nb; k += Lay::THREADS) {
     const int d = k / nb, b = k - d * nb;
     const double lo = edges[d * (nb + 1) + b], hi = edges[d * (nb + 1) + b + 1];
     sEdge[d * CP_MAX_BINS + b] = make_float2((float)lo, (float)(hi - lo));
   }
-  if (tid < CP_TC_WG) abort_flags[tid] = 0;
+  CpCteqPoly* sCteq = reinterpret_cast<CpCteqPoly*>(sm + Lay::CTEQ);
+  double* sRed = reinterpret_cast<double*>(sm + Lay::RED);   // [4 NWG warps][7]
+  if constexpr (ACCEPT) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(L->cteq);
+    for (int e = tid; e < (int)(8 * sizeof(CpCteqPoly) / 4); e += Lay::THREADS) reinterpret_cast<uint32_t*>(sCteq)[e] = src[e];
+  }
+  if (tid < NWG) abort_flags[tid] = 0;
   if (tid == 0) {
-    for (int i = 0; i < 2 * CP_TC_WG; ++i) {
+    for (int i = 0; i < 2 * NWG; ++i) {
       cp_mbar_init(cp_smem_u32(&mbar[i]), 1);
-      cp_mbar_init(cp_smem_u32(&mbar[2 * CP_TC_WG + i]), 4);
+      cp_mbar_init(cp_smem_u32(&mbar[2 * NWG + i]), 4);
     }
-    for (int i = 0; i < CP_TC_WG; ++i) cp_mbar_init(cp_smem_u32(&fin_bar[i]), 1);
+    for (int i = 0; i < NWG; ++i) cp_mbar_init(cp_smem_u32(&fin_bar[i]), 1);
     cp_mbar_init_fence();
   }
   if (warp == 0) {
@@ -294,20 +326,20 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
   __syncthreads();
   cp_tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t ones = sbase + CP_TC_S_ONES;
+  const uint32_t ones = sbase + Lay::ONES;
   const uint64_t npairs = (n + 255) / 256;
-  const uint64_t stride = (uint64_t)gridDim.x * CP_TC_WG;
+  const uint64_t stride = (uint64_t)gridDim.x * NWG;
 
-  if (warp >= 4 * CP_TC_WG) {
+  if (warp >= 4 * NWG) {
     // ---- issuing warps: warp 16 + g serves warpgroup g; one lane scans its two publish barriers
-    const int g = warp - 4 * CP_TC_WG;
+    const int g = warp - 4 * NWG;
     if ((tid & 31) == 0 && !stall) {     // stall: test hook, no MMA is ever issued
-      const uint64_t q0 = (uint64_t)blockIdx.x * CP_TC_WG + g;
+      const uint64_t q0 = (uint64_t)blockIdx.x * NWG + g;
       const uint64_t cnt = q0 < npairs ? (npairs - q0 + stride - 1) / stride : 0;
       uint32_t rem0 = (uint32_t)(3 * CP_FLOW_NC * cnt), rem1 = rem0, pph0 = 0, pph1 = 0;
       uint32_t lay0 = 0, lay1 = 0, bw0 = 0, bw1 = 0;   // layer and coupling image offset >> 4 per slot
-      const uint32_t pub0 = cp_smem_u32(&mbar[2 * CP_TC_WG + 2 * g]), pub1 = pub0 + 8;
-      const uint32_t hb0 = sbase + CP_TC_S_H + (2 * g) * CP_TC_HBYTES, hb1 = hb0 + CP_TC_HBYTES;
+      const uint32_t pub0 = cp_smem_u32(&mbar[2 * NWG + 2 * g]), pub1 = pub0 + 8;
+      const uint32_t hb0 = sbase + Lay::H + (2 * g) * CP_TC_HBYTES, hb1 = hb0 + CP_TC_HBYTES;
       const uint32_t tc0 = tmem + (uint32_t)(2 * g * 64), tc1 = tc0 + 64;
       const uint32_t done0 = cp_smem_u32(&mbar[2 * g]), done1 = done0 + 8;
       volatile int* abort = abort_flags + g;
@@ -367,18 +399,27 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
     uint32_t hb[2], tc[2], mb[2], pb[2], ph[2] = {0u, 0u};
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-      hb[s] = sbase + CP_TC_S_H + (wg * 2 + s) * CP_TC_HBYTES;
+      hb[s] = sbase + Lay::H + (wg * 2 + s) * CP_TC_HBYTES;
       tc[s] = tmem + (uint32_t)((wg * 2 + s) * 64);
       mb[s] = cp_smem_u32(&mbar[wg * 2 + s]);
-      pb[s] = cp_smem_u32(&mbar[2 * CP_TC_WG + wg * 2 + s]);
+      pb[s] = cp_smem_u32(&mbar[2 * NWG + wg * 2 + s]);
     }
     CpTcPoint t[2];
     uint64_t p[2];
+    // production form: the slots' accept draws; each slot's finished points (v, ln J), indices and
+    // draws, held until both slots have started their next pair; the thread's sums
+    [[maybe_unused]] float u[2];
+    [[maybe_unused]] float4 fin0, fin1;
+    [[maybe_unused]] uint64_t fp0 = 0, fp1 = 0;
+    [[maybe_unused]] float fu0 = 0.f, fu1 = 0.f;
+    [[maybe_unused]] CpUnwSums S;
+    [[maybe_unused]] const float wmax = ACCEPT ? (float)L->wmax[0] : 0.f;
     // a slot's start on the pair qq: Philox words -> VEGAS map -> logit, layer-1 input, publish
     auto start = [&](int s, uint64_t qq) {
       p[s] = qq * 256 + s * 128 + row;
       uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
       if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
+      if constexpr (ACCEPT) u[s] = cp_u24(w[3]);
       float jv = 1.f, ld = 0.f, z[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -391,7 +432,7 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
       cp_tc_write_in(hb[s], row, 0, t[s]);
       cp_tc_publish(pb[s]);
     };
-    uint64_t q = (uint64_t)blockIdx.x * CP_TC_WG + wg;
+    uint64_t q = (uint64_t)blockIdx.x * NWG + wg;
     if (q < npairs) {
       start(0, q);
       start(1, q);
@@ -442,14 +483,37 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
             ld += cp_tc_sigmoid(t[s].z0, v0);
             ld += cp_tc_sigmoid(t[s].z1, v1);
             ld += cp_tc_sigmoid(t[s].z2, v2);
-            if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+            if constexpr (ACCEPT) {
+              if (s == 0) {
+                fin0 = make_float4(v0, v1, v2, ld); fp0 = p[s]; fu0 = u[s];
+              } else {
+                fin1 = make_float4(v0, v1, v2, ld); fp1 = p[s]; fu1 = u[s];
+              }
+            } else {
+              if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+            }
             if (qn < npairs) start(s, qn);
           }
+        }
+      }
+      if constexpr (ACCEPT) {
+        // weight, accept test and staging of the pair's two tiles while both slots' next layer-1
+        // MMAs run; a loop over the slots keeps one copy of the integrand's code
+#pragma unroll 1
+        for (int s = 0; s < 2; ++s) {
+          const float4 f = s ? fin1 : fin0;
+          cp_unw_point(*P, sCteq, *L, wmax, s ? fp1 : fp0, f.x, f.y, f.z, expf(f.w), s ? fu1 : fu0, S);
         }
       }
       if (cp_bar_wg_or(bar_id, *abort != 0)) break;
     }
     if (row == 0 && *abort) atomicOr(status, 1);
+    if constexpr (ACCEPT) {
+      double v[7];
+      cp_unw_warp_sums(S, v);
+      if ((tid & 31) == 0)
+        for (int k = 0; k < 7; ++k) sRed[warp * 7 + k] = v[k];
+    }
   }
   cp_tc_fence_before();
   __syncthreads();
@@ -457,6 +521,37 @@ __global__ void __launch_bounds__(CP_TC_THREADS, 1)
     cp_tc_fence_after();
     cp_tc_dealloc(tmem, CP_TC_TMEM_COLS);
   }
+  if constexpr (ACCEPT) {
+    if (tid == 0) {   // the CTA's sums, warps in a fixed order
+      double* slot = L->slots + (size_t)blockIdx.x * CP_UNW_SLOT;
+      for (int k = 0; k < 7; ++k) {
+        double acc = 0.0;
+        for (int q = 0; q < 4 * NWG; ++q) acc = (k == 2) ? fmax(acc, sRed[q * 7 + k]) : acc + sRed[q * 7 + k];
+        slot[k] = acc;
+      }
+      slot[7] = 0.0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(CpTcLayout<CP_TC_WG>::THREADS, 1)
+    k_flow_fwd_tc(const uint4* __restrict__ img_g, const float* __restrict__ params, const double* __restrict__ edges,
+                  int nb, uint64_t seed, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream,
+                  float4* __restrict__ out, int* __restrict__ status, int stall)
+{
+  cp_flow_tc_body<CP_TC_WG, false>(img_g, params, edges, nb, seed, point0, n, iter, stream, out, status, stall,
+                                   nullptr, nullptr);
+}
+
+// Production form: flow forward, integrand and accept step of the points [L.point0, L.point0 + L.n)
+// in one pass (draws of stream 0, as k_unw_accept takes them), one CTA per SM.
+__global__ void __launch_bounds__(CpTcLayout<CP_TC_WG_ACC>::THREADS, 1)
+    k_flow_accept_tc(const uint4* __restrict__ img_g, const float* __restrict__ params,
+                     const __grid_constant__ CpHadParams P, const __grid_constant__ UnwLaunch L,
+                     int* __restrict__ status, int stall)
+{
+  cp_flow_tc_body<CP_TC_WG_ACC, true>(img_g, params, L.edges, L.nb, L.seed, L.point0, L.n, L.iter, 0u, nullptr,
+                                      status, stall, &P, &L);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -476,7 +571,9 @@ int cp_flow_tc_alloc(cp_handle* h)
     CP_CUDA(h, cudaMalloc(&h->d_flow_status, sizeof(int)));
     CP_CUDA(h, cudaMemsetAsync(h->d_flow_status, 0, sizeof(int), h->stream));
   }
-  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CP_TC_SMEM));
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, CpTcLayout<CP_TC_WG>::SMEM));
+  CP_CUDA(h, cudaFuncSetAttribute(k_flow_accept_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  CpTcLayout<CP_TC_WG_ACC>::SMEM));
   return CP_OK;
 }
 
@@ -491,11 +588,33 @@ int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter,
   const uint64_t want = (pairs + CP_TC_WG - 1) / CP_TC_WG;
   const int grid = (int)(want < (uint64_t)h->num_sms ? want : (uint64_t)h->num_sms);
   if (grid < 1) return CP_OK;
-  k_flow_fwd_tc<<<grid, CP_TC_THREADS, CP_TC_SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_flow,
+  k_flow_fwd_tc<<<grid, CpTcLayout<CP_TC_WG>::THREADS, CpTcLayout<CP_TC_WG>::SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_flow,
                                                                  h->d_edges,
                                                                  h->nb, h->cfg.seed, point0, n, iter, stream, out,
                                                                  h->d_flow_status, h->flow_stall);
   CP_LAUNCH_CHECK(h, "k_flow_fwd_tc");
+  return CP_OK;
+}
+
+// Enqueues the production form over the chunk L (its staging and range totals ready); *blocks =
+// the CTAs launched, each of which writes its slot of L.slots.
+int cp_flow_tc_accept_enqueue(cp_handle* h, const UnwLaunch& L, int* blocks)
+{
+  *blocks = 0;
+  if (h->flow_tc_stale) {
+    const int rc = cp_flow_tc_repack(h);
+    if (rc) return rc;
+    h->flow_tc_stale = 0;
+  }
+  const uint64_t pairs = (L.n + 255) / 256;
+  const uint64_t want = (pairs + CP_TC_WG_ACC - 1) / CP_TC_WG_ACC;
+  const int grid = (int)(want < (uint64_t)h->num_sms ? want : (uint64_t)h->num_sms);
+  if (grid < 1) return CP_OK;
+  using Lay = CpTcLayout<CP_TC_WG_ACC>;
+  k_flow_accept_tc<<<grid, Lay::THREADS, Lay::SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc),
+                                                                  h->d_flow, h->P, L, h->d_flow_status, h->flow_stall);
+  CP_LAUNCH_CHECK(h, "k_flow_accept_tc");
+  *blocks = grid;
   return CP_OK;
 }
 
@@ -512,7 +631,7 @@ int cp_flow_tc_status(cp_handle* h)
   CP_CUDA(h, cudaMemsetAsync(h->d_flow_status, 0, sizeof(int), h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return cp_fail(h, CP_ERR_TIMEOUT, (s & 2) ? "k_flow_wgrad_tc: a tensor-core wait expired (this training step's gradient is invalid)"
-                                            : "k_flow_fwd_tc: a tensor-core wait expired (results of this pass are invalid)");
+                                            : "k_flow_fwd_tc / k_flow_accept_tc: a tensor-core wait expired (results of this pass are invalid)");
 }
 
 // Test hook of the failure path: with on != 0 the issuing warps issue nothing, so every bounded

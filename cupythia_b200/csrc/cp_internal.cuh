@@ -166,6 +166,7 @@ struct cp_handle {
   int flow_kernel = 0;
   int flow_tc_stale = 1;                   // the tcgen05 weight image lags the master parameters
   int flow_stall = 0;                      // test hook: the tensor-core forward issues no MMA
+  int flow_fuse = 0;                       // production passes: flow forward + accept in one kernel
   // optional per-kernel timing of the production pass (CUDA events on the handle's stream):
   // 0 = flow forward, 1 = accept (K1), 2 = record build (K2)
   int timing = 0;

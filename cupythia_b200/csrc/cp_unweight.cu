@@ -24,29 +24,7 @@
 #include <vector>
 #include "cp_internal.cuh"
 
-#define CP_UNW_SLOT 8   // sum w, sum w^2, max w, n_bad, n_acc, sum event weight, n_over, unused
-#define CP_UNW_CHUNK (1ull << 24)   // points per production chunk (staging: 80 B per point)
-#define CP_UNW_RANGE 32             // 32-point blocks per record-builder warp (1024 points)
-
-struct UnwLaunch {
-  uint64_t seed, point0, n;
-  uint32_t iter;
-  int nb;
-  const double* edges;
-  const CpCteqPoly* cteq;
-  const double* wmax;          // device threshold
-  CpEventRec* out;
-  float4* pdf;                 // staging per point: fa[8], fb[8] of the accepted points (K1 -> K2)
-  uint4* tails;                // staging per point: event weight and x[3] (bits), or null (no records)
-  unsigned* bmask;             // accept mask of each 32-point block (bit = lane = point - 32 block)
-  unsigned* rsum;              // accepted points per 1024-point range (zeroed before K1)
-  const unsigned long long* roff;   // output index of the first record of each range
-  uint64_t nblk, nrange;
-  float* scalew;               // per record: 6 scale-variation ratios, or null
-  uint64_t capacity;
-  double* slots;
-  const float4* flow;          // flow output (v, ln J) per in-call point, or null (K1 only)
-};
+#include "cp_unweight.cuh"
 
 static_assert(sizeof(CpEventRec) == 64, "event record must be 64 bytes");
 static_assert(sizeof(CpEventRec) == sizeof(cp_event), "C ABI record layout");
@@ -111,57 +89,20 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
   const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
   const uint64_t gtid = (uint64_t)blockIdx.x * CP_THREADS + threadIdx.x;
   const uint64_t rounds = (L.n + stride - 1) / stride;
-  float s1 = 0.f, c1 = 0.f, s2 = 0.f, c2 = 0.f, se = 0.f, ce = 0.f, wm = 0.f;
-  uint32_t nbad = 0, nacc = 0, nover = 0;
-
+  CpUnwSums S;
   for (uint64_t r = 0; r < rounds; ++r) {
+    // the warp's 32 points are one block: p - lane is a multiple of 32 (stride and block slices are)
     const uint64_t p = r * stride + gtid;
-    bool accept = false;
-    float w = 0.f;
-    CpPoint pt;
+    uint32_t wd[4] = {0u, 0u, 0u, 0u};
     CpMapped m{};
     if (p < L.n) {
-      uint32_t wd[4];
       cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
       m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
-      w = cp_had_eval(P, sCteq, m.x[0], m.x[1], m.x[2], pt) * m.jv;
-      if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
-      cp_kahan(s1, c1, w);
-      cp_kahan(s2, c2, w * w);
-      wm = fmaxf(wm, w);
-      accept = cp_u24(wd[3]) * wmax < w;
     }
-    const unsigned ball = __ballot_sync(0xffffffffu, accept);
-    // the warp's 32 points are one block: p0 is a multiple of 32 (stride and block slices are)
-    const uint64_t p0 = p - (uint64_t)lane;
-    if (L.tails && lane == 0 && p0 < L.n) {
-      L.bmask[p0 >> 5] = ball;
-      if (ball) atomicAdd(&L.rsum[p0 >> 10], (unsigned)__popc(ball));   // integer sum: order-free
-    }
-    if (accept) {
-      const float ew = w > wmax ? w / wmax : 1.f;
-      ++nacc;
-      nover += w > wmax ? 1u : 0u;
-      cp_kahan(se, ce, ew);
-      if (L.tails) {
-        const uint64_t q = p0 + (uint64_t)__popc(ball & ((1u << lane) - 1u));
-        // the event weight and the point's coordinates after the map (and flow): the record
-        // builder starts from them, so it needs neither the map nor the flow output
-        L.tails[q] = make_uint4(__float_as_uint(ew), __float_as_uint(m.x[0]), __float_as_uint(m.x[1]),
-                                __float_as_uint(m.x[2]));
-        // the PDFs of the point, so that the record builder need not evaluate CTEQ5L again
-        float4* f = L.pdf + 4 * q;
-        f[0] = make_float4(pt.fa[0], pt.fa[1], pt.fa[2], pt.fa[3]);
-        f[1] = make_float4(pt.fa[4], pt.fa[5], pt.fa[6], pt.fa[7]);
-        f[2] = make_float4(pt.fb[0], pt.fb[1], pt.fb[2], pt.fb[3]);
-        f[3] = make_float4(pt.fb[4], pt.fb[5], pt.fb[6], pt.fb[7]);
-      }
-    }
+    cp_unw_point(P, sCteq, L, wmax, p, m.x[0], m.x[1], m.x[2], m.jv, cp_u24(wd[3]), S);
   }
-  double v[7] = {(double)s1 - (double)c1, (double)s2 - (double)c2, (double)wm, (double)nbad,
-                 (double)nacc, (double)se - (double)ce, (double)nover};
-#pragma unroll
-  for (int k = 0; k < 7; ++k) v[k] = (k == 2) ? cp_warp_max_d(v[k]) : cp_warp_sum_d(v[k]);
+  double v[7];
+  cp_unw_warp_sums(S, v);
   if (lane == 0)
     for (int k = 0; k < 7; ++k) sRed[warp][k] = v[k];
   __syncthreads();
@@ -379,6 +320,10 @@ static void timing_collect(cp_handle* h, size_t nsub, bool flow, bool build)
   h->t_launches[2] += build ? 1 : 0;
 }
 
+// The flow form's production chunks run the tcgen05 kernel's production form (flow forward,
+// integrand and accept step in one kernel) instead of the forward followed by k_unw_accept.
+static bool fused_production(const cp_handle* h) { return h->flow_on && h->flow_kernel == 0 && h->flow_fuse; }
+
 // Enqueue one production chunk of n <= CP_UNW_CHUNK points on h->stream (no host
 // synchronisation).  Its records go to out[*base_dev ...] in point order (records at or beyond
 // `capacity` are counted, not stored) and *base_dev advances by the chunk's accepted points;
@@ -410,7 +355,8 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
     CP_CUDA(h, cudaMemsetAsync(h->d_rsum, 0, sizeof(unsigned) * L.nrange, h->stream));
   }
   L.flow = nullptr;
-  if (h->flow_on) {
+  const bool fused = fused_production(h);
+  if (h->flow_on && !fused) {
     if (flow_pre) {
       L.flow = flow_pre;
     } else {
@@ -423,10 +369,16 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   }
   cudaEvent_t* ev = (h->timing && tslot >= 0 && h->tpool.size() >= 2 + 3 * (size_t)(tslot + 1)) ? &h->tpool[2 + 3 * tslot] : nullptr;
   if (ev) cudaEventRecord(ev[0], h->stream);
-  k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
-  CP_LAUNCH_CHECK(h, "k_unw_accept");
+  int red_blocks = blocks;
+  if (fused) {
+    rc = cp_flow_tc_accept_enqueue(h, L, &red_blocks);
+    if (rc) return rc;
+  } else {
+    k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+    CP_LAUNCH_CHECK(h, "k_unw_accept");
+  }
   if (ev) cudaEventRecord(ev[1], h->stream);
-  k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, blocks, CP_UNW_SLOT, red_dst);
+  k_reduce_slots<0><<<1, CP_UNW_SLOT * 32, 0, h->stream>>>(h->d_slots, red_blocks, CP_UNW_SLOT, red_dst);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
   if (capacity) {
     k_unw_scan<<<1, 1024, 0, h->stream>>>(h->d_rsum, L.nrange, base_dev, h->d_roff);
@@ -500,8 +452,10 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   int rc = timing_reserve(h, nsub);
   if (rc) return rc;
   CP_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), h->stream));
-  // the flow forward once for the whole pass (16 B per point), then the chunks
-  if (h->flow_on) {
+  // the flow forward once for the whole pass (16 B per point), then the chunks; the fused form
+  // runs the forward inside each chunk's accept kernel
+  const bool fused = fused_production(h);
+  if (h->flow_on && !fused) {
     rc = cp_flow_buffer(h, n_points);
     if (rc) return rc;
     if (h->timing) cudaEventRecord(h->tpool[0], h->stream);
@@ -512,7 +466,7 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   for (uint64_t c = 0; c < nsub; ++c) {
     const uint64_t p0 = c * CP_UNW_CHUNK, n = p0 + CP_UNW_CHUNK <= n_points ? CP_UNW_CHUNK : n_points - p0;
     rc = unweight_enqueue(h, p0, n, iter, records_dev, capacity, h->d_unw_red + 8 * c, h->scalew, h->d_counter,
-                          h->flow_on ? h->d_flow_buf + p0 : nullptr, (int)c);
+                          (h->flow_on && !fused) ? h->d_flow_buf + p0 : nullptr, (int)c);
     if (rc) return rc;
   }
   std::vector<double> hred(8 * nsub, 0.0);
@@ -520,7 +474,7 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   CP_CUDA(h, cudaMemcpyAsync(hred.data(), h->d_unw_red, sizeof(double) * 8 * nsub, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaMemcpyAsync(&cnt, h->d_counter, sizeof cnt, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
-  timing_collect(h, nsub, h->flow_on != 0, capacity > 0);
+  timing_collect(h, nsub, h->flow_on && !fused, capacity > 0);
   if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   double red[8];
   combine_chunks(hred.data(), nsub, red);
@@ -666,7 +620,7 @@ extern "C" int cp_set_scale_weights(cp_handle* h, float* weights_dev, uint64_t c
 }
 
 // Per-kernel timing of the production pass: on != 0 records CUDA events around the flow forward,
-// the accept kernel and the record builder (plus the tiny slot reduction) on the handle's stream
+// the accept kernel (or the fused forward + accept kernel) and the record builder (plus the tiny slot reduction) on the handle's stream
 // and accumulates their durations; cp_kernel_times reads and optionally resets them.
 extern "C" int cp_set_kernel_timing(cp_handle* h, int on)
 {

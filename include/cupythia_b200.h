@@ -335,6 +335,14 @@ int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uin
  * accumulators over 128-point tiles (default), 1 = warp-level mma.sync tiles.  Both compute the
  * same map; CP_ERR_TIMEOUT from a flow-routed call means a bounded tensor-core wait expired. */
 int cp_flow_select_kernel(cp_handle* h, int which);
+/* Production passes in the flow form (cp_unweight, cp_generate_host) with the tcgen05 forward:
+ * on != 0 runs the flow forward, the integrand and the accept step as one kernel per chunk, the
+ * flow's output never leaving the SM (no 16-byte-per-point flow buffer); 0 (default) runs the
+ * forward over the pass first and the accept kernel on its stored output, which is faster on
+ * B200 (21.5 ms against 24.6 ms per 2^27-point pass of the two kernels' work).  Both give the
+ * same records, byte for byte, and the same counts; the sums of w and w^2 differ by their FP64
+ * addition order. */
+int cp_flow_fuse_production(cp_handle* h, int on);
 /* Test hook of the failure path of the tcgen05 forward (no reference counterpart): with on != 0
  * the kernel issues no MMA, every bounded wait expires after about one second, the kernel
  * releases its tensor memory and the call returns CP_ERR_TIMEOUT; the handle stays usable. */
@@ -428,7 +436,8 @@ int cp_write_lhef(const cp_config* cfg, const cp_event* events_host, uint64_t n,
 /* ---------------------------------------------------------------- measurement ------ */
 /* Per-kernel CUDA-event timing of cp_unweight: slot 0 the flow forward, 1 the accept kernel,
  * 2 the record builder (with the slot reduction and the output-offset scan), summed over the
- * pass's chunks; launches3 counts the passes that ran each kernel.
+ * pass's chunks; launches3 counts the passes that ran each kernel.  With the fused flow form
+ * (cp_flow_fuse_production) slot 1 is the fused forward + accept kernel and slot 0 stays empty.
  * No reference counterpart (the reference times whole stages with a host clock,
  * cuPythia/03_fused_resident_me/fused_gg2gg.cu:93-100). */
 int cp_set_kernel_timing(cp_handle* h, int on);

@@ -268,6 +268,71 @@ def test_expired_tensor_core_wait_is_reported_and_recoverable(integ):
     assert np.array_equal(again, ref)
 
 
+def test_fused_production_matches_forward_then_accept():
+    """The flow form's production pass as one tcgen05 kernel per chunk (flow forward, integrand and
+    accept step, the flow output never stored) gives the records of the forward-then-accept path
+    byte for byte, with the same counts, over a pass of two staging chunks (the second ragged),
+    with scale weights, and through the host-delivery call; the sums of w differ only by their
+    addition order (relative 1e-6)."""
+    import torch
+
+    import cupythia_b200 as cp
+    n = (1 << 24) + 4099
+    with cp.Integrator() as it:
+        it.integrate(4, 1 << 20, alpha=1.5)
+        it.flow_init(7)
+        it.flow_train(20, 65536, lr=8e-3)
+        it.flow_enable(True)
+        it.iteration(1 << 20, 70, alpha=0.0)
+        it.weight_quantile(0.999)
+        got = {}
+        for fused in (True, False):
+            it.flow_fuse_production(fused)
+            rec, st = it.unweight(n, iteration=71)
+            r2, sw, st2 = it.unweight_scale_weights(1 << 20, iteration=72)
+            host = torch.empty((st["n_accepted"] + 8, 64), dtype=torch.uint8, pin_memory=True)
+            st3 = it.generate_host(n, host, iteration=71, chunk=3 * (1 << 22) + 1)
+            got[fused] = (cp.events_view(rec).tobytes(), st, cp.events_view(r2).tobytes(), sw.cpu().numpy(), st2,
+                          cp.events_view(host[:st3["n_accepted"]]).tobytes(), st3)
+        it.flow_fuse_production(False)
+    a, b = got[True], got[False]
+    assert a[1]["n_accepted"] > 1000 and a[1]["n_bad"] == 0
+    for k in ("n_accepted", "n_overweight", "n_bad", "n_points"):
+        assert a[1][k] == b[1][k] and a[4][k] == b[4][k] and a[6][k] == b[6][k], k
+    assert a[0] == b[0]
+    assert a[2] == b[2] and np.array_equal(a[3], b[3])
+    assert a[5] == a[0] and b[5] == b[0]
+    for st_a, st_b in ((a[1], b[1]), (a[4], b[4]), (a[6], b[6])):
+        for k in ("sigma", "sigma_err", "sigma_unweighted", "w_max_seen"):
+            assert st_a[k] == pytest.approx(st_b[k], rel=1e-6), k
+
+
+def test_expired_wait_in_fused_production_is_reported_and_recoverable():
+    """Failure detection of the fused production kernel without a GPU fault: with MMA issue
+    stopped by the test hook, its bounded waits expire, cp_unweight returns CP_ERR_TIMEOUT (4),
+    and the next pass on the same handle returns the records of an undisturbed pass."""
+    import cupythia_b200 as cp
+    with cp.Integrator() as it:
+        it.integrate(2, 1 << 18, alpha=1.5)
+        it.flow_init(7)
+        it.flow_enable(True)
+        it.flow_fuse_production(True)
+        it.iteration(1 << 18, 80, alpha=0.0)
+        it.weight_quantile(0.999)
+        rec, st = it.unweight(1 << 18, iteration=81)
+        ref = cp.events_view(rec).tobytes()
+        it.lib.cp_flow_test_stall(it.h, 1)
+        try:
+            with pytest.raises(cp.CpError) as e:
+                it.unweight(1 << 18, iteration=81)
+            assert e.value.code == 4
+        finally:
+            it.lib.cp_flow_test_stall(it.h, 0)
+        rec2, st2 = it.unweight(1 << 18, iteration=81)
+        assert st2["n_accepted"] == st["n_accepted"]
+        assert cp.events_view(rec2).tobytes() == ref
+
+
 def test_diverged_flow_is_reported_as_numeric_fault():
     """A flow with non-finite parameters (what a diverged training leaves) makes the next pass report
     CP_ERR_NUMERIC (3) with the bad weights zeroed and counted; with the flow switched off the
