@@ -176,9 +176,11 @@ UNW_CHUNK = 1 << 24               # points per production chunk of the library (
 # div FP32 ops, 35 exp + 26 log + 2 sqrt + 9 reciprocals on the MUFU
 ALG_FP32_OPS_PER_POINT = 795
 ALG_MUFU_OPS_PER_POINT = 72
-# k_unw_accept, executed: FADD + FMUL + 2 FFMA per point from the ncu SASS counters (profiles/),
-# i.e. the algorithm plus the FP32 precision bookkeeping (compensated sums, (hi, lo) logarithms)
-EXEC_FLOP_PER_POINT = 3278.0
+# k_unw_accept, executed: FADD + FMUL + 2 FFMA lane operations per point from the ncu per-opcode
+# counters of a flow-form launch (profiles/k_unw_accept_production_2e24.md; packed two-lane
+# forms counted per lane), i.e. the algorithm plus the FP32 precision bookkeeping (FMA residuals,
+# (hi, lo) logarithms) and the library transcendentals' own arithmetic
+EXEC_FLOP_PER_POINT = 2563.0
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
 # launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points

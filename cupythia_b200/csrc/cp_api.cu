@@ -153,7 +153,7 @@ extern "C" int cp_destroy(cp_handle* h)
   if (h->h_gen_cnt) cudaFreeHost(h->h_gen_cnt);
   void* bufs[] = {h->d_edges, h->d_slots, h->d_red, h->d_iters, h->d_x1, h->d_x2, h->d_sH,
                   h->d_tH, h->d_uH, h->d_as, h->d_q2r, h->d_q2f, h->d_qhist, h->d_wmax, h->d_counter, h->d_cteq, h->d_flow, h->d_flow_pk,
-                  h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_pdfbuf,
+                  h->d_flow_bias, h->d_flow_buf, h->d_flow_tc, h->d_flow_status, h->d_flow_ticket, h->d_pdfbuf,
                   h->d_gen_stage, h->d_gen_red, h->d_gen_cnt, h->d_ftrain, h->d_tails, h->d_bmask,
                   h->d_rsum, h->d_roff, h->d_unw_red};
   for (void* b : bufs)

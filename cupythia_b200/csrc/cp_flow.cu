@@ -27,7 +27,9 @@ __global__ void k_flow_init(float* P, uint64_t seed)
   P[i] = v;
 }
 
-// FP32 master -> BF16 B fragments (forward and transposed) and staged biases.
+// FP32 master -> BF16 B fragments (forward and transposed) and staged biases; grid (coupling,
+// CP_FLOW_PACK_SPLIT blocks sharing its fragments).
+#define CP_FLOW_PACK_SPLIT 8
 __global__ void k_flow_pack(const float* __restrict__ P, uint2* __restrict__ pk, float* __restrict__ bias)
 {
   const int c = blockIdx.x;
@@ -35,7 +37,8 @@ __global__ void k_flow_pack(const float* __restrict__ P, uint2* __restrict__ pk,
   const float* W2 = P + c * CP_FLOW_PER + CP_FLOW_W2;
   const float* W3 = P + c * CP_FLOW_PER + CP_FLOW_W3;
   uint2* q = pk + c * CP_FLOW_P_PER;
-  for (int e = threadIdx.x; e < CP_FLOW_P_PER; e += blockDim.x) {
+  const int t0 = blockIdx.y * blockDim.x + threadIdx.x, tstride = gridDim.y * blockDim.x;
+  for (int e = t0; e < CP_FLOW_P_PER; e += tstride) {
     const int lane = e & 31, gid = lane >> 2, tig = lane & 3, f = e >> 5;
     float a0, a1, a2, a3;
     if (e < CP_FLOW_P_W2) {                       // W1 [16][64]: tile nt = f
@@ -61,7 +64,7 @@ __global__ void k_flow_pack(const float* __restrict__ P, uint2* __restrict__ pk,
     }
     q[e] = make_uint2(cp_bf2(a0, a1), cp_bf2(a2, a3));
   }
-  for (int j = threadIdx.x; j < CP_FLOW_NB; j += blockDim.x) {
+  for (int j = t0; j < CP_FLOW_NB; j += tstride) {
     float v;
     if (j < 64) v = P[c * CP_FLOW_PER + CP_FLOW_B1 + j];
     else if (j < 128) v = P[c * CP_FLOW_PER + CP_FLOW_B2 + j - 64];
@@ -124,6 +127,8 @@ int cp_flow_ensure(cp_handle* h)
   CP_CUDA(h, cudaMemsetAsync(h->d_flow, 0, sizeof(float) * CP_FLOW_NPARAM * 4, h->stream));
   CP_CUDA(h, cudaMalloc(&h->d_flow_pk, sizeof(uint2) * CP_FLOW_NC * CP_FLOW_P_PER));
   CP_CUDA(h, cudaMalloc(&h->d_flow_bias, sizeof(float) * CP_FLOW_NC * CP_FLOW_NB));
+  CP_CUDA(h, cudaMalloc(&h->d_flow_ticket, sizeof(unsigned)));
+  CP_CUDA(h, cudaMemsetAsync(h->d_flow_ticket, 0, sizeof(unsigned), h->stream));
   CP_CUDA(h, cudaFuncSetAttribute(k_flow_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)flow_fwd_smem()));
   return cp_flow_tc_alloc(h);
 }
@@ -133,7 +138,7 @@ int cp_flow_ensure(cp_handle* h)
 // run does not repack it after every update.
 int cp_flow_repack(cp_handle* h)
 {
-  k_flow_pack<<<CP_FLOW_NC, 256, 0, h->stream>>>(h->d_flow, h->d_flow_pk, h->d_flow_bias);
+  k_flow_pack<<<dim3(CP_FLOW_NC, CP_FLOW_PACK_SPLIT), 256, 0, h->stream>>>(h->d_flow, h->d_flow_pk, h->d_flow_bias);
   CP_LAUNCH_CHECK(h, "k_flow_pack");
   h->flow_tc_stale = 1;
   return CP_OK;

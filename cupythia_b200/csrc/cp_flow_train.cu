@@ -97,12 +97,19 @@ __global__ void __launch_bounds__(CP_THREADS, 2) k_flow_fwd_train(const uint2* _
 // ------------------------------------------------------------------------------------------
 // 2. integrand value and d ln f / dx at the flow's points (3-tangent duals), batch sums
 // ------------------------------------------------------------------------------------------
+// Each block writes its (sum w, sum w^2) to its slot; the block that finishes last (integer
+// ticket, after a fence) adds all slots in a fixed order (strided per-thread sums, the xor tree
+// of each warp, the warps in order) into moments[0..1], writes the batch loss <w^2>/<w>^2 over
+// n_loss points when loss != null, and re-arms the ticket.
 __global__ void __launch_bounds__(128) k_flow_igrad(const CpHadParams P, const CpCteqPoly* __restrict__ cteq_g,
                                                     uint64_t n, float lnTauMin, const float4* __restrict__ vj,
-                                                    float4* __restrict__ wg, double* __restrict__ slots)
+                                                    float4* __restrict__ wg, double* __restrict__ slots,
+                                                    unsigned* __restrict__ ticket, double* __restrict__ moments,
+                                                    double n_loss, double* __restrict__ loss)
 {
   __shared__ CpCteqPoly sCteq[8];
   __shared__ double sRed[4][2];
+  __shared__ int sLast;
   cp_stage_cteq(sCteq, cteq_g);
   __syncthreads();
   typedef CpDual<3> D3;
@@ -134,6 +141,33 @@ __global__ void __launch_bounds__(128) k_flow_igrad(const CpHadParams P, const C
     for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += sRed[q][0]; b += sRed[q][1]; }
     slots[2 * blockIdx.x] = a;
     slots[2 * blockIdx.x + 1] = b;
+    __threadfence();
+    sLast = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!sLast) return;
+  __threadfence();
+  double a = 0.0, b = 0.0;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+    a += __ldcg(slots + 2 * k);
+    b += __ldcg(slots + 2 * k + 1);
+  }
+  a = cp_warp_sum_d(a);
+  b = cp_warp_sum_d(b);
+  __syncthreads();   // sRed is reused
+  if ((threadIdx.x & 31) == 0) { sRed[threadIdx.x >> 5][0] = a; sRed[threadIdx.x >> 5][1] = b; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = 0.0;
+    b = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += sRed[q][0]; b += sRed[q][1]; }
+    moments[0] = a;
+    moments[1] = b;
+    if (loss) {
+      const double m = a / n_loss;
+      loss[0] = (b / n_loss) / (m * m);
+    }
+    *ticket = 0u;
   }
 }
 
@@ -677,13 +711,9 @@ __host__ __device__ __forceinline__ bool cp_flow_param_used(int i)
   return (o - CP_FLOW_B3) < nout;
 }
 
-__global__ void k_flow_adam(float* __restrict__ P, float* __restrict__ G, float* __restrict__ Mo, float* __restrict__ Vo,
-                            float lr, float b1t, float b2t)
+__device__ __forceinline__ void cp_flow_adam_one(int i, float g, float* __restrict__ P, float* __restrict__ Mo,
+                                                 float* __restrict__ Vo, float lr, float b1t, float b2t)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= CP_FLOW_NPARAM) return;
-  const float g = G[i];
-  G[i] = 0.f;
   if (!cp_flow_param_used(i)) { P[i] = 0.f; return; }
   const float m = 0.9f * Mo[i] + 0.1f * g, v = 0.999f * Vo[i] + 0.001f * g * g;
   Mo[i] = m;
@@ -691,19 +721,27 @@ __global__ void k_flow_adam(float* __restrict__ P, float* __restrict__ G, float*
   P[i] -= lr * (m / (1.f - b1t)) / (sqrtf(v / (1.f - b2t)) + 1e-8f);
 }
 
-// batch moments of this handle's points from the integrand kernel's block slots, fixed order
-// (one warp: strided lane sums, then the xor tree; the same order on every run)
-__global__ void k_flow_moments(const double* slots, int nblk, double* moments)
+__global__ void k_flow_adam(float* __restrict__ P, float* __restrict__ G, float* __restrict__ Mo, float* __restrict__ Vo,
+                            float lr, float b1t, float b2t)
 {
-  const int lane = threadIdx.x & 31;
-  double a = 0.0, b = 0.0;
-  for (int k = lane; k < nblk; k += 32) { a += slots[2 * k]; b += slots[2 * k + 1]; }
-  a = cp_warp_sum_d(a);
-  b = cp_warp_sum_d(b);
-  if (lane == 0) {
-    moments[0] = a;
-    moments[1] = b;
-  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= CP_FLOW_NPARAM) return;
+  const float g = G[i];
+  G[i] = 0.f;
+  cp_flow_adam_one(i, g, P, Mo, Vo, lr, b1t, b2t);
+}
+
+// k_flow_gsum into a cleared G followed by k_flow_adam, in one pass (a single handle's training
+// loop, where no exchange of G sits between them): the same block-order sum, 0 + sum as the
+// gradient, the same update, so the same parameters bit for bit; G is not touched.
+__global__ void k_flow_gsum_adam(float* __restrict__ P, const float* __restrict__ part, int nblk, float* __restrict__ Mo,
+                                 float* __restrict__ Vo, float lr, float b1t, float b2t)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= CP_FLOW_NPARAM) return;
+  float s = 0.f;
+  for (int b = 0; b < nblk; ++b) s += part[(size_t)b * CP_FLOW_NPARAM + i];
+  cp_flow_adam_one(i, 0.f + s, P, Mo, Vo, lr, b1t, b2t);
 }
 
 // the batch's moments (summed over ranks) for the backward pass, and its loss <w^2> / <w>^2
@@ -785,7 +823,7 @@ static void train_buffers_release(cp_handle* h)
 // Phase 1 of a step: forward and integrand over the batch points [point0, point0 + count) at
 // counter iteration `iter` (Philox stream 2); moments[0..1] = (sum w, sum w^2) over them.
 static int flow_phase_moments(cp_handle* h, const FlowTrainBufs& t, uint64_t point0, uint64_t count, uint32_t iter,
-                              double* moments)
+                              double* moments, double* loss_dev = nullptr)
 {
   k_flow_fwd_train<<<h->num_sms * 2, CP_THREADS, fwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, h->d_edges, h->nb,
                                                                            h->cfg.seed, iter, 2, point0, count, t.zs, t.vj);
@@ -794,20 +832,24 @@ static int flow_phase_moments(cp_handle* h, const FlowTrainBufs& t, uint64_t poi
   int rc = cp_ensure_slots(h, (size_t)2 * gblk);
   if (rc) return rc;
   const float lnTauMin = (float)log(4.0 * h->cfg.pt_hat_min * h->cfg.pt_hat_min / (h->cfg.sqrt_s * h->cfg.sqrt_s));
-  k_flow_igrad<<<gblk, 128, 0, h->stream>>>(h->P, h->d_cteq, count, lnTauMin, t.vj, t.wg, h->d_slots);
+  k_flow_igrad<<<gblk, 128, 0, h->stream>>>(h->P, h->d_cteq, count, lnTauMin, t.vj, t.wg, h->d_slots,
+                                            h->d_flow_ticket, moments, (double)count, loss_dev);
   CP_LAUNCH_CHECK(h, "k_flow_igrad");
-  k_flow_moments<<<1, 32, 0, h->stream>>>(h->d_slots, gblk, moments);
-  CP_LAUNCH_CHECK(h, "k_flow_moments");
   return CP_OK;
 }
 
 // Phase 2: this handle's points' part of the gradient of the batch loss, from the batch's
 // moments over n_batch points, into the gradient buffer G (cleared first); loss_dev = the loss.
+// A single handle's loop passes local = true (moments already in t.sums, the loss written by
+// phase 1): the per-block partial gradients are left in t.gpart for flow_phase_update_local,
+// and *nblk_out receives their number.
 static int flow_phase_gradient(cp_handle* h, const FlowTrainBufs& t, uint64_t count, const double* moments,
-                               uint64_t n_batch, double* loss_dev)
+                               uint64_t n_batch, double* loss_dev, bool local = false, int* nblk_out = nullptr)
 {
-  k_flow_batch_loss<<<1, 1, 0, h->stream>>>(moments, (double)n_batch, t.sums, loss_dev);
-  CP_LAUNCH_CHECK(h, "k_flow_batch_loss");
+  if (!local) {
+    k_flow_batch_loss<<<1, 1, 0, h->stream>>>(moments, (double)n_batch, t.sums, loss_dev);
+    CP_LAUNCH_CHECK(h, "k_flow_batch_loss");
+  }
   k_flow_bwd<<<h->num_sms * 2, CP_BWD_THREADS, bwd_smem(), h->stream>>>(h->d_flow_pk, h->d_flow_bias, count, (double)n_batch, t.zs,
                                                           t.vj, t.wg, t.sums, t, (float)h->flow_loss_p);
   CP_LAUNCH_CHECK(h, "k_flow_bwd");
@@ -834,6 +876,10 @@ static int flow_phase_gradient(cp_handle* h, const FlowTrainBufs& t, uint64_t co
                                                       CP_FLOW_B3 - CP_FLOW_W3);
     CP_LAUNCH_CHECK(h, "k_flow_wgrad");
   }
+  if (local) {
+    *nblk_out = nblk;
+    return CP_OK;
+  }
   CP_CUDA(h, cudaMemsetAsync(G, 0, sizeof(float) * CP_FLOW_NPARAM, h->stream));
   k_flow_gsum<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(t.gpart, nblk, G);
   CP_LAUNCH_CHECK(h, "k_flow_gsum");
@@ -849,6 +895,22 @@ static int flow_phase_update(cp_handle* h, double lr)
       h->d_flow, G, G + CP_FLOW_NPARAM, G + 2 * CP_FLOW_NPARAM, (float)lr, (float)pow(0.9, (double)step),
       (float)pow(0.999, (double)step));
   CP_LAUNCH_CHECK(h, "k_flow_adam");
+  const int rc = cp_flow_repack(h);
+  if (rc) return rc;
+  h->flow_t = step;
+  return CP_OK;
+}
+
+// Phase 3 of a single handle's step: the block-order gradient sum and the Adam step in one kernel
+// (the same parameters as k_flow_gsum + flow_phase_update), BF16 repack.
+static int flow_phase_update_local(cp_handle* h, const FlowTrainBufs& t, int nblk, double lr)
+{
+  float* G = h->d_flow + CP_FLOW_NPARAM;
+  const long step = h->flow_t + 1;
+  k_flow_gsum_adam<<<(CP_FLOW_NPARAM + 255) / 256, 256, 0, h->stream>>>(
+      h->d_flow, t.gpart, nblk, G + CP_FLOW_NPARAM, G + 2 * CP_FLOW_NPARAM, (float)lr, (float)pow(0.9, (double)step),
+      (float)pow(0.999, (double)step));
+  CP_LAUNCH_CHECK(h, "k_flow_gsum_adam");
   const int rc = cp_flow_repack(h);
   if (rc) return rc;
   h->flow_t = step;
@@ -879,9 +941,10 @@ extern "C" int cp_flow_train(cp_handle* h, int n_steps, uint64_t batch, double l
   double* losses = nullptr;
   CP_CUDA(h, cudaMalloc(&losses, sizeof(double) * (size_t)n_steps));
   for (int s = 0; s < n_steps && rc == CP_OK; ++s) {
-    rc = flow_phase_moments(h, t, 0, batch, (uint32_t)h->flow_t, t.sums);
-    if (!rc) rc = flow_phase_gradient(h, t, batch, t.sums, batch, losses + s);
-    if (!rc) rc = flow_phase_update(h, lr);
+    int nblk = 0;
+    rc = flow_phase_moments(h, t, 0, batch, (uint32_t)h->flow_t, t.sums, losses + s);
+    if (!rc) rc = flow_phase_gradient(h, t, batch, t.sums, batch, losses + s, true, &nblk);
+    if (!rc) rc = flow_phase_update_local(h, t, nblk, lr);
   }
   cudaError_t e = cudaSuccess;
   if (!rc && loss_host) e = cudaMemcpyAsync(loss_host, losses, sizeof(double) * n_steps, cudaMemcpyDeviceToHost, h->stream);

@@ -163,6 +163,7 @@ struct cp_handle {
   // flow_kernel 0 = tcgen05 kernel, 1 = the warp-level mma.sync kernel
   uint8_t* d_flow_tc = nullptr;
   int* d_flow_status = nullptr;
+  unsigned* d_flow_ticket = nullptr;       // last-block ticket of the training integrand kernel (0 between launches)
   int flow_kernel = 0;
   int flow_tc_stale = 1;                   // the tcgen05 weight image lags the master parameters
   int flow_stall = 0;                      // test hook: the tensor-core forward issues no MMA

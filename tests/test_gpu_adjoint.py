@@ -208,3 +208,45 @@ def test_variance_gradient_adaptation_vs_classic_vegas():
     assert rel["classic"] < 0.35 * rel["uniform"], rel
     for k in ("gradient", "classic"):
         assert abs(res[k]["sigma"] - res["uniform"]["sigma"]) < 5 * res["uniform"]["sigma_err"]
+
+
+def test_gradient_steps_against_classic_vegas_at_equal_points():
+    """Two-sided comparison with classic VEGAS at equal points (2^22 fresh points, the same draws,
+    on each grid).  From the classic grid (8 x 2^21 points), 12 gradient steps of the weight
+    variance (moment order 2) leave the relative variance within 15% of classic's either way:
+    classic refinement already sits at the variance optimum of a separable grid (measured 0.61 ->
+    0.64).  12 steps of moment order 4 cut their objective R4 = <w^4>/<w>^4 to under half of
+    classic's (measured 25 -> 9) and raise eta at q99.9 by at least 15% (measured 0.208 -> 0.273),
+    for at most 1.5 times the relative variance (measured 0.61 -> 0.80)."""
+    import torch
+
+    import cupythia_b200 as cp
+    n = 1 << 22
+
+    def stats(it):
+        r = it.iteration(n, 91, alpha=0.0)
+        w = it.point_weights(0, n, 91).double()
+        m = w.mean()
+        wq = it.weight_quantile(0.999)
+        return {"relvar": (r["sigma_err"] / r["sigma"]) ** 2 * n, "r4": ((w / m) ** 4).mean().item(),
+                "eta": (torch.clamp(w, max=wq).mean() / wq).item(), "sigma": r["sigma"], "err": r["sigma_err"]}
+
+    res = {}
+    with cp.Integrator() as it:
+        for s in range(8):
+            it.iteration(1 << 21, s, alpha=1.5)
+        res["classic"] = stats(it)
+        g = it.grid
+        for p in (2.0, 4.0):
+            it.grid = g
+            it.gradient_objective(p)
+            it.adapt_gradient(12, 1 << 21, lr=0.2, iteration0=200)
+            it.gradient_objective(2.0)
+            res[p] = stats(it)
+    c = res["classic"]
+    assert 1 / 1.15 < res[2.0]["relvar"] / c["relvar"] < 1.15, res
+    assert res[4.0]["r4"] < 0.5 * c["r4"], res
+    assert res[4.0]["eta"] > 1.15 * c["eta"], res
+    assert res[4.0]["relvar"] < 1.5 * c["relvar"], res
+    for k in (2.0, 4.0):
+        assert abs(res[k]["sigma"] - c["sigma"]) < 5 * np.hypot(res[k]["err"], c["err"]), res
