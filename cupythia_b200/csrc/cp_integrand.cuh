@@ -80,10 +80,29 @@ struct CpHadParams {
   int   nfmax6;       // 1 if nf = 6 above mt
 };
 
-// Math on the device is CUDA's accurate single-precision library; on the host, libm.
+// Math on the host is libm.  On the device exp, expm1 and sqrt are CUDA's accurate
+// single-precision functions, and the natural logarithm is the hardware base-2 approximation
+// times ln 2 (__logf; the accept kernel runs 17% faster than with the accurate logf).  What the integrand needs of a logarithm is a small ABSOLUTE error (about 1e-7): each
+// one enters an exponent (CTEQ5L), a product with an O(1) coefficient, or alpha_s's denominator
+// ln(Q^2 / Lambda^2) >= ln(50 GeV^2 / Lambda_5^2) here.  Measured against the FP64 oracle over
+// 2^20 points on the uniform and an adapted grid and 2^18 at four parameter-range corners, the
+// largest per-point weight error is 6.7e-6 with __logf and 6.7e-6 with logf (with cp_exp_cteq
+// below as well: 7.3e-6).
 CP_HD float cp_expf(float x) { return expf(x); }
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float cp_logf(float x) { return __logf(x); }
+#else
 CP_HD float cp_logf(float x) { return logf(x); }
+#endif
 CP_HD float cp_expm1f(float x) { return expm1f(x); }
+// exp of the CTEQ5L exponent on the device: the hardware base-2 approximation (__expf), relative
+// error about 2^-22 + |x| 2^-24 for exponents of a few units; the accept kernel a further 3%
+// faster, the largest per-point weight error 7.3e-6 (measured as above)
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ float cp_exp_cteq(float x) { return __expf(x); }
+#else
+CP_HD float cp_exp_cteq(float x) { return expf(x); }
+#endif
 CP_HD float cp_sqrtf(float x) { return sqrtf(x); }
 CP_HD float cp_fmaf(float a, float b, float c) { return fmaf(a, b, c); }
 // a / b for a sub-ulp correction term a: the quotient's last bits do not reach the result, so
@@ -240,7 +259,7 @@ CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX&
   const CpF2 t7 = cp_mul2(a2, L), t7l = cp_fma2(a2, L, cp_f2(-t7.x, -t7.y));
   const CpF2 el = cp_add2(cp_add2(t2l, t3l), cp_add2(cp_add2(t4l, t6l), t7l));
   const CpF2 eh = cp_add2(cp_add2(cp_add2(cp_f2s(a.A), t3), cp_add2(t4, t2)), cp_add2(part3, cp_add2(t6, t7)));
-  const CpF2 ex = cp_f2(cp_expf(eh.x), cp_expf(eh.y));
+  const CpF2 ex = cp_f2(cp_exp_cteq(eh.x), cp_exp_cteq(eh.y));
   return cp_mul2(cp_mul2(x, cp_fma2(ex, el, ex)), cp_f2s(a.qfac));
 }
 
