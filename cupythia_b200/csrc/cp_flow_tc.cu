@@ -10,8 +10,8 @@
 // accept step of the production pass (the code of k_unw_accept, shared through cp_unweight.cuh),
 // so no flow output is stored.  Its records equal the two-kernel path's byte for byte, but it is
 // the slower of the two: a warpgroup's slots idle while its warps run the integrand, and the
-// integrand's FMA-bound warps lengthen every flow step (2^27 points on B200: 24.6 ms with 4
-// warpgroups at 96 registers, 25.3 ms with 3 at 128, against 10.4 + 11.1 ms for the two kernels).
+// integrand's FMA-bound warps lengthen every flow step (2^27 points on B200: 21.5 ms with 4
+// warpgroups at 96 registers, against 10.4 + 8.9 ms for the two kernels).
 //
 // Launch: one persistent CTA per SM (the shared-memory footprint admits one): 4 epilogue
 // warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two
