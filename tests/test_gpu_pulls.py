@@ -1,9 +1,9 @@
 """Multi-seed pull distribution of sigma for both forms of the dijet integrator.
 
 One seed is one full run: the config-2 adaptation (10 x 2^24 points, classic refinement), then,
-for the flow+adjoint form, the variance-gradient steps and the flow trained on 200 x 65,536
-points, then one fresh production-sized pass of 2^24 points on counter points disjoint from
-everything the adaptation saw.  Across seeds (the Philox key of the whole run):
+for the flow+adjoint form, the bench's recipe: 12 variance-gradient steps (backtracking) and the
+flow trained on 200 x 65,536 points (moment orders 3 then 4), then one fresh production-sized
+pass of 2^24 points on counter points disjoint from everything the adaptation saw.  Across seeds (the Philox key of the whole run):
   * the error estimate is honest: the spread of sigma_i about the seeds' mean, in units of each
     run's own sigma_err, has a standard deviation between 0.7 and 1.4;
   * the estimate is unbiased against the FP64 oracle (tests/golden/sigma_oracle.json, 2^28 points):
@@ -39,10 +39,12 @@ def _runs(flow):
         with cp.Integrator(seed=seed) as it:
             it.integrate(10, N, alpha=1.5, skip=3)
             if flow:
-                for k in range(12):
-                    it.gradient_step(1 << 22, 200 + k, lr=0.2)
+                it.adapt_gradient(12, 1 << 22, lr=0.2, iteration0=200)
                 it.flow_init(7)
-                it.flow_train(200, 65536, lr=8e-3)
+                for steps, p in ((100, 3.0), (100, 4.0)):
+                    it.flow_objective(p)
+                    it.flow_train(steps, 65536, lr=8e-3)
+                it.flow_objective(2.0)
                 it.flow_enable(True)
             r = it.iteration(N, 7000, alpha=0.0)
             assert r["n_bad"] == 0
