@@ -743,16 +743,21 @@ CP_HD void cp_make_event(const CpHadParams& P, const CpPoint& pt, float r0, floa
   float z = 0.5f * (k.opz - k.omz);
   float sinT = cp_sqrtf(k.omz * k.opz);
   float pT = pstar * sinT;
-  float phi = 6.283185307f * r2;
+  // azimuth phi = 2 pi r2: sin and cos of pi (2 r2), without the argument reduction of sincosf
   float sphi, cphi;
 #if defined(__CUDA_ARCH__)
-  sincosf(phi, &sphi, &cphi);
+  sincospif(2.f * r2, &sphi, &cphi);
 #else
-  sphi = sinf(phi); cphi = cosf(phi);
+  sphi = (float)sin(6.283185307179586 * (double)r2); cphi = (float)cos(6.283185307179586 * (double)r2);
 #endif
   float pzs = pstar * z;
   float y = 0.5f * (k.lnx1 - k.lnx2);
-  float ey = cp_expf(y), iey = cp_expf(-y);
+  float ey = cp_expf(y);
+#if defined(__CUDA_ARCH__)
+  float iey = __frcp_rn(ey);   // correctly rounded 1 / e^y
+#else
+  float iey = 1.f / ey;
+#endif
   float ch = 0.5f * (ey + iey), sh = 0.5f * (ey - iey);
   ev.p3[0] = pT * cphi; ev.p3[1] = pT * sphi;
   ev.p3[2] = pzs * ch + pstar * sh; ev.p3[3] = pstar * ch + pzs * sh;
