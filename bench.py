@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--points", type=int, default=1 << 27, help="points per step and rank")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample length")
+    ap.add_argument("--fused-production", action="store_true",
+                    help="flow form through the fused flow + accept kernel (cp_flow_fuse_production) "
+                         "instead of the forward followed by the accept kernel")
     return ap.parse_args()
 
 
@@ -326,6 +329,7 @@ def run_ours(a):
         relvar = {k: (r["sigma_err"] / r["sigma"]) ** 2 * ADAPT_POINTS for k, r in
                   (("vegas", r_vegas), ("flow", r_flowp))}
         use_flow = relvar["flow"] < relvar["vegas"]
+        it.flow_fuse_production(a.fused_production)
         if not use_flow:
             it.flow_enable(False)
             si.iteration(ADAPT_POINTS, 300, alpha=0.0)
@@ -439,7 +443,8 @@ def run_ours(a):
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * sec_f / a.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (counter-based Philox draws, seed 42)",
-        "config": {"workload": WORKLOAD, "form": "flow+adjoint: classic VEGAS, variance-gradient (adjoint) grid "
+        "config": {"workload": WORKLOAD, "production": "fused flow + accept kernel" if fused else "flow forward, then accept kernel",
+                   "form": "flow+adjoint: classic VEGAS, variance-gradient (adjoint) grid "
                    "refinement, BF16 coupling flow trained 200 x 65536 points (moment orders 3 then 4), "
                    "unweighting at q99.9",
                    "points_per_step_per_gpu": n, "adapt_points": ADAPT_ITERS * ADAPT_POINTS,
