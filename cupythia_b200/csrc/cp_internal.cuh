@@ -115,6 +115,7 @@ struct cp_handle {
   int build_per_sm[2] = {-1, -1};   // record builder without / with scale weights
   // weight histogram of the last iteration and the unweighting threshold (device)
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
+  double wmax_host = 0.0;                  // the unweighting threshold d_wmax[0], as last set
   double* d_wmax = nullptr;                // [0] threshold used by cp_unweight, [1] quantile q
   unsigned long long* d_counter = nullptr; // accepted-event counter
   // production staging for pdfbuf_cap points (K1 -> K2): PDFs and record tails per point, accept

@@ -421,6 +421,7 @@ extern "C" int cp_set_wmax(cp_handle* h, double w_max)
   k_set_wmax<<<1, 1, 0, h->stream>>>(h->d_wmax, w_max);
   CP_LAUNCH_CHECK(h, "k_set_wmax");
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->wmax_host = w_max;
   return CP_OK;
 }
 
@@ -431,10 +432,10 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   if (n_points < 2) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: n_points < 2");
   if (capacity && !records_dev) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: null records");
   if (((uintptr_t)records_dev & 15) != 0) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: records must be 16-byte aligned");
-  double wm[2];
-  CP_CUDA(h, cudaMemcpyAsync(wm, h->d_wmax, sizeof wm, cudaMemcpyDeviceToHost, h->stream));
-  CP_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: no threshold (cp_weight_quantile or cp_set_wmax)");
+  // the threshold as cp_weight_quantile / cp_weight_quantile_hist / cp_set_wmax last set it: no
+  // device read, so the host enqueues the pass while the stream's earlier work still runs
+  const double wm0 = h->wmax_host;
+  if (!(wm0 > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_unweight: no threshold (cp_weight_quantile or cp_set_wmax)");
   if (n_points > (1ull << 32)) return cp_fail(h, CP_ERR_INVALID, "at most 2^32 points per production call");
   if (h->scalew && capacity > h->scalew_cap)
     return cp_fail(h, CP_ERR_INVALID, "cp_unweight: record capacity exceeds the scale-weight buffer (cp_set_scale_weights)");
@@ -478,7 +479,7 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   double red[8];
   combine_chunks(hred.data(), nsub, red);
-  if (out) fill_unw(red, (double)n_points, wm[0], out);
+  if (out) fill_unw(red, (double)n_points, wm0, out);
   if (cnt > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_unweight: record buffer too small (n_accepted reported)");
   if (red[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
   return CP_OK;
@@ -539,10 +540,8 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   CP_CHECK_HANDLE(h);
   if (n_points < 2 || chunk < 2) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: bad sizes");
   if (capacity && !records_host) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: null records");
-  double wm[2];
-  CP_CUDA(h, cudaMemcpyAsync(wm, h->d_wmax, sizeof wm, cudaMemcpyDeviceToHost, h->stream));
-  CP_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (!(wm[0] > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: no threshold");
+  const double wm0 = h->wmax_host;
+  if (!(wm0 > 0)) return cp_fail(h, CP_ERR_INVALID, "cp_generate_host: no threshold");
   if (chunk > n_points) chunk = n_points;
   if (chunk > CP_UNW_CHUNK) chunk = CP_UNW_CHUNK;
   const uint64_t nchunks = (n_points + chunk - 1) / chunk;
@@ -600,7 +599,7 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
   if (h->flow_on && (rc = cp_flow_tc_status(h)) != CP_OK) return rc;
   double tot[8];
   combine_chunks(hred.data(), nchunks, tot);
-  if (out) fill_unw(tot, (double)n_points, wm[0], out);
+  if (out) fill_unw(tot, (double)n_points, wm0, out);
   if (total_acc > capacity) return cp_fail(h, CP_ERR_CAPACITY, "cp_generate_host: record buffer too small");
   if (tot[3] > 0) return cp_fail(h, CP_ERR_NUMERIC, "non-finite or negative weights were zeroed");
   return CP_OK;

@@ -381,12 +381,11 @@ extern "C" int cp_weight_quantile(cp_handle* h, double q, double* w_q)
   if (h->last_n == 0) return cp_fail(h, CP_ERR_INVALID, "cp_weight_quantile: run an iteration first");
   k_quantile<<<1, 256, 0, h->stream>>>(h->d_qhist, q, h->d_wmax);
   CP_LAUNCH_CHECK(h, "k_quantile");
-  if (w_q) {
-    double v[2];
-    CP_CUDA(h, cudaMemcpyAsync(v, h->d_wmax, sizeof v, cudaMemcpyDeviceToHost, h->stream));
-    CP_CUDA(h, cudaStreamSynchronize(h->stream));
-    *w_q = v[0];
-  }
+  double v[2];
+  CP_CUDA(h, cudaMemcpyAsync(v, h->d_wmax, sizeof v, cudaMemcpyDeviceToHost, h->stream));
+  CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->wmax_host = v[0];   // production passes check the threshold without reading the device
+  if (w_q) *w_q = v[0];
   return CP_OK;
 }
 
@@ -446,6 +445,7 @@ extern "C" int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* h
   double v[2];
   CP_CUDA(h, cudaMemcpyAsync(v, h->d_wmax, sizeof v, cudaMemcpyDeviceToHost, h->stream));
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->wmax_host = v[0];
   if (w_q) *w_q = v[0];
   return CP_OK;
 }
