@@ -107,6 +107,16 @@ def test_tiny_passes_and_size_limits(integ):
     # a misaligned record buffer is refused
     rc = integ.lib.cp_unweight(integ.h, 1024, 0, C.c_void_p(recs.data_ptr() + 4), 1, C.byref(res))
     assert rc == cp._lib.CP_ERR_INVALID
+    # a production pass needs a threshold (cp_weight_quantile or cp_set_wmax); cp_set_wmax sets it
+    with cp.Integrator() as fresh:
+        rc = fresh.lib.cp_unweight(fresh.h, 1024, 0, C.c_void_p(recs.data_ptr()), 1, C.byref(res))
+        assert rc == cp._lib.CP_ERR_INVALID
+        hrec = torch.empty((1, 64), dtype=torch.uint8, pin_memory=True)
+        rc = fresh.lib.cp_generate_host(fresh.h, 1024, 0, 512, C.c_void_p(hrec.data_ptr()), 1, C.byref(res))
+        assert rc == cp._lib.CP_ERR_INVALID
+        fresh.set_wmax(1e30)   # nothing is accepted against an unreachable threshold
+        _, st0 = fresh.unweight(1024, iteration=42)
+        assert st0["n_accepted"] == 0 and st0["w_max"] == 1e30
     # the flow forward of a single point (far below one 128-point tile)
     integ.flow_init(7)
     out = integ.flow_sample(11, 1, 3, 0).cpu().numpy()
