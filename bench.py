@@ -281,6 +281,7 @@ def run_ours(a):
     n = a.points
     r0 = 1000
     si = ShardedIntegrator(it)           # adaptation: shared points, one exchange per iteration
+    it.adjoint_parameter_tangents(False)   # the gradient steps use only the edge gradients
     records = torch.empty((n, RECORD_BYTES), dtype=torch.uint8, device=f"cuda:{dev}")
 
     with torch.cuda.stream(stream):

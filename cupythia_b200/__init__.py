@@ -232,6 +232,11 @@ class Integrator:
         """Moment order of the adjoint passes: <w^p>/<w>^p instead of the variance (p = 2)."""
         self._check(self.lib.cp_vegas_gradient_objective(self.h, float(p)))
 
+    def adjoint_parameter_tangents(self, on=True):
+        """Adjoint passes with or without the alpha_s(mZ), k_ren and pT-cut tangents; without
+        them the edge gradients and grid steps are the same bit for bit and the passes faster."""
+        self._check(self.lib.cp_adjoint_parameter_tangents(self.h, 1 if on else 0))
+
     def gradient_step(self, n_points, iteration=0, lr=0.5):
         g = cp_grad()
         self._check(self.lib.cp_vegas_gradient_step(self.h, n_points, iteration, lr, C.byref(g)))

@@ -130,6 +130,7 @@ SIGNATURES = {
     "cp_vegas_gradient_step": [_P, _u64, _u32, _d, C.POINTER(cp_grad)],
     "cp_adjoint_sums_size": [_P, C.POINTER(_i)],
     "cp_vegas_gradient_objective": [_P, _d],
+    "cp_adjoint_parameter_tangents": [_P, _i],
     "cp_adjoint_accumulate": [_P, _u64, _u32, _u32, _P],
     "cp_vegas_gradient_apply": [_P, _P, _u64, _d, C.POINTER(cp_grad)],
     "cp_flow_step_moments": [_P, _u64, _u64, _P],

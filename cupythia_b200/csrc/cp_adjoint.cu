@@ -19,11 +19,9 @@
 #include "cp_dual.cuh"
 #include "cp_internal.cuh"
 
-#define CP_ADJ_N 6
 #define CP_ADJ_THREADS 128
 #define CP_ADJ_WARPS (CP_ADJ_THREADS / 32)
 #define CP_ADJ_HEAD 10   // sum w, sum w^2, sum dw[3], sum w dw[3], max w, n_bad
-typedef CpDual<CP_ADJ_N> D6;
 
 struct AdjLaunch {
   uint64_t seed, point0, n;
@@ -37,8 +35,13 @@ struct AdjLaunch {
   float pm1;                       // moment order - 1 (1: the variance)
 };
 
+// NT = 6: tangents x0, x1, x2, alpha_s(mZ), k_ren, pT_hat_min; NT = 3: the x tangents only (the
+// edge gradients and the sums of w are the same bit for bit, since tangents never mix; the
+// parameter sums stay zero)
+template <int NT>
 __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P, const AdjLaunch L)
 {
+  typedef CpDual<NT> D6;
   extern __shared__ float sDyn[];   // [warp][dim][4][nb]: lo, hi, w*lo, w*hi
   __shared__ float2 sEdge[3][CP_MAX_BINS];
   __shared__ CpCteqPoly sCteq[8];
@@ -55,13 +58,13 @@ __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P,
   __syncthreads();
 
   CpHadParamsT<D6> Q;
-  Q.lnTauMin = cp_dconst<CP_ADJ_N>(L.lnTauMin);
-  Q.lnTauMin.d[5] = L.dlnTauMin_dpt;
-  Q.kR = cp_dconst<CP_ADJ_N>(P.kR);
-  Q.kR.d[4] = 1.f;
-  for (int k = 0; k < 4; ++k) {
-    Q.lnL2[k] = cp_dconst<CP_ADJ_N>(L.lnL2[k]);
-    Q.lnL2[k].d[3] = L.dlnL2_da[k];
+  Q.lnTauMin = cp_dconst<NT>(L.lnTauMin);
+  Q.kR = cp_dconst<NT>(P.kR);
+  for (int k = 0; k < 4; ++k) Q.lnL2[k] = cp_dconst<NT>(L.lnL2[k]);
+  if constexpr (NT == 6) {
+    Q.lnTauMin.d[5] = L.dlnTauMin_dpt;
+    Q.kR.d[4] = 1.f;
+    for (int k = 0; k < 4; ++k) Q.lnL2[k].d[3] = L.dlnL2_da[k];
   }
 
   const float nbf = (float)nb;
@@ -91,17 +94,22 @@ __global__ void __launch_bounds__(CP_ADJ_THREADS) k_adjoint(const CpHadParams P,
         width[d] = e.y;
         jv *= nbf * e.y;
       }
-      D6 wb = cp_had_weight_t<D6>(P, Q, sCteq, cp_dvar<CP_ADJ_N>(x[0], 0), cp_dvar<CP_ADJ_N>(x[1], 1),
-                                  cp_dvar<CP_ADJ_N>(x[2], 2));
+      D6 wb = cp_had_weight_t<D6>(P, Q, sCteq, cp_dvar<NT>(x[0], 0), cp_dvar<NT>(x[1], 1),
+                                  cp_dvar<NT>(x[2], 2));
       w = wb.v * jv;
       bool ok = (w >= 0.f) && !isinf(w);
 #pragma unroll
-      for (int k = 0; k < CP_ADJ_N; ++k) ok = ok && isfinite(wb.d[k]);
+      for (int k = 0; k < NT; ++k) ok = ok && isfinite(wb.d[k]);
       if (!ok) {
         ++nbad;
         w = 0.f;
       } else {
-        float dth[3] = {wb.d[3] * jv, wb.d[4] * jv, wb.d[5] * jv};
+        float dth[3] = {0.f, 0.f, 0.f};
+        if constexpr (NT == 6) {
+          dth[0] = wb.d[3] * jv;
+          dth[1] = wb.d[4] * jv;
+          dth[2] = wb.d[5] * jv;
+        }
         wq = L.pm1 == 1.f ? w : powf(w, L.pm1);
         cp_kahan(acc[0], cmp[0], w);
         cp_kahan(acc[1], cmp[1], w * wq);
@@ -215,16 +223,17 @@ static int adjoint_accumulate(cp_handle* h, uint64_t n, uint32_t iter, uint32_t 
   const int nb = h->nb, width = CP_ADJ_HEAD + 12 * nb;
   const size_t dyn = sizeof(float) * CP_ADJ_WARPS * 12 * nb;
   // the attribute is per device: set it on every call (host-side, cheap)
-  CP_CUDA(h, cudaFuncSetAttribute(k_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const int full = h->adj_params ? 1 : 0;
+  const void* kfn = full ? reinterpret_cast<const void*>(k_adjoint<6>) : reinterpret_cast<const void*>(k_adjoint<3>);
+  CP_CUDA(h, cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(float) * CP_ADJ_WARPS * 12 * CP_MAX_BINS)));
-  if (h->adj_per_sm < 0) {
+  if (h->adj_per_sm_nt[full] < 0) {
     int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, CP_ADJ_THREADS, dyn) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, CP_ADJ_THREADS, dyn) != cudaSuccess || per_sm < 1)
       per_sm = 1;
-    h->adj_per_sm = per_sm;
+    h->adj_per_sm_nt[full] = per_sm;
   }
-  const int blocks = h->num_sms * h->adj_per_sm;
+  const int blocks = h->num_sms * h->adj_per_sm_nt[full];
   int rc = cp_ensure_slots(h, (size_t)blocks * width);
   if (rc) return rc;
   AdjLaunch L;
@@ -239,7 +248,8 @@ static int adjoint_accumulate(cp_handle* h, uint64_t n, uint32_t iter, uint32_t 
     L.lnL2[k] = h->P.lnL2[k];
     L.dlnL2_da[k] = (float)(12.0 * M_PI / (b0[k] * a * a));
   }
-  k_adjoint<<<blocks, CP_ADJ_THREADS, dyn, h->stream>>>(h->P, L);
+  if (full) k_adjoint<6><<<blocks, CP_ADJ_THREADS, dyn, h->stream>>>(h->P, L);
+  else k_adjoint<3><<<blocks, CP_ADJ_THREADS, dyn, h->stream>>>(h->P, L);
   CP_LAUNCH_CHECK(h, "k_adjoint");
   k_reduce_slots<0><<<(width + 7) / 8, 256, 0, h->stream>>>(h->d_slots, blocks, width, sums_out, 8);
   CP_LAUNCH_CHECK(h, "k_reduce_slots");
@@ -295,6 +305,13 @@ extern "C" int cp_vegas_gradient_objective(cp_handle* h, double p)
   CP_CHECK_HANDLE(h);
   if (!(p >= 2.0 && p <= 8.0)) return cp_fail(h, CP_ERR_INVALID, "cp_vegas_gradient_objective: p must be in [2, 8]");
   h->adj_p = p;
+  return CP_OK;
+}
+
+extern "C" int cp_adjoint_parameter_tangents(cp_handle* h, int on)
+{
+  CP_CHECK_HANDLE(h);
+  h->adj_params = on ? 1 : 0;
   return CP_OK;
 }
 

@@ -111,7 +111,7 @@ struct cp_handle {
   float* d_uH = nullptr;          // uHat, formed at the input precision (FP64 for cp_set2kin_batch_f64)
   // launch shapes (resident blocks per SM on this handle's device; -1 until first use)
   int had_blocks = 0;
-  int adj_per_sm = -1, flow_per_sm = -1, unw_per_sm = -1;
+  int adj_per_sm_nt[2] = {-1, -1}, flow_per_sm = -1, unw_per_sm = -1;   // adjoint: x tangents only / all six
   int build_per_sm[2] = {-1, -1};   // record builder without / with scale weights
   // weight histogram of the last iteration and the unweighting threshold (device)
   unsigned long long* d_qhist = nullptr;   // CP_QBINS
@@ -156,6 +156,7 @@ struct cp_handle {
   long flow_t = 0;                         // optimiser updates so far (a step's batch iteration)
   double flow_loss_p = 2.0;                // training objective <w^p>/<w>^p
   double adj_p = 2.0;                      // adjoint / variance-gradient objective: moment order
+  int adj_params = 1;                      // adjoint passes carry the parameter tangents too
   // training buffers of the current step (per-point forward state and GEMM operands for
   // ftrain_count points), kept between the phases of a data-parallel step
   void* d_ftrain = nullptr;

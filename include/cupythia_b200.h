@@ -296,6 +296,11 @@ int cp_vegas_gradient_step(cp_handle* h, uint64_t n_points, uint32_t iter, doubl
  * of the weights, which sets the unweighting efficiency at a high-quantile w_max; classic VEGAS
  * refinement (a w^2 histogram) has no such choice.  No reference counterpart. */
 int cp_vegas_gradient_objective(cp_handle* h, double p);
+/* Adjoint passes with (on != 0, default) or without the three parameter tangents (alpha_s(mZ),
+ * k_ren, pT_hat cut).  Off, the pass carries only the x tangents the grid needs: the edge
+ * gradients, sigma, Var and every variance-gradient step come out the same bit for bit, the
+ * parameter derivatives of cp_grad read zero, and the pass runs about twice as fast. */
+int cp_adjoint_parameter_tangents(cp_handle* h, int on);
 /* The same step data-parallel, with one exchange (the reference shards its passes by point range,
  * cuPythia/common/rng.cuh:5-19, and merges on the host; here the ranks sum device arrays):
  * cp_adjoint_accumulate writes the adjoint sums of this handle's points [offset, offset +

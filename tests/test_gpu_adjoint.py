@@ -250,3 +250,29 @@ def test_gradient_steps_against_classic_vegas_at_equal_points():
     assert res[4.0]["relvar"] < 1.5 * c["relvar"], res
     for k in (2.0, 4.0):
         assert abs(res[k]["sigma"] - c["sigma"]) < 5 * np.hypot(res[k]["err"], c["err"]), res
+
+
+def test_adjoint_without_parameter_tangents_keeps_edge_gradients(adapted):
+    """With the parameter tangents switched off the adjoint pass carries only x0, x1, x2: sigma,
+    Var and both edge-gradient arrays are the same bit for bit, the parameter derivatives read
+    zero, and a variance-gradient step moves the grid exactly as with all six tangents."""
+    it = adapted
+    full = it.adjoint(1 << 22, 33)
+    it.adjoint_parameter_tangents(False)
+    try:
+        xo = it.adjoint(1 << 22, 33)
+        g0 = it.grid
+        it.gradient_step(1 << 22, 34, lr=0.2)
+        grid_x = it.grid
+    finally:
+        it.adjoint_parameter_tangents(True)
+    it.grid = g0
+    it.gradient_step(1 << 22, 34, lr=0.2)
+    grid_full = it.grid
+    it.grid = g0
+    assert xo["sigma"] == full["sigma"] and xo["var"] == full["var"]
+    assert np.array_equal(xo["dsigma_dedges"], full["dsigma_dedges"])
+    assert np.array_equal(xo["dvar_dedges"], full["dvar_dedges"])
+    assert xo["dsigma"] == [0.0, 0.0, 0.0] and xo["dvar"] == [0.0, 0.0, 0.0]
+    assert any(v != 0.0 for v in full["dsigma"])
+    assert np.array_equal(grid_x, grid_full)
