@@ -13,6 +13,9 @@ struct HandoffLaunch {
   int* bad;
 };
 
+// VEC4: maxPart == 4 and every per-particle array 16-byte aligned, so an event's four entries of
+// a member are one 16-byte store (int) or two (double) instead of four scalar stores
+template <bool VEC4>
 __global__ void __launch_bounds__(CP_THREADS) k_to_device_events(const HandoffLaunch L)
 {
   const cp_device_events& ev = L.ev;
@@ -32,6 +35,30 @@ __global__ void __launch_bounds__(CP_THREADS) k_to_device_events(const HandoffLa
     const size_t b = (size_t)e * ev.maxPart;
     const double pin[2] = {(double)r.pz_in[0], (double)r.pz_in[1]};
     const float* pout[2] = {r.p3, r.p4};
+    if (VEC4) {
+      // the same values as the scalar path below, member by member
+      auto st_d = [&](double* base, double a, double bb, double c, double d) {
+        double2* q = reinterpret_cast<double2*>(base + b);
+        q[0] = make_double2(a, bb);
+        q[1] = make_double2(c, d);
+      };
+      auto st_i = [&](int* base, int a, int bb, int c, int d) { *reinterpret_cast<int4*>(base + b) = make_int4(a, bb, c, d); };
+      st_d(ev.px, 0.0, 0.0, (double)r.p3[0], (double)r.p4[0]);
+      st_d(ev.py, 0.0, 0.0, (double)r.p3[1], (double)r.p4[1]);
+      st_d(ev.pz, pin[0], pin[1], (double)r.p3[2], (double)r.p4[2]);
+      st_d(ev.e, fabs(pin[0]), fabs(pin[1]), (double)r.p3[3], (double)r.p4[3]);
+      st_d(ev.m, 0.0, 0.0, 0.0, 0.0);
+      st_i(ev.pdg, r.id[0], r.id[1], r.id[2], r.id[3]);
+      st_i(ev.status, -21, -21, 23, 23);
+      st_i(ev.col, col[0] ? 500 + col[0] : 0, col[1] ? 500 + col[1] : 0, col[2] ? 500 + col[2] : 0,
+           col[3] ? 500 + col[3] : 0);
+      st_i(ev.acol, acol[0] ? 500 + acol[0] : 0, acol[1] ? 500 + acol[1] : 0, acol[2] ? 500 + acol[2] : 0,
+           acol[3] ? 500 + acol[3] : 0);
+      st_i(ev.mo1, -1, -1, 0, 0);
+      st_i(ev.mo2, -1, -1, 1, 1);
+      st_i(ev.d1, -1, -1, -1, -1);
+      st_i(ev.d2, -1, -1, -1, -1);
+    } else {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const size_t j = b + k;
@@ -48,6 +75,7 @@ __global__ void __launch_bounds__(CP_THREADS) k_to_device_events(const HandoffLa
       ev.col[j] = col[k] ? 500 + col[k] : 0;
       ev.acol[j] = acol[k] ? 500 + acol[k] : 0;
       ev.d1[j] = -1; ev.d2[j] = -1;
+    }
     }
     ev.nPart[e] = 4;
     ev.seed[e] = cp_splitmix64(L.seed ^ ((uint64_t)r.point * 0x9E3779B97F4A7C15ULL));
@@ -92,7 +120,12 @@ extern "C" int cp_records_to_device_events(cp_handle* h, const cp_event* records
   L.bad = bad;
   const uint64_t want = (n + CP_THREADS - 1) / CP_THREADS;
   const unsigned blocks = (unsigned)(want < (uint64_t)h->num_sms * 8 ? want : (uint64_t)h->num_sms * 8);
-  k_to_device_events<<<blocks, CP_THREADS, 0, h->stream>>>(L);
+  bool vec4 = ev->maxPart == 4;
+  const void* part[] = {ev->px, ev->py, ev->pz, ev->e, ev->m, ev->pdg, ev->status, ev->col, ev->acol, ev->mo1,
+                        ev->mo2, ev->d1, ev->d2};
+  for (const void* p : part) vec4 = vec4 && ((uintptr_t)p & 15) == 0;
+  if (vec4) k_to_device_events<true><<<blocks, CP_THREADS, 0, h->stream>>>(L);
+  else k_to_device_events<false><<<blocks, CP_THREADS, 0, h->stream>>>(L);
   cudaError_t e = cudaGetLastError();
   int hb = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream);

@@ -9,9 +9,16 @@
 // AQCDUP and one line per parton (IDUP ISTUP MOTHUP1 MOTHUP2 ICOLUP1 ICOLUP2 PUP1..5 VTIMUP
 // SPINUP).  Unlike the reference (one process, a fixed gg -> gg colour ring) every record
 // carries its own process code and the colour flow its setIdColAcol chose.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+#if defined(__linux__)
+#include <sched.h>
+#endif
 #include "cp_internal.cuh"
 
 extern "C" int cp_colour_tags(uint16_t process, uint16_t colour, int col[4], int acol[4])
@@ -54,6 +61,57 @@ extern "C" int cp_set_id_col_acol(int code, int id1, int id2, double t_over_s, d
 // LHEF tag of a colour index (0 = none)
 static inline int lhef_tag(int c) { return c ? 500 + c : 0; }
 
+// The <event> blocks of events [a, b) appended to out; false if a record's process code or
+// colour flow is invalid.
+static bool lhef_events(const cp_config* cfg, const CpHadParams& P, const cp_event* events, uint64_t a, uint64_t b,
+                        std::string& out)
+{
+  char line[512];
+  out.clear();
+  out.reserve((size_t)(b - a) * 560);
+  auto put = [&](int len) {
+    if (len > 0) out.append(line, (size_t)(len < (int)sizeof line ? len : (int)sizeof line - 1));
+  };
+  for (uint64_t i = a; i < b; ++i) {
+    const cp_event& e = events[i];
+    int col[4], acol[4];
+    if (cp_colour_tags(e.process, e.colour, col, acol) != CP_OK) return false;
+    const double pT2 = (double)e.pt_hat * e.pt_hat;
+    const double scale = sqrt(pT2 * cfg->k_fac);
+    const double aS = cp_alphas(P, (float)(pT2 * cfg->k_ren));
+    out.append("<event>\n");
+    // NUP IDPRUP XWGTUP SCALUP AQEDUP AQCDUP
+    put(snprintf(line, sizeof line, "4 %d %.8E %.8E 7.8175100E-03 %.8E\n", (int)e.process, (double)e.weight, scale, aS));
+    // IDUP ISTUP MOTHUP1 MOTHUP2 ICOLUP1 ICOLUP2 PX PY PZ E M VTIMUP SPINUP
+    for (int k = 0; k < 2; ++k)
+      put(snprintf(line, sizeof line,
+                   "%d -1 0 0 %d %d 0.0000000000E+00 0.0000000000E+00 %.10E %.10E 0.0000000000E+00 0. 9.\n",
+                   (int)e.id[k], lhef_tag(col[k]), lhef_tag(acol[k]), (double)e.pz_in[k], fabs((double)e.pz_in[k])));
+    const float* p[2] = {e.p3, e.p4};
+    for (int k = 0; k < 2; ++k)
+      put(snprintf(line, sizeof line, "%d 1 1 2 %d %d %.10E %.10E %.10E %.10E 0.0000000000E+00 0. 9.\n",
+                   (int)e.id[2 + k], lhef_tag(col[2 + k]), lhef_tag(acol[2 + k]), (double)p[k][0], (double)p[k][1],
+                   (double)p[k][2], (double)p[k][3]));
+    out.append("</event>\n");
+  }
+  return true;
+}
+
+// host threads this process may run on (its CPU affinity), at most 64
+static int lhef_threads()
+{
+#if defined(__linux__)
+  cpu_set_t set;
+  CPU_ZERO(&set);
+  if (sched_getaffinity(0, sizeof set, &set) == 0) {
+    const int c = CPU_COUNT(&set);
+    if (c > 0) return c < 64 ? c : 64;
+  }
+#endif
+  const unsigned c = std::thread::hardware_concurrency();
+  return c ? (c < 64 ? (int)c : 64) : 1;
+}
+
 extern "C" int cp_write_lhef(const cp_config* cfg, const cp_event* events, uint64_t n, double sigma_mb,
                              double sigma_err_mb, const char* path)
 {
@@ -95,26 +153,26 @@ extern "C" int cp_write_lhef(const cp_config* cfg, const cp_event* events, uint6
     fprintf(f, "%.10E %.10E %.10E %d\n", xs, xe, wmax, 111 + k);
   }
   fprintf(f, "</init>\n");
-  for (uint64_t i = 0; i < n; ++i) {
-    const cp_event& e = events[i];
-    int col[4], acol[4];
-    if (cp_colour_tags(e.process, e.colour, col, acol) != CP_OK) { fclose(f); return CP_ERR_INVALID; }
-    const double pT2 = (double)e.pt_hat * e.pt_hat;
-    const double scale = sqrt(pT2 * cfg->k_fac);
-    const double aS = cp_alphas(P, (float)(pT2 * cfg->k_ren));
-    fprintf(f, "<event>\n");
-    // NUP IDPRUP XWGTUP SCALUP AQEDUP AQCDUP
-    fprintf(f, "4 %d %.8E %.8E 7.8175100E-03 %.8E\n", (int)e.process, (double)e.weight, scale, aS);
-    // IDUP ISTUP MOTHUP1 MOTHUP2 ICOLUP1 ICOLUP2 PX PY PZ E M VTIMUP SPINUP
-    for (int k = 0; k < 2; ++k)
-      fprintf(f, "%d -1 0 0 %d %d 0.0000000000E+00 0.0000000000E+00 %.10E %.10E 0.0000000000E+00 0. 9.\n",
-              (int)e.id[k], lhef_tag(col[k]), lhef_tag(acol[k]), (double)e.pz_in[k], fabs((double)e.pz_in[k]));
-    const float* p[2] = {e.p3, e.p4};
-    for (int k = 0; k < 2; ++k)
-      fprintf(f, "%d 1 1 2 %d %d %.10E %.10E %.10E %.10E 0.0000000000E+00 0. 9.\n", (int)e.id[2 + k],
-              lhef_tag(col[2 + k]), lhef_tag(acol[2 + k]), (double)p[k][0], (double)p[k][1], (double)p[k][2],
-              (double)p[k][3]);
-    fprintf(f, "</event>\n");
+  // the <event> blocks: host threads format chunks of 8192 events each into their own buffer,
+  // the calling thread writes the buffers in event order (the same bytes as one thread writing)
+  const uint64_t chunk = 8192;
+  const int nt = n > chunk ? lhef_threads() : 1;
+  std::vector<std::string> bufs((size_t)nt);
+  for (uint64_t base = 0; base < n; base += chunk * (uint64_t)nt) {
+    std::atomic<int> bad{0};
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) {
+      const uint64_t a = base + (uint64_t)t * chunk;
+      if (a >= n) break;
+      const uint64_t b = a + chunk < n ? a + chunk : n;
+      th.emplace_back([&, t, a, b] {
+        if (!lhef_events(cfg, P, events, a, b, bufs[(size_t)t])) bad = 1;
+      });
+    }
+    if (!lhef_events(cfg, P, events, base, base + chunk < n ? base + chunk : n, bufs[0])) bad = 1;
+    for (std::thread& x : th) x.join();
+    if (bad) { fclose(f); return CP_ERR_INVALID; }
+    for (int t = 0; t <= (int)th.size(); ++t) fwrite(bufs[(size_t)t].data(), 1, bufs[(size_t)t].size(), f);
   }
   fprintf(f, "</LesHouchesEvents>\n");
   const int bad = ferror(f);
