@@ -49,7 +49,10 @@
 // the nine polynomials of a parametrisation, in the order of CpCteqPoly::co
 enum { CP_CQ_A, CP_CQ_B, CP_CQ_AF1, CP_CQ_AF2, CP_CQ_P, CP_CQ_AF5, CP_CQ_AF6, CP_CQ_AF7, CP_CQ_AF8, CP_CQ_N };
 
-// 160 bytes, 16-byte aligned: the kernels read one record as ten 128-bit shared-memory loads
+// 160 bytes, 16-byte aligned.  The production, VEGAS and record-builder kernels read the records
+// from their own parameters (CpHadParams::cteq, constant memory, __grid_constant__): 2.6% faster
+// accept kernel than ten 128-bit shared-memory loads per record and point.  Kernels with a
+// staged copy read it as 128-bit shared-memory loads.
 struct alignas(16) CpCteqPoly {
   // per parametrisation i: co[k][f] = coefficient of sb1^k in polynomial f (CP_CQ_*), sb1 =
   // ln ln(Q/alpha_i) - 1.2.  The pairs (A, B), (af1, af2), (p, af5), (af6, af7) sit side by side
@@ -215,7 +218,10 @@ CP_HD float cp_from_bits(int i)
 //   exact and the last FMA rounds once.
 // k comes from the FMA a log2(e) + 1.5 * 2^23, which rounds the exact product to an integer kept
 // in the low mantissa bits; shifting those bits left by 23 places k in the exponent field.  For a
-// in [-80, 80] (clamped there) every 2^k is a normal float.  Near a = 0 (k = 0) e^a - 1 is the
+// in [-87, 87] every 2^k is a normal float; the callers' arguments lie well inside: CTEQ5L's
+// p ln y in [-32.1, 3.7] (p in [-0.03, 1.40] over its table for Q >= 1, ln y in [-23.1, 2.7]),
+// ln x in [ln 1e-6, 0], and x0 ln tauMin in [ln tauMin, 0] with ln tauMin > -80, which
+// cp_build_had_params checks.  Near a = 0 (k = 0) e^a - 1 is the
 // polynomial alone, accurate relative to itself; elsewhere both results are within about 2 ulp
 // (measured over 2e7 arguments against FP64: 2.0 ulp relative for |a| < ln 2 / 2, 1.9 ulp of
 // max(|e^a - 1|, 1) elsewhere; CUDA's and libm's expm1f 1.3 and 1.4).  Every operation is a
@@ -227,8 +233,6 @@ CP_HD void cp_exp_reduce2(CpF2 a, CpF2& s, CpF2& q)
   const float LN2_HI = 0.693145751953125f;          // ln 2 to 16 significant bits
   const float LN2_LO = 1.42860682030941723e-6f;     // ln 2 - LN2_HI
   const float RND = 12582912.f;                     // 1.5 * 2^23
-  a.x = fminf(fmaxf(a.x, -80.f), 80.f);
-  a.y = fminf(fmaxf(a.y, -80.f), 80.f);
   const CpF2 kf = cp_fma2(a, cp_f2s(LOG2E), cp_f2s(RND));
   const CpF2 k = cp_sub2(kf, cp_f2s(RND));
   CpF2 r = cp_fma2(k, cp_f2s(-LN2_HI), a);
@@ -368,7 +372,8 @@ CP_HD CpF2 cp_cteq_answer2(const CpCteqPoly& c, const CpCteqQ& a, const CpBeamX&
   return cp_mul2(cp_mul2(x, cp_fma2(ex, el, ex)), cp_f2s(a.qfac));
 }
 
-// one coefficient record in 128-bit loads (on the device; a plain copy on the host)
+// one coefficient record in 128-bit loads (on the device, from constant or shared memory; a
+// plain copy on the host)
 CP_HD CpCteqPoly cp_load_poly(const CpCteqPoly* p)
 {
 #if defined(__CUDA_ARCH__)
@@ -384,8 +389,8 @@ CP_HD CpCteqPoly cp_load_poly(const CpCteqPoly* p)
 }
 
 // CTEQ5L of a proton for both beams at one factorisation scale (PDF::xf + CTEQ5L::xfUpdate):
-// fa, fb = {xd, xu, xg, xubar, xdbar, xs, xc, xb}, from the coefficient records `cteq` (staged
-// in shared memory by the kernels).  UNROLL = 8 unrolls the 8 parametrisations, so the per-i
+// fa, fb = {xd, xu, xg, xubar, xdbar, xs, xc, xb}, from the coefficient records `cteq` (the
+// kernel's parameters or a shared-memory copy).  UNROLL = 8 unrolls the 8 parametrisations, so the per-i
 // structure (the ln(1 - x) and Qmin cases, the dbar/ubar ratio, which register a result lands in)
 // is resolved at compile time: about 8% fewer cycles in the integrand kernels than the rolled
 // loop.  UNROLL = 1 keeps the rolled loop where code size or registers matter more (the second

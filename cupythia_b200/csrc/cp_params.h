@@ -111,6 +111,7 @@ static inline int cp_build_had_params(const CpHadConfig& c, CpHadParams& P)
   double s = c.sqrtS * c.sqrtS;
   double tauMin = 4.0 * c.pTmin * c.pTmin / s;
   double lnTauMin = log(tauMin);
+  if (!(lnTauMin > -80.0)) return 1;   // the range of the kernels' exp reduction (cp_exp_reduce2)
   P.lnTauMin = (float)lnTauMin;
   P.lnTauMinLo = (float)(lnTauMin - (double)P.lnTauMin);
   P.K0 = (float)(2.0 * M_PI * c.convert2mb * (-lnTauMin) / s);

@@ -76,14 +76,13 @@ __device__ __forceinline__ void cp_stage_edges(float2 (*sEdge)[CP_MAX_BINS], con
 // K1: weight, accept; per 32-point block the accept mask (its popcount added to its range's
 // total), and each accepted point's event weight, coordinates and PDFs packed at the front of the
 // block's staging slots in point order; K2 builds the record from them.
-__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const CpHadParams P, const UnwLaunch L)
+__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const __grid_constant__ CpHadParams P,
+                                                                           const __grid_constant__ UnwLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
-  __shared__ CpCteqPoly sCteq[8];
   __shared__ double sRed[CP_WARPS][7];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   cp_stage_edges(sEdge, L.edges, L.nb);
-  cp_stage_cteq(sCteq, L.cteq);
   __syncthreads();
   const float wmax = (float)L.wmax[0];
   const uint64_t stride = (uint64_t)gridDim.x * CP_THREADS;
@@ -99,7 +98,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
       cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
       m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
     }
-    cp_unw_point(P, sCteq, L, wmax, p, m.x[0], m.x[1], m.x[2], m.jv, cp_u24(wd[3]), S);
+    cp_unw_point(P, P.cteq, L, wmax, p, m.x[0], m.x[1], m.x[2], m.jv, cp_u24(wd[3]), S);
   }
   double v[7];
   cp_unw_warp_sums(S, v);
@@ -164,11 +163,9 @@ __global__ void __launch_bounds__(1024) k_unw_scan(const unsigned* __restrict__ 
 // at its output index.
 // 4 resident blocks per SM without scale weights (64 registers), 2 with them
 template <bool SCALEW>
-__global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const CpHadParams P, const UnwLaunch L)
+__global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const __grid_constant__ CpHadParams P,
+                                                                          const __grid_constant__ UnwLaunch L)
 {
-  __shared__ CpCteqPoly sCteq[8];
-  cp_stage_cteq(sCteq, L.cteq);
-  __syncthreads();
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = (uint64_t)gridDim.x * (CP_THREADS / 32);
   for (uint64_t U = ((uint64_t)blockIdx.x * CP_THREADS + threadIdx.x) >> 5; U < 4 * L.nrange; U += nwarps) {
@@ -219,13 +216,13 @@ __global__ void __launch_bounds__(CP_THREADS, SCALEW ? 2 : 4) k_unw_build(const 
         pdf[4 * f] = v.x; pdf[4 * f + 1] = v.y; pdf[4 * f + 2] = v.z; pdf[4 * f + 3] = v.w;
       }
       CpPoint pt;
-      cp_had_eval(P, sCteq, __uint_as_float(tail.y), __uint_as_float(tail.z), __uint_as_float(tail.w), pt, pdf);
+      cp_had_eval(P, P.cteq, __uint_as_float(tail.y), __uint_as_float(tail.z), __uint_as_float(tail.w), pt, pdf);
       CpEventRec ev;
       cp_make_event(P, pt, cp_u24(w2[0]), cp_u24(w2[1]), cp_u24(w2[2]), cp_u24(w2[3]), cp_colour_rc(w2),
                     cp_colour_rs(w2), __uint_as_float(tail.x), (uint32_t)point, ev);
       if (SCALEW) {
         float r[6];
-        cp_scale_ratios(P, sCteq, pt, r);
+        cp_scale_ratios(P, P.cteq, pt, r);
         float2* sw = reinterpret_cast<float2*>(L.scalew + 6 * k);
         sw[0] = make_float2(r[0], r[1]);
         sw[1] = make_float2(r[2], r[3]);

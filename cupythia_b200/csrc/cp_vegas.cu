@@ -18,7 +18,6 @@ struct HadLaunch {
   uint32_t iter, stream;
   int nb;
   const double* edges;
-  const CpCteqPoly* cteq;
   double* slots;   // gridDim.x * (CP_SLOT_HEAD + 3 nb)
   float* w_out;    // optional per-point weights
   float* x_out;    // optional per-point mapped x (3 per point)
@@ -27,15 +26,14 @@ struct HadLaunch {
 };
 
 template <bool WRITE>
-__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const CpHadParams P, const HadLaunch L)
+__global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const __grid_constant__ CpHadParams P,
+                                                                          const __grid_constant__ HadLaunch L)
 {
   __shared__ float2 sEdge[3][CP_MAX_BINS];
   __shared__ float sHist[CP_WARPS][3][CP_MAX_BINS];
   __shared__ float sRed[CP_WARPS][6];
   __shared__ unsigned sQ[CP_QBINS];
-  __shared__ CpCteqPoly sCteq[8];
   const int nb = L.nb;
-  cp_stage_cteq(sCteq, L.cteq);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int k = threadIdx.x; k < 3 * nb; k += CP_THREADS) {
     int d = k / nb, b = k - d * nb;
@@ -82,7 +80,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_had_accum(const C
           jv *= nbf * e.y;
         }
       }
-      w = cp_had_weight(P, sCteq, x[0], x[1], x[2], nullptr) * jv;
+      w = cp_had_weight(P, P.cteq, x[0], x[1], x[2], nullptr) * jv;
       if (!(w >= 0.f) || isinf(w)) { ++nbad; w = 0.f; }
       cp_kahan(s1, c1, w);
       cp_kahan(s2, c2, w * w);
@@ -235,7 +233,6 @@ static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, 
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.stream = stream;
   L.nb = h->nb; L.edges = h->d_edges; L.slots = h->d_slots; L.w_out = w_out; L.x_out = x_out;
   L.qhist = h->d_qhist;
-  L.cteq = h->d_cteq;
   L.flow = nullptr;
   if (h->flow_on) {
     rc = cp_flow_buffer(h, n);
@@ -458,36 +455,29 @@ extern "C" int cp_weight_quantile_hist(cp_handle* h, const unsigned long long* h
 // would break), a process held to a fixed device-memory budget, or a plugin such as a Pythia
 // SigmaProcess running inside someone else's event loop, which cannot create and keep a handle
 // with its own buffers.  This entry point creates no handle and calls no cudaMalloc / cudaFree:
-// its scratch (the per-block partial sums, the weight histogram and the CTEQ5L coefficient
-// records) lives in the file-scope array below, which every GPU that loads this library keeps
+// its scratch (the per-block partial sums and the weight histogram; the CTEQ5L coefficient
+// records travel in the kernel's parameters) lives in the file-scope array below, which every GPU that loads this library keeps
 // until the process exits.  The first call on a device looks up the array's address and the
 // launch shape (later calls only re-check the address); make that first call before any stream
 // capture.
 //
 // Limits: the partial sums hold at most CP_NOALLOC_MAX_BLOCKS blocks of CP_SLOT_HEAD + 3 *
 // CP_MAX_BINS doubles, so n_bins above CP_MAX_BINS is rejected; the grid is capped at
-// CP_NOALLOC_MAX_BLOCKS blocks (296 are used on a B200).  Total: 1,623,296 bytes per device.
-// Every call shares the array and it keeps the last call's contents; each call rewrites the
-// coefficient records, clears the weight histogram and rewrites every partial-sum slot it
-// reads.  Calls that overlap on the GPU (different streams, or several host threads) race on the
+// CP_NOALLOC_MAX_BLOCKS blocks (296 are used on a B200).  Total: 1,622,016 bytes per device.
+// Every call shares the array and it keeps the last call's contents; each call clears the
+// weight histogram and rewrites every partial-sum slot it reads.  Calls that overlap on the GPU (different streams, or several host threads) race on the
 // array and must not be issued; calls in one stream are ordered and safe.
 // ------------------------------------------------------------------------------------------
 #define CP_NOALLOC_MAX_BLOCKS 512
 #define CP_NOALLOC_SLOT_DOUBLES (CP_NOALLOC_MAX_BLOCKS * (CP_SLOT_HEAD + 3 * CP_MAX_BINS))
-#define CP_NOALLOC_CTEQ_DOUBLES 160   // 8 CpCteqPoly records (1280 bytes)
-#define CP_NOALLOC_DOUBLES (CP_NOALLOC_CTEQ_DOUBLES + CP_QBINS + CP_NOALLOC_SLOT_DOUBLES)
+#define CP_NOALLOC_DOUBLES (CP_QBINS + CP_NOALLOC_SLOT_DOUBLES)
 
 static __device__ __align__(256) double cp_noalloc_scratch[CP_NOALLOC_DOUBLES];
-static_assert(sizeof(CpCteqPoly) * 8 <= CP_NOALLOC_CTEQ_DOUBLES * sizeof(double), "CTEQ records fit");
 
-// Per-call set-up of the shared array, on the caller's stream: the CTEQ5L coefficient records
-// (taken from the kernel parameters, so no host copy is involved) and a cleared weight histogram.
-__global__ void k_noalloc_setup(const CpHadParams P, double* base)
+// Per-call set-up of the shared array, on the caller's stream: a cleared weight histogram.
+__global__ void k_noalloc_setup(double* base)
 {
-  uint32_t* cteq = reinterpret_cast<uint32_t*>(base);
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(P.cteq);
-  for (int k = threadIdx.x; k < (int)(8 * sizeof(CpCteqPoly) / 4); k += blockDim.x) cteq[k] = src[k];
-  unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base + CP_NOALLOC_CTEQ_DOUBLES);
+  unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base);
   for (int k = threadIdx.x; k < CP_QBINS; k += blockDim.x) qhist[k] = 0ull;
 }
 
@@ -542,16 +532,16 @@ extern "C" int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, ui
   }
   if (rc == CP_OK) {
     double* base = D.scratch;
-    unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base + CP_NOALLOC_CTEQ_DOUBLES);
-    double* slots = base + CP_NOALLOC_CTEQ_DOUBLES + CP_QBINS;
+    unsigned long long* qhist = reinterpret_cast<unsigned long long*>(base);
+    double* slots = base + CP_QBINS;
     int nb = cfg->n_bins, width = CP_SLOT_HEAD + 3 * nb, max_col = 2;
     HadLaunch L;
     L.seed = cfg->seed; L.point0 = 0; L.n = n_points; L.iter = iter; L.stream = 0;
-    L.nb = nb; L.edges = edges_dev; L.cteq = reinterpret_cast<const CpCteqPoly*>(base);
+    L.nb = nb; L.edges = edges_dev;
     L.slots = slots; L.w_out = nullptr; L.x_out = nullptr; L.qhist = qhist; L.flow = nullptr;
     // Each launch's own return code is checked; an error the caller left pending from earlier,
     // unrelated work is neither reported as this call's nor cleared.
-    void* a_setup[] = {&P, &base};
+    void* a_setup[] = {&base};
     void* a_accum[] = {&P, &L};
     void* a_reduce[] = {&slots, &D.blocks, &width, &sums_dev, &max_col};
     if (cudaLaunchKernel((const void*)k_noalloc_setup, dim3(1), dim3(256), a_setup, 0, stream) != cudaSuccess ||

@@ -212,14 +212,15 @@ int cp_last_histogram(cp_handle* h, double* out_host);
  * owns every device allocation (a caching allocator or pool whose accounting an allocation
  * behind its back would break), a process held to a fixed device-memory budget, or a plugin (a
  * Pythia SigmaProcess) running inside another program's event loop without a handle of its own.
- * No handle is created; the scratch (block partial sums for up to 512 blocks, the weight
- * histogram, the CTEQ5L records: 1,623,296 bytes) is a file-scope device array that every GPU
+ * No handle is created; the scratch (block partial sums for up to 512 blocks and the weight
+ * histogram: 1,622,016 bytes) is a file-scope device array that every GPU
  * loading this library keeps until exit.
  * Inputs: cfg (host), the grid edges_dev (3 x (n_bins + 1) doubles).  Output: sums_dev (4 + 3
  * n_bins doubles, the layout of cp_last_histogram).  n_bins > CP_MAX_BINS is rejected
  * (CP_ERR_INVALID).  The first call on a device looks up the array's device address and the
  * launch shape and should come before any stream capture; later calls re-check the address.
- * Each call rewrites the coefficient records and clears the weight histogram on the stream; the
+ * Each call clears the weight histogram on the stream (the CTEQ5L records travel in the kernel's
+ * parameters); the
  * array keeps the last call's contents, and calls that overlap on the GPU race on it. */
 int cp_vegas_pass_noalloc(const cp_config* cfg, uint64_t n_points, uint32_t iter,
                           const double* edges_dev, double* sums_dev, void* cuda_stream);
