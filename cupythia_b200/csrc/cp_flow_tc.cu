@@ -10,8 +10,8 @@
 // accept step of the production pass (the code of k_unw_accept, shared through cp_unweight.cuh),
 // so no flow output is stored.  Its records equal the two-kernel path's byte for byte, but it is
 // the slower of the two: a warpgroup's slots idle while its warps run the integrand, and the
-// integrand's FMA-bound warps lengthen every flow step (2^27 points on B200: 21.5 ms with 4
-// warpgroups at 96 registers, against 10.4 + 8.9 ms for the two kernels).
+// integrand's FMA-bound warps lengthen every flow step (2^27 points on B200: 19.3 ms with 4
+// warpgroups at 96 registers, against 10.4 + 7.5 ms for the two kernels).
 //
 // Launch: one persistent CTA per SM (the shared-memory footprint admits one): 4 epilogue
 // warpgroups of 128 threads and 4 issuing warps, one per warpgroup.  Each warpgroup owns two
@@ -68,10 +68,9 @@ struct CpTcLayout {
   static constexpr int EDGE = H + NWG * 2 * CP_TC_HBYTES;
   static constexpr int MISC = EDGE + 3 * CP_MAX_BINS * 8;  // mbarriers, TMEM address, abort flags, final barriers
   static constexpr int B3 = MISC + 256;                    // FP32 layer-3 biases, 8 per coupling
-  static constexpr int CTEQ = B3 + 128;                    // production form: CTEQ5L coefficient records
-  static constexpr int RED = CTEQ + 8 * (int)sizeof(CpCteqPoly);   // production form: per-warp sums
+  static constexpr int RED = B3 + 128;                     // production form: per-warp sums
   static constexpr int SMEM = RED + NWG * 4 * 7 * 8 + 1024;        // + 1024-byte base alignment slack
-  static_assert(H % 1024 == 0 && CTEQ % 16 == 0, "activation buffers and records must stay aligned");
+  static_assert(H % 1024 == 0 && RED % 16 == 0, "activation buffers and sums must stay aligned");
   static_assert(SMEM < (1 << 18), "descriptor offsets are added to the 14-bit address field");
   static_assert(SMEM <= 227 * 1024, "shared memory budget");
   static_assert(NWG <= 4 && 2 * NWG * 64 <= CP_TC_TMEM_COLS, "barrier area and TMEM columns");
@@ -302,12 +301,7 @@ __device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g,
     const double lo = edges[d * (nb + 1) + b], hi = edges[d * (nb + 1) + b + 1];
     sEdge[d * CP_MAX_BINS + b] = make_float2((float)lo, (float)(hi - lo));
   }
-  CpCteqPoly* sCteq = reinterpret_cast<CpCteqPoly*>(sm + Lay::CTEQ);
   double* sRed = reinterpret_cast<double*>(sm + Lay::RED);   // [4 NWG warps][7]
-  if constexpr (ACCEPT) {
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(L->cteq);
-    for (int e = tid; e < (int)(8 * sizeof(CpCteqPoly) / 4); e += Lay::THREADS) reinterpret_cast<uint32_t*>(sCteq)[e] = src[e];
-  }
   if (tid < NWG) abort_flags[tid] = 0;
   if (tid == 0) {
     for (int i = 0; i < 2 * NWG; ++i) {
@@ -502,7 +496,7 @@ __device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g,
 #pragma unroll 1
         for (int s = 0; s < 2; ++s) {
           const float4 f = s ? fin1 : fin0;
-          cp_unw_point(*P, sCteq, *L, wmax, s ? fp1 : fp0, f.x, f.y, f.z, expf(f.w), s ? fu1 : fu0, S);
+          cp_unw_point(*P, P->cteq, *L, wmax, s ? fp1 : fp0, f.x, f.y, f.z, expf(f.w), s ? fu1 : fu0, S);
         }
       }
       if (cp_bar_wg_or(bar_id, *abort != 0)) break;
