@@ -182,12 +182,12 @@ ALG_MUFU_OPS_PER_POINT = 72
 # k_unw_accept, executed: FADD + FMUL + 2 FFMA lane operations per point from the ncu per-opcode
 # counters of a flow-form launch (profiles/k_unw_accept_production_2e24.md; packed two-lane
 # forms counted per lane), i.e. the algorithm plus the FP32 precision bookkeeping (FMA residuals,
-# (hi, lo) logarithms) and the library transcendentals' own arithmetic
-EXEC_FLOP_PER_POINT = 1816.0
+# (hi, lo) logarithms) and the transcendentals' own arithmetic (the exp reduction's polynomial)
+EXEC_FLOP_PER_POINT = 1866.7
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
 # launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points
-TRAFFIC_PER_POINT = {"k_unw_accept": (276453376 + 686571776) / 2 ** 24,
+TRAFFIC_PER_POINT = {"k_unw_accept": (276270336 + 686841600) / 2 ** 24,
                      "k_flow_fwd_tc": (366592 + 209136896) / 2 ** 24}
 
 
