@@ -222,9 +222,10 @@ CP_HD float cp_from_bits(int i)
 // p ln y in [-32.1, 3.7] (p in [-0.03, 1.40] over its table for Q >= 1, ln y in [-23.1, 2.7]),
 // ln x in [ln 1e-6, 0], and x0 ln tauMin in [ln tauMin, 0] with ln tauMin > -80, which
 // cp_build_had_params checks.  Near a = 0 (k = 0) e^a - 1 is the
-// polynomial alone, accurate relative to itself; elsewhere both results are within about 2 ulp
-// (measured over 2e7 arguments against FP64: 2.0 ulp relative for |a| < ln 2 / 2, 1.9 ulp of
-// max(|e^a - 1|, 1) elsewhere; CUDA's and libm's expm1f 1.3 and 1.4).  Every operation is a
+// polynomial alone, accurate relative to itself; elsewhere both results are within about 2 u
+// (u = 2^-24; measured over 2e7 arguments against FP64: 2.0 u relative for |a| < ln 2 / 2, 1.9 u of
+// max(|e^a - 1|, 1) elsewhere; libm's expm1f 1.3 and 1.4; tests/test_fp32_formulation.py holds
+// it to 2.5 u over the callers' argument ranges).  Every operation is a
 // two-lane FP32 operation (FFMA2 / FMUL2 / FADD2 on the device), rounded per lane as the scalar
 // one, so the host build gives the device's result bit for bit.
 CP_HD void cp_exp_reduce2(CpF2 a, CpF2& s, CpF2& q)

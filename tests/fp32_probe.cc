@@ -49,4 +49,16 @@ void probe_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k
 {
   cp_philox(c0, c1, c2, c3, k0, k1, out);
 }
+// the integrand's two-lane exp reduction: e^a and e^a - 1 of n arguments (pairs of lanes)
+void probe_exp_reduce(const float* a, int n, float* e, float* em1)
+{
+  for (int i = 0; i < n; i += 2) {
+    const float a1 = i + 1 < n ? a[i + 1] : 0.f;
+    CpF2 s, q;
+    cp_exp_reduce2(cp_f2(a[i], a1), s, q);
+    const CpF2 ex = cp_fma2(s, q, s), m1 = cp_expm1_2(cp_f2(a[i], a1));
+    e[i] = ex.x; em1[i] = m1.x;
+    if (i + 1 < n) { e[i + 1] = ex.y; em1[i + 1] = m1.y; }
+  }
+}
 }

@@ -81,3 +81,27 @@ def test_dual_number_gradients_match_complex_step(probe, orc):
         err = np.abs(got[1:] - ref[1:]) / (np.abs(ref[1:]) + 1e-3 * scale)
         worst = max(worst, err.max())
     assert worst < 2e-3, worst
+
+
+@pytest.mark.parametrize("lo,hi", [(-32.1, 3.7), (-13.9, 0.0), (-80.0, 0.0), (-0.35, 0.35)])
+def test_exp_reduction_within_its_bound(probe, lo, hi):
+    """cp_exp_reduce2 (e^a = 2^k e^r, Taylor e^r - 1 to r^7) over the argument ranges its callers
+    pass (CTEQ5L's p ln y, the beams' ln x, x0 ln tauMin, and the k = 0 band around zero) against
+    FP64, in units u = 2^-24: e^a within 2.5 u relative, e^a - 1 within 2.5 u of max(|e^a - 1|, 1)
+    and, for |a| < ln 2 / 2, within 2.5 u relative."""
+    rng = np.random.default_rng(3)
+    a = rng.uniform(lo, hi, 400000).astype(np.float32)
+    a[:4] = np.array([lo, hi, 0.0, -1e-30], np.float32)
+    e = np.zeros_like(a)
+    m = np.zeros_like(a)
+    fp = C.POINTER(C.c_float)
+    probe.probe_exp_reduce(a.ctypes.data_as(fp), len(a), e.ctypes.data_as(fp), m.ctypes.data_as(fp))
+    ad = a.astype(np.float64)
+    ulp = 2.0 ** -24
+    ref_e, ref_m = np.exp(ad), np.expm1(ad)
+    assert np.max(np.abs(e - ref_e) / ref_e) < 2.5 * ulp
+    assert np.max(np.abs(m - ref_m) / np.maximum(np.abs(ref_m), 1.0)) < 2.5 * ulp
+    small = (np.abs(ad) < 0.3465) & (ad != 0)
+    if small.any():
+        assert np.max(np.abs(m[small] - ref_m[small]) / np.abs(ref_m[small])) < 2.5 * ulp
+    assert m[2] == 0.0 and m[3] == np.float32(-1e-30)
