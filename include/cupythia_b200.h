@@ -182,7 +182,7 @@ int cp_vegas_iteration(cp_handle* h, uint64_t n_points, uint32_t iter, double al
 int cp_integrate(cp_handle* h, int n_iter, uint64_t n_points, double alpha, int skip,
                  cp_result* per_iter_host, cp_result* combined_host);
 /* Multi-GPU iteration (one process per GPU, contiguous point shards via cp_set_point_offset;
- * the exchange of the survey's multi-GPU plan): cp_vegas_accumulate runs this handle's pass over
+ * the only exchange of a VEGAS iteration across ranks): cp_vegas_accumulate runs this handle's pass over
  * n_points points and writes its CP_SLOT_HEAD + 3 n_bins sums (dev) -- sum w, sum w^2, max w,
  * n_bad, then the per-bin sums of w^2 of each dimension; the caller reduces them over ranks
  * (sum, max for entry 2) and every rank refines identically with cp_vegas_refine_sums
