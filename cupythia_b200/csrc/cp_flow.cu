@@ -151,16 +151,20 @@ int cp_flow_buffer(cp_handle* h, uint64_t n)
     CP_CUDA(h, cudaStreamSynchronize(h->stream));
     CP_CUDA(h, cudaFree(h->d_flow_buf));
     h->d_flow_buf = nullptr;
+    h->d_flow_u = nullptr;
   }
-  CP_CUDA(h, cudaMalloc(&h->d_flow_buf, sizeof(float4) * n));
+  // the points' (v, ln J), then their accept draws
+  CP_CUDA(h, cudaMalloc(&h->d_flow_buf, (sizeof(float4) + sizeof(float)) * n));
+  h->d_flow_u = reinterpret_cast<float*>(h->d_flow_buf + n);
   h->flow_buf_cap = n;
   return CP_OK;
 }
 
 // Enqueues the flow forward for points [point0, point0 + n) into out (no synchronisation).
-int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out)
+int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out,
+                            float* uout)
 {
-  if (h->flow_kernel == 0) return cp_flow_tc_enqueue(h, point0, n, iter, stream, out);
+  if (h->flow_kernel == 0) return cp_flow_tc_enqueue(h, point0, n, iter, stream, out, uout);
   if (h->flow_per_sm < 0) {
     int per_sm = 1;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flow_fwd, CP_THREADS, flow_fwd_smem()) != cudaSuccess ||
@@ -258,7 +262,7 @@ extern "C" int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_
   if (!h->d_flow) return cp_fail(h, CP_ERR_INVALID, "flow not initialised (cp_flow_init)");
   if (n && (!out_dev || ((uintptr_t)out_dev & 15))) return cp_fail(h, CP_ERR_INVALID, "cp_flow_sample: output must be 16-byte aligned");
   if (!n) return CP_OK;
-  int rc = cp_flow_forward_enqueue(h, point0, n, iter, stream, reinterpret_cast<float4*>(out_dev));
+  int rc = cp_flow_forward_enqueue(h, point0, n, iter, stream, reinterpret_cast<float4*>(out_dev), nullptr);
   if (rc) return rc;
   CP_CUDA(h, cudaStreamSynchronize(h->stream));
   return cp_flow_tc_status(h);

@@ -274,7 +274,8 @@ template <int NWG, bool ACCEPT>
 __device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g, const float* __restrict__ params,
                                                 const double* __restrict__ edges, int nb, uint64_t seed, uint64_t point0,
                                                 uint64_t n, uint32_t iter, uint32_t stream, float4* __restrict__ out,
-                                                int* __restrict__ status, int stall, const CpHadParams* P,
+                                                float* __restrict__ uout, int* __restrict__ status, int stall,
+                                                const CpHadParams* P,
                                                 const UnwLaunch* L)
 {
   using Lay = CpTcLayout<NWG>;
@@ -413,7 +414,7 @@ __device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g,
       p[s] = qq * 256 + s * 128 + row;
       uint32_t w[4] = {0x80000000u, 0x80000000u, 0x80000000u, 0u};
       if (p[s] < n) cp_point_words(seed, point0 + p[s], iter, stream, w);
-      if constexpr (ACCEPT) u[s] = cp_u24(w[3]);
+      if (ACCEPT || uout) u[s] = cp_u24(w[3]);
       float jv = 1.f, ld = 0.f, z[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -484,7 +485,10 @@ __device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g,
                 fin1 = make_float4(v0, v1, v2, ld); fp1 = p[s]; fu1 = u[s];
               }
             } else {
-              if (p[s] < n) out[p[s]] = make_float4(v0, v1, v2, ld);
+              if (p[s] < n) {
+                out[p[s]] = make_float4(v0, v1, v2, ld);
+                if (uout) uout[p[s]] = u[s];   // the accept draw, so the accept kernel need not redraw it
+              }
             }
             if (qn < npairs) start(s, qn);
           }
@@ -531,9 +535,9 @@ __device__ __forceinline__ void cp_flow_tc_body(const uint4* __restrict__ img_g,
 __global__ void __launch_bounds__(CpTcLayout<CP_TC_WG>::THREADS, 1)
     k_flow_fwd_tc(const uint4* __restrict__ img_g, const float* __restrict__ params, const double* __restrict__ edges,
                   int nb, uint64_t seed, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream,
-                  float4* __restrict__ out, int* __restrict__ status, int stall)
+                  float4* __restrict__ out, float* __restrict__ uout, int* __restrict__ status, int stall)
 {
-  cp_flow_tc_body<CP_TC_WG, false>(img_g, params, edges, nb, seed, point0, n, iter, stream, out, status, stall,
+  cp_flow_tc_body<CP_TC_WG, false>(img_g, params, edges, nb, seed, point0, n, iter, stream, out, uout, status, stall,
                                    nullptr, nullptr);
 }
 
@@ -545,7 +549,7 @@ __global__ void __launch_bounds__(CpTcLayout<CP_TC_WG_ACC>::THREADS, 1)
                      int* __restrict__ status, int stall)
 {
   cp_flow_tc_body<CP_TC_WG_ACC, true>(img_g, params, L.edges, L.nb, L.seed, L.point0, L.n, L.iter, 0u, nullptr,
-                                      status, stall, &P, &L);
+                                      nullptr, status, stall, &P, &L);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -571,7 +575,8 @@ int cp_flow_tc_alloc(cp_handle* h)
   return CP_OK;
 }
 
-int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out)
+int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out,
+                       float* uout)
 {
   if (h->flow_tc_stale) {
     const int rc = cp_flow_tc_repack(h);
@@ -585,7 +590,7 @@ int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter,
   k_flow_fwd_tc<<<grid, CpTcLayout<CP_TC_WG>::THREADS, CpTcLayout<CP_TC_WG>::SMEM, h->stream>>>(reinterpret_cast<const uint4*>(h->d_flow_tc), h->d_flow,
                                                                  h->d_edges,
                                                                  h->nb, h->cfg.seed, point0, n, iter, stream, out,
-                                                                 h->d_flow_status, h->flow_stall);
+                                                                 uout, h->d_flow_status, h->flow_stall);
   CP_LAUNCH_CHECK(h, "k_flow_fwd_tc");
   return CP_OK;
 }

@@ -151,6 +151,7 @@ struct cp_handle {
   uint2* d_flow_pk = nullptr;
   float* d_flow_bias = nullptr;
   float4* d_flow_buf = nullptr;
+  float* d_flow_u = nullptr;                // accept draws of d_flow_buf's points (same allocation)
   uint64_t flow_buf_cap = 0;
   int flow_on = 0;
   long flow_t = 0;                         // optimiser updates so far (a step's batch iteration)
@@ -184,10 +185,15 @@ int cp_fail_cuda(cp_handle* h, cudaError_t e, const char* what);
 int cp_ensure_slots(cp_handle* h, size_t doubles);
 int cp_ensure_iters(cp_handle* h, int n);
 int cp_flow_buffer(cp_handle* h, uint64_t n);
-int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out);
+// uout, if not null, receives each point's accept draw u24(word 3) of its Philox block when the
+// tensor-core forward runs (cp_flow_writes_u); the mma.sync forward leaves it untouched.
+int cp_flow_forward_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out,
+                            float* uout);
+inline bool cp_flow_writes_u(const cp_handle* h) { return h->flow_kernel == 0; }
 int cp_flow_tc_alloc(cp_handle* h);
 int cp_flow_tc_repack(cp_handle* h);
-int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out);
+int cp_flow_tc_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float4* out,
+                       float* uout);
 int cp_flow_tc_status(cp_handle* h);
 
 // Makes `dev` the calling thread's current device for the rest of the scope and restores the

@@ -94,11 +94,19 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
     const uint64_t p = r * stride + gtid;
     uint32_t wd[4] = {0u, 0u, 0u, 0u};
     CpMapped m{};
+    float u = 0.f;
     if (p < L.n) {
-      cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
-      m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
+      if (L.flow_u) {
+        // the flow forward drew this point's Philox block for the map and kept its accept draw
+        m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
+        u = L.flow_u[p];
+      } else {
+        cp_point_words(L.seed, L.point0 + p, L.iter, 0, wd);
+        m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
+        u = cp_u24(wd[3]);
+      }
     }
-    cp_unw_point(P, P.cteq, L, wmax, p, m.x[0], m.x[1], m.x[2], m.jv, cp_u24(wd[3]), S);
+    cp_unw_point(P, P.cteq, L, wmax, p, m.x[0], m.x[1], m.x[2], m.jv, u, S);
   }
   double v[7];
   cp_unw_warp_sums(S, v);
@@ -329,7 +337,7 @@ static bool fused_production(const cp_handle* h) { return h->flow_on && h->flow_
 // runs its own.  tslot >= 0 records the chunk's timing events.
 static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, cp_event* out,
                             uint64_t capacity, double* red_dst, float* scalew, unsigned long long* base_dev,
-                            const float4* flow_pre, int tslot)
+                            const float4* flow_pre, const float* flow_u_pre, int tslot)
 {
   if (n > CP_UNW_CHUNK) return cp_fail(h, CP_ERR_INVALID, "production chunk above CP_UNW_CHUNK points");
   const int blocks = unw_blocks(h);
@@ -352,16 +360,20 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
     CP_CUDA(h, cudaMemsetAsync(h->d_rsum, 0, sizeof(unsigned) * L.nrange, h->stream));
   }
   L.flow = nullptr;
+  L.flow_u = nullptr;
   const bool fused = fused_production(h);
   if (h->flow_on && !fused) {
     if (flow_pre) {
       L.flow = flow_pre;
+      L.flow_u = flow_u_pre;
     } else {
       rc = cp_flow_buffer(h, n);
       if (rc) return rc;
-      rc = cp_flow_forward_enqueue(h, point0, n, iter, 0, h->d_flow_buf);
+      float* ut = cp_flow_writes_u(h) ? h->d_flow_u : nullptr;
+      rc = cp_flow_forward_enqueue(h, point0, n, iter, 0, h->d_flow_buf, ut);
       if (rc) return rc;
       L.flow = h->d_flow_buf;
+      L.flow_u = ut;
     }
   }
   cudaEvent_t* ev = (h->timing && tslot >= 0 && h->tpool.size() >= 2 + 3 * (size_t)(tslot + 1)) ? &h->tpool[2 + 3 * tslot] : nullptr;
@@ -457,14 +469,16 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
     rc = cp_flow_buffer(h, n_points);
     if (rc) return rc;
     if (h->timing) cudaEventRecord(h->tpool[0], h->stream);
-    rc = cp_flow_forward_enqueue(h, h->point_offset, n_points, iter, 0, h->d_flow_buf);
+    rc = cp_flow_forward_enqueue(h, h->point_offset, n_points, iter, 0, h->d_flow_buf,
+                                 cp_flow_writes_u(h) ? h->d_flow_u : nullptr);
     if (rc) return rc;
     if (h->timing) cudaEventRecord(h->tpool[1], h->stream);
   }
   for (uint64_t c = 0; c < nsub; ++c) {
     const uint64_t p0 = c * CP_UNW_CHUNK, n = p0 + CP_UNW_CHUNK <= n_points ? CP_UNW_CHUNK : n_points - p0;
     rc = unweight_enqueue(h, p0, n, iter, records_dev, capacity, h->d_unw_red + 8 * c, h->scalew, h->d_counter,
-                          (h->flow_on && !fused) ? h->d_flow_buf + p0 : nullptr, (int)c);
+                          (h->flow_on && !fused) ? h->d_flow_buf + p0 : nullptr,
+                          (h->flow_on && !fused && cp_flow_writes_u(h)) ? h->d_flow_u + p0 : nullptr, (int)c);
     if (rc) return rc;
   }
   std::vector<double> hred(8 * nsub, 0.0);
@@ -574,7 +588,7 @@ extern "C" int cp_generate_host(cp_handle* h, uint64_t n_points, uint32_t iter, 
       const uint64_t p0 = c * chunk, n = (p0 + chunk <= n_points) ? chunk : n_points - p0;
       if (c >= CP_GEN_BUFS && (e = cudaStreamWaitEvent(h->stream, h->gen_copied[b], 0)) != cudaSuccess) break;
       rc = unweight_enqueue(h, p0, n, iter, h->d_gen_stage + (uint64_t)b * chunk, chunk, h->d_gen_red + 8 * c,
-                            nullptr, h->d_gen_cnt + c, nullptr, -1);
+                            nullptr, h->d_gen_cnt + c, nullptr, nullptr, -1);
       if (rc) break;
       k_gen_count<<<1, 1, 0, h->stream>>>(h->d_gen_cnt + c, dcnt_mapped + c);
       if ((e = cudaGetLastError()) != cudaSuccess) break;

@@ -26,6 +26,7 @@ struct UnwLaunch {
   uint64_t capacity;
   double* slots;
   const float4* flow;          // flow output (v, ln J) per in-call point, or null (K1 only)
+  const float* flow_u;         // the flow forward's accept draw per in-call point, or null: K1 draws it
 };
 
 // the tensor-core flow kernel's production form over one chunk (cp_flow_tc.cu)

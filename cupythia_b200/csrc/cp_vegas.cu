@@ -237,7 +237,7 @@ static int had_launch(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, 
   if (h->flow_on) {
     rc = cp_flow_buffer(h, n);
     if (rc) return rc;
-    rc = cp_flow_forward_enqueue(h, point0, n, iter, stream, h->d_flow_buf);
+    rc = cp_flow_forward_enqueue(h, point0, n, iter, stream, h->d_flow_buf, nullptr);
     if (rc) return rc;
     L.flow = h->d_flow_buf;
   }
