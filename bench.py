@@ -187,8 +187,8 @@ EXEC_FLOP_PER_POINT = 1866.7
 FLOW_FLOP_PER_POINT = 35072.0     # k_flow_fwd: 2 x sum over couplings of (n_in*64 + 64*64 + 64*n_out) MACs
 # DRAM bytes (read + write) per point of the flow-form launches, from ncu captures of 2^24-point
 # launches of the same workload (profiles/traffic_flow_form_2e24.md); scaled to a launch's points
-TRAFFIC_PER_POINT = {"k_unw_accept": (276270336 + 686841600) / 2 ** 24,
-                     "k_flow_fwd_tc": (366592 + 209136896) / 2 ** 24}
+TRAFFIC_PER_POINT = {"k_unw_accept": (343450880 + 688227584) / 2 ** 24,
+                     "k_flow_fwd_tc": (158976 + 275642624) / 2 ** 24}
 
 
 def production(it, n, records, k0, warmup, steps, pg, dev, stream, clocks=None):
