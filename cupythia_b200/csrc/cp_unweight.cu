@@ -462,7 +462,7 @@ extern "C" int cp_unweight(cp_handle* h, uint64_t n_points, uint32_t iter, cp_ev
   int rc = timing_reserve(h, nsub);
   if (rc) return rc;
   CP_CUDA(h, cudaMemsetAsync(h->d_counter, 0, sizeof(unsigned long long), h->stream));
-  // the flow forward once for the whole pass (16 B per point), then the chunks; the fused form
+  // the flow forward once for the whole pass (20 B per point: (v, ln J) and the accept draw), then the chunks; the fused form
   // runs the forward inside each chunk's accept kernel
   const bool fused = fused_production(h);
   if (h->flow_on && !fused) {

@@ -343,7 +343,7 @@ int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uin
 int cp_flow_select_kernel(cp_handle* h, int which);
 /* Production passes in the flow form (cp_unweight, cp_generate_host) with the tcgen05 forward:
  * on != 0 runs the flow forward, the integrand and the accept step as one kernel per chunk, the
- * flow's output never leaving the SM (no 16-byte-per-point flow buffer); 0 (default) runs the
+ * flow's output never leaving the SM (no 20-byte-per-point flow buffer); 0 (default) runs the
  * forward over the pass first and the accept kernel on its stored output, which is faster on
  * B200 (17.9 ms against 19.3 ms per 2^27-point pass of the two kernels' work).  Both give the
  * same records, byte for byte, and the same counts; the sums of w and w^2 differ by their FP64
