@@ -150,20 +150,38 @@ CP_HD T cp_poly_t(const CpCteqPoly& c, int f, const T& t)
   return (c.co[2][f] * t + c.co[1][f]) * t + c.co[0][f];
 }
 
+// the x-dependent quantities of one beam, shared by the 8 parametrisations
 template <class T>
-CP_HD T cp_cteq_answer_t(const CpCteqPoly& c, const T& sb1, const T& invQ, const T& lnxIn)
+struct CpBeamT {
+  T x, omx, y, u, x1L, lny;
+};
+
+template <class T>
+CP_HD CpBeamT<T> cp_beam_t(const T& lnxIn)
 {
   // x <= 1 - 1e-10 clamp of PartonDistributions.cc:926 (constant beyond it)
-  T lnx = cp_val(lnxIn) > -1e-10f ? T(lnxIn * 0.f - 1e-10f) : lnxIn;
-  T x = cp_exp_t(lnx);
-  T omx = -cp_expm1_t(lnx);
-  T y = -lnx;
-  T u = lnx + 11.512925465f;
-  T x1L = cp_log_t(omx);
+  const T lnx = cp_val(lnxIn) > -1e-10f ? T(lnxIn * 0.f - 1e-10f) : lnxIn;
+  CpBeamT<T> b;
+  b.x = cp_exp_t(lnx);
+  b.omx = -cp_expm1_t(lnx);
+  b.y = -lnx;
+  b.u = lnx + 11.512925465f;
+  b.x1L = cp_log_t(b.omx);
+  b.lny = cp_log_t(b.y);
+  return b;
+}
+
+template <class T>
+CP_HD T cp_cteq_answer_t(const CpCteqPoly& c, const T& sb1, const T& invQ, const CpBeamT<T>& b)
+{
+  const T& x = b.x;
+  const T& omx = b.omx;
+  const T& u = b.u;
+  const T& x1L = b.x1L;
   T A = cp_poly_t(c, CP_CQ_A, sb1), B = cp_poly_t(c, CP_CQ_B, sb1), af1 = cp_poly_t(c, CP_CQ_AF1, sb1);
   T af2 = cp_poly_t(c, CP_CQ_AF2, sb1), p = cp_poly_t(c, CP_CQ_P, sb1), af5 = cp_poly_t(c, CP_CQ_AF5, sb1);
   T af6 = cp_poly_t(c, CP_CQ_AF6, sb1), af7 = cp_poly_t(c, CP_CQ_AF7, sb1), af8 = cp_poly_t(c, CP_CQ_AF8, sb1);
-  T ym1 = cp_expm1_t(p * cp_log_t(y));
+  T ym1 = cp_expm1_t(p * b.lny);
   T U = af8 * u + 1.f;
   T part3 = x * omx * (af5 + af6 * omx + af7 * x * omx);
   T L = c.useX1L ? x1L : cp_log_t(omx + c.eut2);
@@ -183,17 +201,22 @@ CP_HD void cp_cteq_pair_t(const CpCteqPoly* cteq, T Q2, T lnxA, T lnxB, T fa[8],
   T Q = cp_sqrt_t(Q2);
   T lnQ = 0.5f * cp_log_t(Q2);
   T invQ = 1.f / Q;
+  // once per beam rather than once per parametrisation and beam: the same operations on the same
+  // values (the host build gives bit-identical results; on the device the compiler may contract a
+  // different product into an FMA, a last-bit difference).  12 adjoint passes of 2^22 points:
+  // 38.1 -> 33.6 ms
+  const CpBeamT<T> bA = cp_beam_t(lnxA), bB = cp_beam_t(lnxB);
 #pragma unroll 1
   for (int i = 0; i < 8; ++i) {
     const CpCteqPoly& c = cteq[i];
     T sb1 = cp_log_t(lnQ - c.lnAlpha) - 1.2f;
     T ra, rb;
     if (cp_val(Q) > c.qlim) {
-      ra = cp_cteq_answer_t(c, sb1, invQ, lnxA);
-      rb = cp_cteq_answer_t(c, sb1, invQ, lnxB);
+      ra = cp_cteq_answer_t(c, sb1, invQ, bA);
+      rb = cp_cteq_answer_t(c, sb1, invQ, bB);
       if (i != 4) {
-        ra = ra * cp_exp_t(cp_val(lnxA) > -1e-10f ? T(lnxA * 0.f - 1e-10f) : lnxA);
-        rb = rb * cp_exp_t(cp_val(lnxB) > -1e-10f ? T(lnxB * 0.f - 1e-10f) : lnxB);
+        ra = ra * bA.x;
+        rb = rb * bB.x;
       }
     } else {
       ra = sb1 * 0.f;
