@@ -76,6 +76,9 @@ __device__ __forceinline__ void cp_stage_edges(float2 (*sEdge)[CP_MAX_BINS], con
 // K1: weight, accept; per 32-point block the accept mask (its popcount added to its range's
 // total), and each accepted point's event weight, coordinates and PDFs packed at the front of the
 // block's staging slots in point order; K2 builds the record from them.
+// FLOW_U: the points' accept draws come from the flow forward's output (L.flow_u) instead of their
+// Philox blocks; a separate instance, so the plain form's kernel carries no code for it
+template <bool FLOW_U>
 __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const __grid_constant__ CpHadParams P,
                                                                            const __grid_constant__ UnwLaunch L)
 {
@@ -96,7 +99,7 @@ __global__ void __launch_bounds__(CP_THREADS, CP_MIN_BLOCKS) k_unw_accept(const 
     CpMapped m{};
     float u = 0.f;
     if (p < L.n) {
-      if (L.flow_u) {
+      if constexpr (FLOW_U) {
         // the flow forward drew this point's Philox block for the map and kept its accept draw
         m = cp_map_any(sEdge, L.nb, wd, L.flow, p);
         u = L.flow_u[p];
@@ -250,7 +253,7 @@ static int unw_blocks(cp_handle* h)
 {
   if (h->unw_per_sm < 0) {
     int per_sm = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unw_accept, CP_THREADS, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_unw_accept<false>, CP_THREADS, 0) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
     h->unw_per_sm = per_sm;
@@ -383,7 +386,8 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
     rc = cp_flow_tc_accept_enqueue(h, L, &red_blocks);
     if (rc) return rc;
   } else {
-    k_unw_accept<<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+    if (L.flow_u) k_unw_accept<true><<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
+    else k_unw_accept<false><<<blocks, CP_THREADS, 0, h->stream>>>(h->P, L);
     CP_LAUNCH_CHECK(h, "k_unw_accept");
   }
   if (ev) cudaEventRecord(ev[1], h->stream);
