@@ -349,7 +349,7 @@ static int unweight_enqueue(cp_handle* h, uint64_t point0, uint64_t n, uint32_t 
   point0 += h->point_offset;
   UnwLaunch L;
   L.seed = h->cfg.seed; L.point0 = point0; L.n = n; L.iter = iter; L.nb = h->nb;
-  L.edges = h->d_edges; L.cteq = h->d_cteq; L.wmax = h->d_wmax;
+  L.edges = h->d_edges; L.wmax = h->d_wmax;
   L.out = reinterpret_cast<CpEventRec*>(out);
   L.capacity = capacity; L.slots = h->d_slots;
   L.pdf = nullptr; L.tails = nullptr; L.bmask = nullptr; L.roff = nullptr; L.rsum = nullptr;

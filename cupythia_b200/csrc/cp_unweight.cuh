@@ -13,7 +13,6 @@ struct UnwLaunch {
   uint32_t iter;
   int nb;
   const double* edges;
-  const CpCteqPoly* cteq;
   const double* wmax;          // device threshold
   CpEventRec* out;
   float4* pdf;                 // staging per point: fa[8], fb[8] of the accepted points (K1 -> K2)
