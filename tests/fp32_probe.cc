@@ -49,6 +49,13 @@ void probe_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k
 {
   cp_philox(c0, c1, c2, c3, k0, k1, out);
 }
+// cp_build_had_params' verdict on a configuration (0: the kernels support it)
+int probe_build_params(double sqrtS, double pTmin, double aSmZ)
+{
+  CpHadConfig c{sqrtS, pTmin, aSmZ, 1.0, 1.0, 0.389380, 5, 3, 31};
+  CpHadParams P;
+  return cp_build_had_params(c, P);
+}
 // the integrand's two-lane exp reduction: e^a and e^a - 1 of n arguments (pairs of lanes)
 void probe_exp_reduce(const float* a, int n, float* e, float* em1)
 {

@@ -105,3 +105,13 @@ def test_exp_reduction_within_its_bound(probe, lo, hi):
     if small.any():
         assert np.max(np.abs(m[small] - ref_m[small]) / np.abs(ref_m[small])) < 2.5 * ulp
     assert m[2] == 0.0 and m[3] == np.float32(-1e-30)
+
+
+def test_parameter_builder_keeps_the_exp_reduction_in_range(probe):
+    """x0 ln tauMin enters the kernels' exp reduction, whose 2^k scale is valid for arguments above
+    -87: configurations with ln tauMin <= -80 are refused, ordinary ones accepted."""
+    f = probe.probe_build_params
+    f.argtypes = [C.c_double, C.c_double, C.c_double]
+    assert f(13000.0, 20.0, 0.13) == 0
+    assert f(1.0e6, 2.0, 0.13) == 0              # ln tauMin = ln(16 / 1e12) = -27.2
+    assert f(1.0e18, 2.0, 0.13) != 0             # ln tauMin = -80.1
