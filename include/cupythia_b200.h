@@ -339,7 +339,9 @@ int cp_flow_set_state(cp_handle* h, const float* state_host, int n, int64_t upda
 int cp_flow_sample(cp_handle* h, uint64_t point0, uint64_t n, uint32_t iter, uint32_t stream, float* out_dev);
 /* Forward kernel used by cp_flow_sample and the flow-routed passes: 0 = tcgen05 MMAs with TMEM
  * accumulators over 128-point tiles (default), 1 = warp-level mma.sync tiles.  Both compute the
- * same map; CP_ERR_TIMEOUT from a flow-routed call means a bounded tensor-core wait expired. */
+ * same map; CP_ERR_TIMEOUT from a flow-routed call means a bounded tensor-core wait expired.  In
+ * production passes the tcgen05 forward also hands each point's accept draw to the accept kernel;
+ * with the mma.sync forward the accept kernel draws it itself (same values, slower pass). */
 int cp_flow_select_kernel(cp_handle* h, int which);
 /* Production passes in the flow form (cp_unweight, cp_generate_host) with the tcgen05 forward:
  * on != 0 runs the flow forward, the integrand and the accept step as one kernel per chunk, the
